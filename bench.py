@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the plain PISO + LES time step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl windfvm|reference]
+
+A step is one complete time step (wall function, LES, momentum predictor with
+50 Jacobi sweeps, Rhie-Chow pressure correction with 40 sweeps, 2 PISO
+correctors with 40 sweeps each) of the urban-block workload: 256 x 96(up) x
+192 cells of 0.5 m, 48 seeded buildings, log-law inflow u* = 0.6 m/s, z0 =
+0.3 m with a 5 % inlet perturbation (synthetic, seeded; the reference ships
+no dataset).  The metric is Mcell-steps/s = cells x steps / s / 1e6.
+
+Multi-GPU: replicas only -- every rank steps its own copy of the workload,
+there is no data-path collective; value = all ranks' cell-steps / max rank
+time.  Rank 0 prints one JSON line.
+
+--impl reference times the reference's algorithm on the host cores: the
+reference itself (C# + HLSL through Unity/D3D) cannot run on this machine, so
+its CPU restatement (oracle/, FP32, OpenMP over all cores) stands in.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s"
+B_ALG_FIXED = 287  # compulsory bytes per cell-step of the non-iterative kernels
+
+
+def b_alg(nv: int, np_: int, nc: int) -> int:
+    """Algorithmic bytes per cell-step of the reference kernel sequence (each
+    kernel reads each input once and writes each output once; vector 12 B,
+    scalar 4 B, flag 1 B)."""
+    return B_ALG_FIXED + 77 * nv + 29 * np_ + nc * (123 + 33 * np_)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="windfvm", choices=["windfvm", "reference"])
+    ap.add_argument("--workload", default="urban_block")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_case(name: str):
+    from unitywindsimulation_b200 import cases
+    return cases.WORKLOADS[name]()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """DRAM bytes per cell of one launch of `kernel`, from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)
+        return d[kernel]
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), p[5], p[6], p[7], p[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = []
+        for i, name in enumerate(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]):
+            if any(r[2 + i].lower() == "active" for r in rows):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(case, steps: int):
+    """The FP32 oracle on all host cores over a bounded sample of the workload."""
+    from oracle import OracleSolver
+    cores = os.cpu_count() or 1
+    o = OracleSolver(case.cfg, 32, threads=cores)
+    o.InitFlags(case.flags)
+    if case.inlet is not None:
+        o.set_inflow_plane(case.inlet)
+    o.Step(1)  # warm-up (first touch of the fields)
+    t0 = time.perf_counter()
+    o.Step(steps)
+    dt = time.perf_counter() - t0
+    v = case.n_cells * steps / dt / 1e6
+    return {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": f"{steps} full steps of {case.name} ({case.n_cells} cells) after 1 warm-up step, "
+                      f"FP32 oracle, OpenMP {cores} threads"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    case = make_case(args.workload)
+    k = max(1, min(args.steps, 6))
+    w = min(args.warmup, 1)
+    from oracle import OracleSolver
+    cores = os.cpu_count() or 1
+    o = OracleSolver(case.cfg, 32, threads=cores)
+    o.InitFlags(case.flags)
+    if case.inlet is not None:
+        o.set_inflow_plane(case.inlet)
+    o.Step(w)
+    t0 = time.perf_counter()
+    o.Step(k)
+    dt = time.perf_counter() - t0
+    v = case.n_cells * k / dt / 1e6
+    cfg = case.cfg
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(case),
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{k} full steps after {w} warm-up of {case.name}; the reference (C#/HLSL via "
+                                   f"Unity+D3D) cannot run here, its CPU restatement (FP32 oracle, OpenMP "
+                                   f"{cores} threads) stands in"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(case):
+    c = case.cfg
+    ws = 4 * case.n_cells * (3 * 8 + 6 + 6 + 9 + 5 + 0.25)
+    return {"workload": f"{case.name} {c.nx}x{c.ny}(up)x{c.nz} cells, PISO+LES, nV={c.vel_iters} "
+                        f"nP={c.pres_iters} nC={c.piso_correctors}",
+            "cells": case.n_cells, "grid_ref_order": [c.nx, c.ny, c.nz], "dx": c.dx, "dt": c.dt,
+            "vel_iters": c.vel_iters, "pres_iters": c.pres_iters, "piso_correctors": c.piso_correctors,
+            "b_alg_bytes_per_cell_step": b_alg(c.vel_iters, c.pres_iters, c.piso_correctors),
+            "l2": f"inputs larger than L2: {ws / 1e6:.0f} MB of fields vs 126 MB L2",
+            "parallelism": "replicas", "seed": case.seed}
+
+
+def run_windfvm(args):
+    import numpy as np
+    import torch
+
+    from unitywindsimulation_b200 import FvmSolverCuda, _lib, cases
+
+    rank, world, local = dist_env()
+    dist = world > 1
+    if dist:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    case = make_case(args.workload)
+    cfg = case.cfg
+    N = case.n_cells
+    solver = FvmSolverCuda(cfg, device=local)
+    cases.apply_case(solver, case)
+
+    def barrier():
+        if dist:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident throughput ----
+    solver.Step(args.warmup)
+    barrier()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    smi_index = int(vis.split(",")[local]) if vis and vis.split(",")[local].isdigit() else local
+    clk = ClockSampler(smi_index)
+    clk.start()
+    l0 = solver.kernel_launches()
+    solver.Step(args.steps)
+    ms = solver.last_step_ms()
+    launches = solver.kernel_launches() - l0
+    clocks = clk.stop()
+    barrier()
+    ms_max = max_over_ranks(ms)
+    value = world * N * args.steps / (ms_max / 1e3) / 1e6
+    solver.check_finite()
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        inlet = case.inlet if case.inlet is not None else np.zeros((cfg.nz, cfg.ny, 3), np.float32)
+        h_in = torch.empty(inlet.size, dtype=torch.float32, pin_memory=True)
+        h_in.numpy()[:] = inlet.reshape(-1)
+        h_vel = torch.empty(3 * N, dtype=torch.float32, pin_memory=True)
+        h_pres = torch.empty(N, dtype=torch.float32, pin_memory=True)
+        stream = torch.cuda.ExternalStream(solver.stream_ptr)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            solver.set_inflow_plane(h_in.numpy())
+            solver.Step(1)
+            solver.GetVelField(out=h_vel.numpy())
+            solver.GetPresField(out=h_pres.numpy())
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        e_ms = max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": world * N * args.steps / (e_ms / 1e3) / 1e6, "unit": METRIC,
+               "h2d_bytes_per_step": int(inlet.size * 4), "d2h_bytes_per_step": int(4 * N * 4),
+               "api": "set_inflow_plane + Step + GetVelField + GetPresField, pinned host buffers"}
+
+    # ---- roofline of the dominant kernel (pressure Jacobi sweep) ----
+    peak, peak_kind = measured_peaks()
+    k_ms, k_bytes, k_sweeps = solver.time_kernel(_lib.KERNEL_PRES_SWEEP, reps=20, flush_l2=True)
+    achieved = k_bytes / (k_ms / 1e3) / 1e9
+    tr = committed_traffic("pres_sweep")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tr * N) if tr is not None else None,
+                "kernel": "pressure Jacobi sweep", "ms_per_launch": k_ms, "sweeps_per_launch": k_sweeps,
+                "alg_bytes_per_launch": k_bytes, "peak_source": f"hbm_gbs of {peak_kind}"}
+    v_ms, v_bytes, v_sweeps = solver.time_kernel(_lib.KERNEL_VEL_SWEEP, reps=10, flush_l2=True)
+    step_gbs = value / world * b_alg(cfg.vel_iters, cfg.pres_iters, cfg.piso_correctors) / 1e3
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(case, args.cpu_sample_steps)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(case),
+            "e2e": e2e, "gpu_launches": launches * world, "clocks": clocks, "roofline": roofline,
+            "cpu_baseline": cpu,
+            "step_alg_gbs": step_gbs, "step_alg_frac": step_gbs / peak,
+            "vel_sweep_kernel": {"ms_per_launch": v_ms, "alg_bytes_per_launch": v_bytes,
+                                 "achieved_gbs": v_bytes / (v_ms / 1e3) / 1e9, "sweeps_per_launch": v_sweeps},
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_windfvm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

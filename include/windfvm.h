@@ -1,0 +1,284 @@
+/*
+ * windfvm.h - C ABI of the B200 (sm_100a) urban-wind FVM solver.
+ *
+ * This library is a drop-in for the HLSL compute-dispatch path of
+ * puppy2333/UnityWindSimulation: the collocated, uniform-grid SIMPLE/PISO
+ * time step with Smagorinsky LES and log-law wall functions that
+ * FvmSolverController drives through IFvmSolver.Step().
+ *
+ *   reference interface             replaced by
+ *   IFvmSolver (Assets/Code/FvmSolver/IFvmSolver.cs:3-24)
+ *     FvmSolverGpu ctor (FvmSolverGpu.cs:173-222)        wf_create
+ *     Step()            (FvmSolverGpu.cs:1050-1121)      wf_step
+ *     InitFlags(int[])  (FvmSolverGpu.cs:972-987)        wf_init_flags
+ *     InitVelPresFields (FvmSolverGpu.cs:790-896)        wf_init_vel_pres_fields
+ *     SetFixedValueVelBndCond (FvmSolverGpu.cs:996-1022) wf_set_fixed_value_vel_bnd_cond
+ *     ChangePhysFieldPos (FvmSolverGpu.cs:1026-1032)     wf_change_phys_field_pos
+ *     ChangePhysDomainSize (FvmSolverGpu.cs:1034-1046)   (re-create the handle; see below)
+ *     GetVelField/GetPresField/GetFlagField (:1568-1582) wf_get_vel / wf_get_pres / wf_get_flags
+ *
+ * Conventions
+ *   - Axes follow the reference: x streamwise, y vertical (ground at y = 0),
+ *     z spanwise.  Host arrays are flat, x fastest: index = z*nx*ny + y*nx + x
+ *     (InitShaderColl.compute:353, BuildingVoxelizer.cs:392).
+ *   - Every entry point returns an int status (WF_OK = 0).  Nothing throws or
+ *     aborts across the ABI.  wf_last_error(h) gives a message for the last
+ *     failure on a handle, wf_strerror(status) a generic one.
+ *   - A handle is not thread-safe.  All work of a handle runs on its own CUDA
+ *     stream; blocking host copies synchronise that stream only.  Distinct
+ *     handles may be used from distinct threads.
+ *   - The library owns all device memory.  Host buffers are owned by the
+ *     caller and copied synchronously.
+ *   - All arithmetic is FP32.
+ */
+#ifndef WINDFVM_H
+#define WINDFVM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WF_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    WF_OK = 0,
+    WF_ERR_INVALID_ARG = 1,  /* bad pointer, size, enum value or config      */
+    WF_ERR_CUDA = 2,         /* a CUDA runtime call failed                   */
+    WF_ERR_OOM = 3,          /* device allocation failed                     */
+    WF_ERR_NONFINITE = 4,    /* NaN/Inf found in the solution                */
+    WF_ERR_TIMEOUT = 5,      /* a bounded device wait gave up                */
+    WF_ERR_UNSUPPORTED = 6,  /* option not implemented for this build        */
+    WF_NOT_FINISHED = 7,     /* step stopped early (time budget)             */
+    WF_ERR_STATE = 8         /* call not valid in the handle's current state */
+};
+
+/* ---- enums mirroring Constants.hlsl:4-14 and FluidSimConfig.cs:16-96 ---- */
+enum { WF_CELL_FLUID = 0, WF_CELL_SOLID = 1 };
+enum { WF_BND_FIXED_VALUE = 0, WF_BND_ZERO_GRAD = 1, WF_BND_SYMMETRY = 2 };
+enum { WF_FACE_X0 = 0, WF_FACE_XN = 1, WF_FACE_Y0 = 2, WF_FACE_YN = 3,
+       WF_FACE_Z0 = 4, WF_FACE_ZN = 5 };
+enum { WF_SOLVER_SIMPLE = 0, WF_SOLVER_PISO = 1 };
+enum { WF_TURB_NONE = 0, WF_TURB_SMAGORINSKY = 1 };
+enum { WF_INFLOW_CONSTANT = 0, WF_INFLOW_LOG = 1 };
+
+/* ---- reference-quirk switches (wf_config.compat_flags) ------------------
+ * WF_COMPAT_RFLOAT_FACE_EDDY_VIS: faceEddyVisField is allocated RFloat
+ *   (FvmSolverGpu.cs:304) but written/read as float4 (WallFunc.compute:189,
+ *   FvmColl.compute:93).  Under D3D typed-UAV rules only .x survives, so the
+ *   y- and z-normal wall viscosities read back as 0.  Set this flag to get the
+ *   as-shipped behaviour; clear it (default) for the intended three channels.
+ * WF_COMPAT_INIT_PROFILE_CELL_CENTRE: the reference initialises the interior
+ *   log profile at y = j*dx (InitShaderColl.compute:120) but the inlet at
+ *   (j+0.5)*dx (:279).  Set this flag to use (j+0.5)*dx for both.
+ * WF_COMPAT_PISO_CONSISTENT: the reference PISO corrector uses nu only in
+ *   A_od and no fixed-pressure boundary term (PisoColl.compute:135-169,
+ *   200-253).  Set this flag to use nu + nu_t face viscosities and the
+ *   fixed-pressure face term instead.  Default: reproduce the reference.     */
+#define WF_COMPAT_RFLOAT_FACE_EDDY_VIS     0x1u
+#define WF_COMPAT_INIT_PROFILE_CELL_CENTRE 0x2u
+#define WF_COMPAT_PISO_CONSISTENT          0x4u
+
+/* ---- configuration -------------------------------------------------------
+ * Mirrors FluidSimConfig (FluidSimConfig.cs:113-178) + RuntimeConfig
+ * (RuntimeConfig.cs:8-9) + the inflow constants hard-coded in
+ * FvmSolverGpu.cs:816-819.  Fill it with wf_config_default() first.        */
+typedef struct wf_config {
+    uint32_t struct_size;       /* = sizeof(wf_config)                       */
+    int32_t  nx, ny, nz;        /* gridRes (x streamwise, y vertical)        */
+    float    dx;                /* cell size [m]; ds = dx^2, dv = dx^3       */
+    float    dt;                /* time step [s]                             */
+    float    mu;                /* dynamic viscosity; nu = mu / den          */
+    float    den;               /* density                                   */
+    float    ext_force[3];      /* externalForce                             */
+    int32_t  vel_bc[6];         /* WF_BND_*, indexed by WF_FACE_*            */
+    int32_t  pres_bc[6];        /* WF_BND_*, indexed by WF_FACE_*            */
+    int32_t  solver_type;       /* WF_SOLVER_SIMPLE / WF_SOLVER_PISO         */
+    int32_t  piso_correctors;   /* PISONumCorrectors                         */
+    int32_t  turbulence;        /* WF_TURB_NONE / WF_TURB_SMAGORINSKY        */
+    float    cs;                /* smagorinskyConstant                       */
+    int32_t  vel_iters;         /* velMaxNumIter (Jacobi sweeps, momentum)   */
+    int32_t  pres_iters;        /* presMaxNumIter (Jacobi sweeps, pressure)  */
+    int32_t  inflow_type;       /* WF_INFLOW_CONSTANT / WF_INFLOW_LOG        */
+    float    wind_speed;        /* RuntimeConfig.windSpeed (= velX0.x)       */
+    float    inflow_ustar;      /* > 0: friction velocity used directly      */
+    float    inflow_z0;         /* roughParam (reference: 1.0)               */
+    float    inflow_kappa;      /* karmanConst (reference: 0.4)              */
+    float    inflow_href;       /* refHeight (reference: 10.0)               */
+    float    vel_zn[3];         /* velZn, fixed value on the Zn face         */
+    int32_t  calc_residual;     /* calResidual                               */
+    int32_t  vel_res_interval;  /* velResidualCheckInterval                  */
+    int32_t  pres_res_interval; /* presResidualCheckInterval                 */
+    float    vel_tol;           /* velTolerance                              */
+    float    pres_tol;          /* presTolerance                             */
+    uint32_t compat_flags;      /* WF_COMPAT_*                               */
+    int32_t  check_finite;      /* != 0: wf_step returns WF_ERR_NONFINITE
+                                   when the new fields hold NaN/Inf          */
+    int32_t  use_graph;         /* != 0 (default): replay the step as a CUDA
+                                   graph when the handle is in steady state  */
+} wf_config;
+
+/* Fills *cfg with the reference's FluidSimConfig defaults
+ * (FluidSimConfig.cs:113-178) and the canonical urban boundary set of
+ * Assets/Code/Config/AijBuilding0.asset (log inlet X0, zero-gradient/p=0
+ * outlet Xn, wall Y0, symmetry Yn/Z0/Zn). */
+void wf_config_default(wf_config* cfg);
+
+/* ---- handle lifecycle ---------------------------------------------------- */
+typedef struct wf_solver wf_solver;
+
+/* Allocates every field and runs the constructor's set-up sequence
+ * (FvmSolverGpu.cs:173-222): all cells fluid, initial fields, face eddy
+ * viscosity 0, boundary planes.  SolidType.Box is not honoured: obstacles
+ * come only through wf_init_flags.  `device` is a CUDA ordinal. */
+int wf_create(const wf_config* cfg, int device, wf_solver** out);
+int wf_destroy(wf_solver* h);
+
+/* ---- IFvmSolver operations ----------------------------------------------- */
+/* InitFlags(int[]): flags[i] > 0.5 marks cell i solid and zeroes its three
+ * velocity buffers; otherwise the cell becomes fluid (CSInitModelFlag,
+ * InitShaderColl.compute:346-364).  n = nx*ny*nz int32 values. */
+int wf_init_flags(wf_solver* h, const int32_t* flags, size_t n);
+/* InitVelPresFields(): constant or log-law interior velocity, p = 0
+ * (CSInitVelPresFields / CSInitLogVelPresFields, InitShaderColl.compute:95-132). */
+int wf_init_vel_pres_fields(wf_solver* h);
+/* SetFixedValueVelBndCond() with RuntimeConfig.windSpeed = wind_speed
+ * (CSSetFixedValueVelBndCond / CSSetLogVelBndCond, InitShaderColl.compute:253-285). */
+int wf_set_fixed_value_vel_bnd_cond(wf_solver* h, float wind_speed);
+/* ChangePhysFieldPos(): re-initialise the fields (FvmSolverGpu.cs:1026-1032). */
+int wf_change_phys_field_pos(wf_solver* h);
+/* Replaces the X0 inlet plane with caller data: ny*nz*3 floats, index
+ * (z*ny + y)*3 + c (perturbed inflow). */
+int wf_set_inflow_plane(wf_solver* h, const float* x0_plane_xyz);
+/* Step() repeated n_steps times, each a complete time step with fixed
+ * iteration counts (no 30 ms time slicing).  *ready (may be NULL) = 1. */
+int wf_step(wf_solver* h, int n_steps, int* ready);
+
+/* ---- field access -------------------------------------------------------- */
+enum { WF_LAYOUT_SOA = 0,   /* 3 planes of N floats: [c][z][y][x]           */
+       WF_LAYOUT_XYZW = 1,  /* N float4 (x,y,z,0), the RenderTexture layout */
+       WF_LAYOUT_XYZ = 2 }; /* N float3 interleaved                         */
+
+/* Current velocity (velFieldLastTime after a step). */
+int wf_get_vel(wf_solver* h, float* out, int layout);
+/* Current pressure (presFieldLastTime). N floats. */
+int wf_get_pres(wf_solver* h, float* out);
+/* Flag field, N int32 (0 fluid, 1 solid). */
+int wf_get_flags(wf_solver* h, int32_t* out);
+/* Velocity, pressure and step counter for an exact resume. vel: 3N floats
+ * (SoA), pres: N floats. */
+int wf_get_state(wf_solver* h, float* vel, float* pres, int64_t* step);
+int wf_set_state(wf_solver* h, const float* vel, const float* pres, int64_t step);
+
+/* Named fields of the reference's field set (MallocTextures,
+ * FvmSolverGpu.cs:263-305) for per-kernel parity checks. */
+enum {
+    WF_FIELD_VEL = 0,                  /* velField            (vector) */
+    WF_FIELD_VEL_LAST_TIME = 1,        /* velFieldLastTime    (vector) */
+    WF_FIELD_VEL_LAST_ITER = 2,        /* velFieldLastIter    (vector) */
+    WF_FIELD_VEL_CORRECT = 3,          /* velCorrectField     (vector) */
+    WF_FIELD_PRES = 4,                 /* presFieldLastTime   (scalar) */
+    WF_FIELD_PRES_CORRECT = 5,         /* presCorrectField    (scalar) */
+    WF_FIELD_PRES_CORRECT_LAST_ITER = 6,/* presCorrectFieldLastIter    */
+    WF_FIELD_D = 7,                    /* DField              (vector) */
+    WF_FIELD_B = 8,                    /* bField              (vector) */
+    WF_FIELD_DP = 9,                   /* DFieldPresCorrect   (scalar) */
+    WF_FIELD_BP = 10,                  /* bFieldPresCorrect   (scalar) */
+    WF_FIELD_AODU = 11,                /* AodUCorrectField    (vector) */
+    WF_FIELD_EDDY_VIS = 12,            /* eddyVisField        (scalar) */
+    WF_FIELD_FACE_EDDY_VIS = 13,       /* faceEddyVisField    (vector, W/S/D faces) */
+    WF_FIELD_BND_X0 = 14,              /* boundary planes (vector):     */
+    WF_FIELD_BND_XN = 15,              /*   X planes ny*nz, index z*ny+y */
+    WF_FIELD_BND_Y0 = 16,              /*   Y planes nx*nz, index z*nx+x */
+    WF_FIELD_BND_YN = 17,              /*   Z planes nx*ny, index y*nx+x */
+    WF_FIELD_BND_Z0 = 18,
+    WF_FIELD_BND_ZN = 19,
+    WF_FIELD_COUNT = 20
+};
+/* Number of cells (or plane points) of a field; vectors carry 3 floats per
+ * point in SoA order. */
+int wf_field_size(const wf_solver* h, int field, size_t* points, int* comps);
+int wf_get_field(wf_solver* h, int field, float* out);
+int wf_set_field(wf_solver* h, int field, const float* in);
+
+/* Device pointers for zero-copy consumers (e.g. torch).  Valid until the
+ * next wf_step / wf_init_* / wf_set_* / wf_destroy. */
+typedef struct wf_device_fields {
+    float*   vel[3];     /* velocity components (SoA planes), N floats each */
+    float*   pres;       /* pressure, N floats                              */
+    uint8_t* flags;      /* N bytes, 0 fluid / 1 solid                      */
+    int64_t  n_cells;
+    void*    stream;     /* the handle's cudaStream_t                       */
+} wf_device_fields;
+int wf_get_device_fields(wf_solver* h, wf_device_fields* out);
+
+/* Residual norms of the last step, as the reference defines them
+ * (FvmSolverGpu.cs:1232-1233,1361-1362): vel = sqrt(sum (D*du)^2 / 3N) of
+ * the last momentum sweep, pres = sqrt(sum (Dp*dp')^2 / N) of the last
+ * pressure sweep; mass = sum over fluid cells of |face-flux divergence| of
+ * the final velocity.  Values are -1 when calc_residual was off. */
+int wf_residuals(wf_solver* h, float* vel, float* pres, float* mass);
+/* Mass imbalance sum |div u| (face-averaged fluxes, BC-aware) of the
+ * current velocity; computed on demand. */
+int wf_mass_imbalance(wf_solver* h, double* out);
+/* Scans velocity and pressure for NaN/Inf: WF_OK or WF_ERR_NONFINITE. */
+int wf_check_finite(wf_solver* h);
+
+/* ---- per-kernel operations (parity checks against the CPU oracle) ------- */
+/* Each runs exactly one reference kernel (or loop) on the handle's current
+ * fields, with the reference's buffer roles and swaps. */
+int wf_op_wallfunc(wf_solver* h);        /* CSCalLogLawWallFunc  WallFunc.compute:128-190 */
+int wf_op_eddy_vis(wf_solver* h);        /* CSCalEddyVis         LES.compute:268-324      */
+int wf_op_les_term(wf_solver* h);        /* CSCalLesDeferCorrectTerm LES.compute:327-687  */
+int wf_op_vel_precompute(wf_solver* h);  /* CSVelPredictPreCompute FvmColl.compute:1292-1859 */
+/* n sweeps of CSVelPredict (FvmColl.compute:1863-2069) with the swap of
+ * FvmSolverGpu.cs:1265 after each and the final swap of :1279. */
+int wf_op_vel_sweeps(wf_solver* h, int n);
+int wf_op_pres_precompute(wf_solver* h); /* CSPresCorrectRhieChowPreCompute FvmColl.compute:2481-2787 */
+/* n sweeps of CSPresCorrectRhieChow (FvmColl.compute:2790-2848), swaps as in
+ * FvmSolverGpu.cs:1401,1415. */
+int wf_op_pres_sweeps(wf_solver* h, int n);
+int wf_op_apply_pres(wf_solver* h);      /* CSApplyPresCorrection FvmColl.compute:2851-2862 */
+int wf_op_normalize(wf_solver* h);       /* CSPresNormalization  FvmColl.compute:2865-2880 (reference value read first) */
+int wf_op_apply_vel(wf_solver* h);       /* CSApplyVelCorrectionDivergenceTheorem FvmColl.compute:2951-3121 */
+int wf_op_zero_pres_correct(wf_solver* h); /* SetPresCorrectFieldtoZero FvmSolverGpu.cs:1545-1554 */
+/* One PisoCorrection() (FvmSolverGpu.cs:1482-1533) with n pressure sweeps. */
+int wf_op_piso(wf_solver* h, int n);
+/* End of step: swap(velLastTime, vel); velLastIter <- velLastTime
+ * (FvmSolverGpu.cs:1103-1118). */
+int wf_op_end_step(wf_solver* h);
+/* Residual kernels (FvmColl.compute:3124-3199) on the current fields. */
+int wf_op_vel_residual(wf_solver* h, float* out);
+int wf_op_pres_residual(wf_solver* h, float* out);
+
+/* ---- diagnostics --------------------------------------------------------- */
+const char* wf_last_error(const wf_solver* h);
+const char* wf_strerror(int status);
+int wf_version(void);   /* WF_ABI_VERSION */
+
+/* Device time of the kernels of the last wf_step call, in milliseconds,
+ * measured with CUDA events on the handle's stream. */
+int wf_last_step_ms(const wf_solver* h, float* ms);
+
+/* Number of kernels this library launched inside wf_step calls since the
+ * handle was created (graph replays count every kernel node). */
+int wf_kernel_launches(const wf_solver* h, int64_t* total);
+
+/* Times `reps` launches of one hot kernel of the step on the handle's
+ * current coefficients, with CUDA events on the handle's stream; when
+ * flush_l2 != 0 a 256 MiB buffer is written before each launch so every
+ * launch starts with a cold L2.  Outputs: mean device time per launch, the
+ * algorithmic bytes of one launch (the reference kernel's compulsory bytes
+ * per cell times the cells and sweeps one launch covers) and the Jacobi
+ * sweeps one launch performs.  The solver state is not modified. */
+enum { WF_KERNEL_PRES_SWEEP = 0, WF_KERNEL_VEL_SWEEP = 1 };
+int wf_time_kernel(wf_solver* h, int kernel, int reps, int flush_l2, float* ms_per_launch,
+                   double* alg_bytes_per_launch, int* sweeps_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WINDFVM_H */

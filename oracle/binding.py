@@ -1,0 +1,162 @@
+"""ctypes binding of libwindfvm_oracle.so (test infrastructure only)."""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, byref, c_double, c_float, c_int, c_int32, c_size_t, c_void_p
+
+import numpy as np
+
+from unitywindsimulation_b200._lib import WfConfig
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwindfvm_oracle.so")
+
+_lib = None
+
+
+def build_oracle(force: bool = False) -> str:
+    args = ["make", "-s", "-C", HERE]
+    if force:
+        args.append("-B")
+    subprocess.run(args, check=True)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build_oracle()
+    lib = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "wfo_create": (c_int, [POINTER(WfConfig), c_int, c_int, POINTER(c_void_p)]),
+        "wfo_destroy": (c_int, [c_void_p]),
+        "wfo_init_flags": (c_int, [c_void_p, POINTER(c_int32), c_size_t]),
+        "wfo_init_vel_pres_fields": (c_int, [c_void_p]),
+        "wfo_set_fixed_value_vel_bnd_cond": (c_int, [c_void_p, c_float]),
+        "wfo_set_inflow_plane": (c_int, [c_void_p, POINTER(c_float)]),
+        "wfo_step": (c_int, [c_void_p, c_int]),
+        "wfo_field_size": (c_int, [c_void_p, c_int, POINTER(c_size_t), POINTER(c_int)]),
+        "wfo_get_field": (c_int, [c_void_p, c_int, POINTER(c_double)]),
+        "wfo_set_field": (c_int, [c_void_p, c_int, POINTER(c_double)]),
+        "wfo_get_flags": (c_int, [c_void_p, POINTER(c_int32)]),
+        "wfo_op_vel_sweeps": (c_int, [c_void_p, c_int]),
+        "wfo_op_pres_sweeps": (c_int, [c_void_p, c_int]),
+        "wfo_op_piso": (c_int, [c_void_p, c_int]),
+        "wfo_op_vel_residual": (c_int, [c_void_p, POINTER(c_double)]),
+        "wfo_op_pres_residual": (c_int, [c_void_p, POINTER(c_double)]),
+        "wfo_residuals": (c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
+        "wfo_mass_imbalance": (c_int, [c_void_p, POINTER(c_double)]),
+        "wfo_log_law_wall_func": (c_double, [c_double, c_double, c_double, c_double, c_int]),
+    }
+    for op in ["wallfunc", "eddy_vis", "les_term", "vel_precompute", "pres_precompute", "apply_pres",
+               "normalize", "apply_vel", "zero_pres_correct", "end_step"]:
+        sig[f"wfo_op_{op}"] = (c_int, [c_void_p])
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def log_law_wall_func(uP: float, dx: float, nu: float, den: float = 1.0, precision: int = 64) -> float:
+    return load().wfo_log_law_wall_func(uP, dx, nu, den, precision)
+
+
+class OracleSolver:
+    """CPU restatement of the step with the same operations as FvmSolverCuda."""
+
+    def __init__(self, cfg: WfConfig, precision: int = 64, threads: int = 0):
+        self._lib = load()
+        self.cfg = cfg.copy()
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        self.n_cells = cfg.nx * cfg.ny * cfg.nz
+        h = c_void_p()
+        st = self._lib.wfo_create(byref(self.cfg), precision, threads, byref(h))
+        if st != 0:
+            raise RuntimeError(f"wfo_create failed with status {st}")
+        self._h = h
+        self.wind_speed = cfg.wind_speed
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.wfo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, st):
+        if st != 0:
+            raise RuntimeError(f"oracle call failed with status {st}")
+
+    def Step(self, n_steps: int = 1) -> bool:
+        self._ok(self._lib.wfo_step(self._h, int(n_steps)))
+        return True
+
+    def InitFlags(self, flags):
+        f = np.ascontiguousarray(np.asarray(flags, dtype=np.int32).reshape(-1))
+        self._ok(self._lib.wfo_init_flags(self._h, f.ctypes.data_as(POINTER(c_int32)), f.size))
+
+    def InitVelPresFields(self):
+        self._ok(self._lib.wfo_init_vel_pres_fields(self._h))
+
+    def SetFixedValueVelBndCond(self, wind_speed=None):
+        if wind_speed is not None:
+            self.wind_speed = float(wind_speed)
+        self._ok(self._lib.wfo_set_fixed_value_vel_bnd_cond(self._h, c_float(self.wind_speed)))
+
+    def set_inflow_plane(self, plane_xyz):
+        a = np.ascontiguousarray(plane_xyz, dtype=np.float32).reshape(-1)
+        self._ok(self._lib.wfo_set_inflow_plane(self._h, a.ctypes.data_as(POINTER(c_float))))
+
+    def GetFlagField(self):
+        out = np.empty(self.n_cells, dtype=np.int32)
+        self._ok(self._lib.wfo_get_flags(self._h, out.ctypes.data_as(POINTER(c_int32))))
+        return out.reshape(self.shape)
+
+    def field_size(self, field):
+        pts, comps = c_size_t(0), c_int(0)
+        self._ok(self._lib.wfo_field_size(self._h, field, byref(pts), byref(comps)))
+        return pts.value, comps.value
+
+    def get_field(self, field) -> np.ndarray:
+        pts, comps = self.field_size(field)
+        out = np.empty(pts * comps, dtype=np.float64)
+        self._ok(self._lib.wfo_get_field(self._h, field, out.ctypes.data_as(POINTER(c_double))))
+        return out.reshape((comps, pts)) if comps > 1 else out
+
+    def set_field(self, field, data):
+        a = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)
+        self._ok(self._lib.wfo_set_field(self._h, field, a.ctypes.data_as(POINTER(c_double))))
+
+    def GetVelField(self):
+        return self.get_field(1).reshape((3,) + self.shape)
+
+    def GetPresField(self):
+        return self.get_field(4).reshape(self.shape)
+
+    def op(self, name, *args):
+        self._ok(getattr(self._lib, f"wfo_op_{name}")(self._h, *[int(a) for a in args]))
+
+    def op_residual(self, which) -> float:
+        out = c_double(0)
+        self._ok(getattr(self._lib, f"wfo_op_{which}_residual")(self._h, byref(out)))
+        return out.value
+
+    def residuals(self):
+        v, p = c_double(0), c_double(0)
+        self._ok(self._lib.wfo_residuals(self._h, byref(v), byref(p)))
+        return v.value, p.value
+
+    def mass_imbalance(self) -> float:
+        m = c_double(0)
+        self._ok(self._lib.wfo_mass_imbalance(self._h, byref(m)))
+        return m.value

@@ -1,0 +1,287 @@
+"""Seeded case generator: obstacle flags, inflow and solver settings.
+
+Stands in for the reference's voxelizer (BuildingVoxelizer.cs:355-413), which
+ray-casts Unity meshes into an ``int[]`` flag array indexed
+``z*nx*ny + y*nx + x`` with 1 = solid, keeps a 10-cell building-free margin
+near the x/z boundaries (:379) and rotates the domain by the wind direction
+(:364).  Here buildings are seeded axis-aligned or rotated boxes rasterised at
+cell centres into the same layout.
+
+Axis convention: the reference (and this library) uses y vertical; workload
+descriptions written as nx x ny x nz with z vertical map to
+(nx, ny_ref, nz_ref) = (nx, nz, ny).
+
+Workloads (synthetic, seeded):
+  plain_cube      64 x 32(up) x 48, one 8-cell cube, log inflow u*=0.5 z0=0.1
+  urban_block     256 x 96(up) x 192, 48 buildings on a street lattice,
+                  u*=0.6 z0=0.3 with 5 % Gaussian inlet perturbation
+  batch_directions 16 uneven grids 96..192 x 48..80(up) x 96..160, 8-32
+                  buildings each, wind rotated by k * 22.5 degrees
+  adjoint_street  128 x 64(up) x 96, 12 buildings with continuous heights
+  adjoint_batch   8 directions x 256 x 96(up) x 256, 64 buildings
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import _lib
+from .config import default_config
+
+MARGIN = 10  # building-free cells next to the x and z boundaries (BuildingVoxelizer.cs:379)
+KAPPA = 0.41
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    cfg: object                       # WfConfig
+    flags: np.ndarray                 # int32, (nz, ny, nx)
+    inlet: np.ndarray | None = None   # (nz, ny, 3) float32 X0 plane, None = built-in profile
+    steps: int = 1
+    seed: int | None = None
+    buildings: list = dataclasses.field(default_factory=list)  # (x0, x1, z0, z1, height[, angle])
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.cfg.nx) * int(self.cfg.ny) * int(self.cfg.nz)
+
+
+def log_profile(y_phys, ustar: float, z0: float, kappa: float = KAPPA):
+    return ustar / kappa * np.log((np.asarray(y_phys, dtype=np.float64) + z0) / z0)
+
+
+def inlet_plane(ny: int, nz: int, dx: float, ustar: float, z0: float, kappa: float = KAPPA,
+                perturb: float = 0.0, rng: np.random.Generator | None = None) -> np.ndarray:
+    """X0 plane (nz, ny, 3): log profile at cell centres (y + 0.5) dx
+    (CSSetLogVelBndCond, InitShaderColl.compute:273-285), optionally with a
+    multiplicative Gaussian perturbation per inlet face."""
+    y = (np.arange(ny, dtype=np.float32) + np.float32(0.5)) * np.float32(dx)
+    u = log_profile(y, ustar, z0, kappa).astype(np.float32)
+    plane = np.zeros((nz, ny, 3), dtype=np.float32)
+    plane[:, :, 0] = u[None, :]
+    if perturb:
+        rng = rng or np.random.default_rng(0)
+        plane[:, :, 0] *= (1.0 + perturb * rng.standard_normal((nz, ny))).astype(np.float32)
+    return plane
+
+
+def cfl_dt(u_max: float, dx: float, cfl: float = 0.5) -> float:
+    return float(cfl * dx / u_max)
+
+
+def remove_isolated_fluid(flags: np.ndarray) -> np.ndarray:
+    """Marks solid every fluid cell with no fluid neighbour inside the domain:
+    such a cell has a zero pressure diagonal (the reference divides by it,
+    FvmColl.compute:2847, PisoColl.compute:255)."""
+    f = flags.copy()
+    while True:
+        fluid = f == 0
+        cnt = np.zeros(f.shape, dtype=np.int32)
+        for ax in range(3):
+            for sh in (1, -1):
+                r = np.roll(fluid, sh, axis=ax)
+                idx = [slice(None)] * 3
+                idx[ax] = 0 if sh == 1 else -1
+                r[tuple(idx)] = False
+                cnt += r
+        iso = fluid & (cnt == 0)
+        if not iso.any():
+            return f
+        f[iso] = 1
+
+
+def isolated_fluid_count(flags: np.ndarray) -> int:
+    return int(((flags == 0) & (remove_isolated_fluid(flags) == 1)).sum())
+
+
+def rasterise_boxes(nx: int, ny: int, nz: int, boxes, angle_deg: float = 0.0, margin: int = MARGIN) -> np.ndarray:
+    """Boxes (x0, x1, z0, z1, h) in cells, rotated by angle_deg about the
+    domain centre in the x-z plane, rasterised at cell centres.  Cells within
+    `margin` of the x/z boundaries stay fluid.  Returns int32 (nz, ny, nx)."""
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    xs = np.arange(nx) + 0.5
+    zs = np.arange(nz) + 0.5
+    X, Z = np.meshgrid(xs, zs)  # (nz, nx)
+    cx, cz = nx / 2.0, nz / 2.0
+    th = math.radians(angle_deg)
+    c, s = math.cos(th), math.sin(th)
+    # inverse-rotate cell centres into the building frame
+    Xr = cx + (X - cx) * c + (Z - cz) * s
+    Zr = cz - (X - cx) * s + (Z - cz) * c
+    inside_margin = (X > margin) & (X < nx - margin) & (Z > margin) & (Z < nz - margin)
+    for b in boxes:
+        x0, x1, z0, z1, h = b[:5]
+        h = int(round(h))
+        m = (Xr >= x0) & (Xr < x1) & (Zr >= z0) & (Zr < z1) & inside_margin
+        if h <= 0 or not m.any():
+            continue
+        hh = min(h, ny - 1)
+        flags[:, :hh, :][np.broadcast_to(m[:, None, :], (nz, hh, nx))] = 1
+    return flags
+
+
+def street_lattice_buildings(rng: np.random.Generator, nx: int, nz: int, count: int, fp_lo: int, fp_hi: int,
+                             h_lo: float, h_hi: float, block: int = 16, street: int = 2, margin: int = MARGIN,
+                             integer_heights: bool = True):
+    """`count` buildings placed without overlap, one per lot of a street
+    lattice with `block`-cell blocks separated by `street`-cell streets.
+    Footprints are uniform in [fp_lo, fp_hi] cells per side, heights uniform
+    in [h_lo, h_hi]."""
+    pitch = block + street
+    lots_x = (nx - 2 * margin - street) // pitch
+    lots_z = (nz - 2 * margin - street) // pitch
+    lots = [(i, j) for i in range(lots_x) for j in range(lots_z)]
+    if count > len(lots):
+        raise ValueError(f"{count} buildings do not fit {len(lots)} lots")
+    pick = rng.choice(len(lots), size=count, replace=False)
+    out = []
+    for k in pick:
+        i, j = lots[k]
+        wx = int(rng.integers(fp_lo, fp_hi + 1))
+        wz = int(rng.integers(fp_lo, fp_hi + 1))
+        bx = margin + street + i * pitch + int(rng.integers(0, block - wx + 1))
+        bz = margin + street + j * pitch + int(rng.integers(0, block - wz + 1))
+        h = int(rng.integers(int(h_lo), int(h_hi) + 1)) if integer_heights else float(rng.uniform(h_lo, h_hi))
+        out.append((bx, bx + wx, bz, bz + wz, h))
+    return out
+
+
+def _les_piso_cfg(nx, ny, nz, dx, dt, ustar, z0, cs, nv, np_, nc=2):
+    return default_config(
+        nx=nx, ny=ny, nz=nz, dx=dx, dt=dt, mu=1.5e-5, den=1.0,
+        solver_type=_lib.SOLVER_PISO, piso_correctors=nc,
+        turbulence=_lib.TURB_SMAGORINSKY, cs=cs,
+        vel_iters=nv, pres_iters=np_,
+        inflow_type=_lib.INFLOW_LOG, inflow_ustar=ustar, inflow_z0=z0, inflow_kappa=KAPPA,
+        wind_speed=0.0,
+    )
+
+
+def plain_cube(nv: int = 50, np_: int = 30, steps: int = 100) -> Case:
+    """64 x 32(up) x 48 cells of 0.5 m, one 8-cell cube spanning x 12..20,
+    y 0..8, z 20..28; log inflow u* = 0.5, z0 = 0.1; Cs = 0.1; CFL 0.5."""
+    nx, ny, nz, dx = 64, 32, 48, 0.5
+    ustar, z0 = 0.5, 0.1
+    umax = float(log_profile((ny - 0.5) * dx, ustar, z0))
+    cfg = _les_piso_cfg(nx, ny, nz, dx, cfl_dt(umax, dx), ustar, z0, 0.1, nv, np_)
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    flags[20:28, 0:8, 12:20] = 1
+    return Case("plain_cube", cfg, flags, None, steps, None, [(12, 20, 20, 28, 8)])
+
+
+def urban_block(seed: int = 2, nv: int = 50, np_: int = 40, steps: int = 500) -> Case:
+    """256 x 96(up) x 192 cells of 0.5 m, 48 buildings (footprints 6-16 cells,
+    heights 4-40 cells) on a 16-cell block lattice; inflow u* = 0.6, z0 = 0.3
+    with a 5 % multiplicative Gaussian perturbation per inlet face; Cs = 0.12."""
+    nx, ny, nz, dx = 256, 96, 192, 0.5
+    ustar, z0 = 0.6, 0.3
+    rng = np.random.default_rng(seed)
+    blds = street_lattice_buildings(rng, nx, nz, 48, 6, 16, 4, 40)
+    flags = remove_isolated_fluid(rasterise_boxes(nx, ny, nz, blds))
+    inlet = inlet_plane(ny, nz, dx, ustar, z0, perturb=0.05, rng=rng)
+    dt = cfl_dt(float(inlet[:, :, 0].max()), dx)
+    cfg = _les_piso_cfg(nx, ny, nz, dx, dt, ustar, z0, 0.12, nv, np_)
+    return Case("urban_block", cfg, flags, inlet, steps, seed, blds)
+
+
+def batch_directions(seed: int = 3, n_cases: int = 16, nv: int = 50, np_: int = 30, steps: int = 300):
+    """16 cases of uneven size (nx 96..192, ny 48..80 up, nz 96..160, multiples
+    of 8), 8-32 buildings (heights 4-30 cells) each, footprints rotated by
+    k * 22.5 degrees before rasterising (the domain stays aligned with the
+    flow, the buildings rotate)."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for k in range(n_cases):
+        nx = int(rng.integers(12, 25)) * 8
+        ny = int(rng.integers(6, 11)) * 8
+        nz = int(rng.integers(12, 21)) * 8
+        dx = 0.5
+        nb = int(rng.integers(8, 33))
+        lots = ((nx - 2 * MARGIN - 2) // 18) * ((nz - 2 * MARGIN - 2) // 18)
+        blds = street_lattice_buildings(rng, nx, nz, min(nb, lots), 6, 16, 4, 30)
+        angle = 22.5 * (k % 16)
+        flags = remove_isolated_fluid(rasterise_boxes(nx, ny, nz, blds, angle_deg=angle))
+        ustar, z0 = 0.5, 0.1
+        umax = float(log_profile((ny - 0.5) * dx, ustar, z0))
+        cfg = _les_piso_cfg(nx, ny, nz, dx, cfl_dt(umax, dx), ustar, z0, 0.1, nv, np_)
+        cases.append(Case(f"batch_{k:02d}_{angle:g}deg", cfg, flags, None, steps, seed,
+                          [b + (angle,) for b in blds]))
+    return cases
+
+
+def adjoint_street(seed: int = 4, nv: int = 50, np_: int = 30, steps: int = 200) -> Case:
+    """128 x 64(up) x 96 cells, 12 buildings with continuous heights in
+    [4, 30] cells (the rasterised flags round them)."""
+    nx, ny, nz, dx = 128, 64, 96, 0.5
+    rng = np.random.default_rng(seed)
+    blds = street_lattice_buildings(rng, nx, nz, 12, 6, 16, 4, 30, integer_heights=False)
+    flags = remove_isolated_fluid(rasterise_boxes(nx, ny, nz, blds))
+    ustar, z0 = 0.5, 0.1
+    umax = float(log_profile((ny - 0.5) * dx, ustar, z0))
+    cfg = _les_piso_cfg(nx, ny, nz, dx, cfl_dt(umax, dx), ustar, z0, 0.1, nv, np_)
+    return Case("adjoint_street", cfg, flags, None, steps, seed, blds)
+
+
+def aij_building(nv: int = 100, np_: int = 1000, steps: int = 1) -> Case:
+    """The reference's validation case, Assets/Code/Config/AijBuilding0.asset:
+    80 x 40 x 40 cells of 1 m, dt 0.04, mu 1.5e-5, SIMPLE, Smagorinsky 0.18,
+    log inflow at 10 m/s with the reference's hard-coded kappa 0.4, z0 1,
+    href 10, and the hard-coded box of CSInitBoxFlag (x 20..24, y 0..8,
+    z 18..22, InitShaderColl.compute:320)."""
+    nx, ny, nz = 80, 40, 40
+    cfg = default_config(nx=nx, ny=ny, nz=nz, dx=1.0, dt=0.04, mu=1.5e-5, den=1.0,
+                         solver_type=_lib.SOLVER_SIMPLE, turbulence=_lib.TURB_SMAGORINSKY, cs=0.18,
+                         inflow_type=_lib.INFLOW_LOG, wind_speed=10.0, vel_iters=nv, pres_iters=np_)
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    flags[18:22, 0:8, 20:24] = 1
+    return Case("aij_building", cfg, flags, None, steps, None, [(20, 24, 18, 22, 8)])
+
+
+def small_case(nx=24, ny=12, nz=16, piso=True, les=True, seed=0, nv=8, np_=12, buildings=2,
+               inflow_log=True, compat=0) -> Case:
+    """Small seeded case for parity tests (oracle finishes in well under a second)."""
+    rng = np.random.default_rng(seed)
+    dx = 0.5
+    cfg = default_config(nx=nx, ny=ny, nz=nz, dx=dx, mu=1.5e-5, den=1.0,
+                         solver_type=_lib.SOLVER_PISO if piso else _lib.SOLVER_SIMPLE, piso_correctors=2,
+                         turbulence=_lib.TURB_SMAGORINSKY if les else _lib.TURB_NONE, cs=0.12,
+                         vel_iters=nv, pres_iters=np_, compat_flags=compat)
+    if inflow_log:
+        cfg.inflow_type = _lib.INFLOW_LOG
+        cfg.inflow_ustar, cfg.inflow_z0, cfg.inflow_kappa = 0.5, 0.1, KAPPA
+        umax = float(log_profile((ny - 0.5) * dx, 0.5, 0.1))
+    else:
+        cfg.inflow_type = _lib.INFLOW_CONSTANT
+        cfg.wind_speed = 3.0
+        umax = 3.0
+    cfg.dt = cfl_dt(umax, dx)
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    blds = []
+    for _ in range(buildings):
+        wx, wz = int(rng.integers(2, 5)), int(rng.integers(2, 5))
+        x0 = int(rng.integers(4, max(5, nx - 6 - wx)))
+        z0_ = int(rng.integers(3, max(4, nz - 3 - wz)))
+        h = int(rng.integers(2, max(3, ny // 2)))
+        flags[z0_:z0_ + wz, 0:h, x0:x0 + wx] = 1
+        blds.append((x0, x0 + wx, z0_, z0_ + wz, h))
+    flags = remove_isolated_fluid(flags)
+    return Case(f"small_{nx}x{ny}x{nz}_s{seed}", cfg, flags, None, 1, seed, blds)
+
+
+def apply_case(solver, case: Case) -> None:
+    """Reference set-up order: flags after the fields (FvmSolverController.cs:
+    368-375), then the inlet plane."""
+    solver.InitFlags(case.flags)
+    if case.inlet is not None:
+        solver.set_inflow_plane(case.inlet)
+
+
+WORKLOADS = {
+    "plain_cube": plain_cube,
+    "urban_block": urban_block,
+    "adjoint_street": adjoint_street,
+    "aij_building": aij_building,
+}

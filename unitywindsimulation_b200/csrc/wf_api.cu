@@ -1,0 +1,921 @@
+// wf_api.cu - host implementation of the windfvm C ABI (include/windfvm.h).
+//
+// Sequencing follows FvmSolverGpu (Assets/Code/FvmSolver/FvmSolverGpu.cs of
+// puppy2333/UnityWindSimulation): constructor :173-222, Step :1050-1121,
+// VelPredict :1238-1282, PresCorrect :1367-1439, ApplyVelCorrection
+// :1441-1452, PisoCorrection :1482-1533.  Buffer roles are rotated exactly
+// where the C# driver swaps its textures; the two copies it makes per step
+// (end-of-step velocity copy and zeroing the pressure correction) are
+// replaced by role flags (iter_alias, pc_zero) that the kernels honour.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "wf_kernels.cuh"
+#include "wf_solver.cuh"
+#include "wf_sweeps.cuh"
+
+using wf::Params;
+
+namespace {
+
+#define WF_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                \
+            return e_ == cudaErrorMemoryAllocation ? WF_ERR_OOM : WF_ERR_CUDA;          \
+        }                                                                               \
+    } while (0)
+
+#define WF_CHECK_LAUNCH()                                                               \
+    do {                                                                                \
+        cudaError_t e_ = cudaGetLastError();                                            \
+        if (e_ != cudaSuccess) {                                                        \
+            h->err = std::string("kernel launch: ") + cudaGetErrorString(e_);           \
+            return WF_ERR_CUDA;                                                         \
+        }                                                                               \
+    } while (0)
+
+#define WF_TRY(expr)                \
+    do {                            \
+        int s_ = (expr);            \
+        if (s_ != WF_OK) return s_; \
+    } while (0)
+
+int set_err(wf_solver* h, int code, const char* msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+bool any_fixed_pres(const wf_config& c) {
+    for (int f = 0; f < 6; ++f)
+        if (c.pres_bc[f] == WF_BND_FIXED_VALUE) return true;
+    return false;
+}
+
+const char* validate(const wf_config* c) {
+    if (!c) return "config is NULL";
+    if (c->struct_size != sizeof(wf_config)) return "config struct_size does not match this library";
+    if (c->nx < 3 || c->ny < 3 || c->nz < 3) return "grid must be at least 3 cells on every axis";
+    const double n = double(c->nx) * c->ny * c->nz;
+    if (n * 4.0 >= 2147483647.0) return "grid too large (4*nx*ny*nz must fit in int32)";
+    if (!(c->dx > 0.f) || !std::isfinite(c->dx)) return "dx must be > 0";
+    if (!(c->dt > 0.f) || !std::isfinite(c->dt)) return "dt must be > 0";
+    if (!(c->den > 0.f)) return "den must be > 0";
+    if (!(c->mu >= 0.f)) return "mu must be >= 0";
+    for (int f = 0; f < 6; ++f) {
+        if (c->vel_bc[f] < 0 || c->vel_bc[f] > 2) return "vel_bc out of range";
+        if (c->pres_bc[f] < 0 || c->pres_bc[f] > 2) return "pres_bc out of range";
+    }
+    if (c->solver_type != WF_SOLVER_SIMPLE && c->solver_type != WF_SOLVER_PISO) return "solver_type out of range";
+    if (c->turbulence != WF_TURB_NONE && c->turbulence != WF_TURB_SMAGORINSKY) return "turbulence out of range";
+    if (c->inflow_type != WF_INFLOW_CONSTANT && c->inflow_type != WF_INFLOW_LOG) return "inflow_type out of range";
+    if (c->vel_iters < 0 || c->pres_iters < 0 || c->piso_correctors < 0) return "iteration counts must be >= 0";
+    if (c->inflow_type == WF_INFLOW_LOG) {
+        if (!(c->inflow_z0 > 0.f) || !(c->inflow_kappa > 0.f)) return "log inflow needs z0 > 0 and kappa > 0";
+        if (!(c->inflow_ustar > 0.f) && !(c->inflow_href > 0.f)) return "log inflow needs ustar > 0 or href > 0";
+    }
+    if (c->calc_residual && (c->vel_res_interval <= 0 || c->pres_res_interval <= 0))
+        return "residual intervals must be > 0 when calc_residual is set";
+    if (c->compat_flags & ~(WF_COMPAT_RFLOAT_FACE_EDDY_VIS | WF_COMPAT_INIT_PROFILE_CELL_CENTRE |
+                            WF_COMPAT_PISO_CONSISTENT))
+        return "unknown compat flag";
+    return nullptr;
+}
+
+float fric_vel(const wf_solver* h) {
+    const wf_config& c = h->cfg;
+    if (c.inflow_ustar > 0.f) return c.inflow_ustar;
+    return c.inflow_kappa * h->wind / logf((c.inflow_href + c.inflow_z0) / c.inflow_z0);
+}
+
+int alloc(wf_solver* h, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return WF_ERR_OOM;
+    }
+    e = cudaMemsetAsync(*p, 0, bytes, h->st);
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaMemset: ") + cudaGetErrorString(e);
+        return WF_ERR_CUDA;
+    }
+    return WF_OK;
+}
+
+void free_all(wf_solver* h) {
+    for (auto& kv : h->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    h->graphs.clear();
+    void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
+                    h->pcb[0], h->pcb[1], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->part, h->dsum, h->dref,
+                    h->dbad, h->stage, h->bnd[0]};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->hsum) cudaFreeHost(h->hsum);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->st) cudaStreamDestroy(h->st);
+}
+
+int sync(wf_solver* h) {
+    WF_CUDA(cudaStreamSynchronize(h->st));
+    return WF_OK;
+}
+
+// Makes velFieldLastIter a real buffer again (copy of velFieldLastTime).
+int materialize_iter(wf_solver* h) {
+    if (!h->iter_alias) return WF_OK;
+    WF_CUDA(cudaMemcpyAsync(h->vb[h->iI], h->vb[h->iT], 3 * sizeof(float) * h->P.N, cudaMemcpyDeviceToDevice, h->st));
+    h->iter_alias = false;
+    return WF_OK;
+}
+// Makes both pressure-correction buffers real zeros again.
+int materialize_pc(wf_solver* h) {
+    if (!h->pc_zero) return WF_OK;
+    WF_CUDA(cudaMemsetAsync(h->pcb[0], 0, sizeof(float) * h->P.N, h->st));
+    WF_CUDA(cudaMemsetAsync(h->pcb[1], 0, sizeof(float) * h->P.N, h->st));
+    h->pc_zero = false;
+    return WF_OK;
+}
+
+// ---------------------------------------------------------- stage bodies
+// Each function enqueues work on h->st only (no host sync) unless residuals
+// are requested, so a whole step can be captured into a CUDA graph.
+
+int do_les(wf_solver* h) {
+    const Params& P = h->P;
+    const float* uT = h->vb[h->iT];
+    wf::launch_wallfunc(P, h->st, h->fl, uT, h->face);
+    wf::launch_eddy_vis(P, h->B, h->st, h->fl, uT, h->eddy);
+    wf::launch_les_term(P, h->B, h->st, h->fl, uT, h->eddy, h->face, h->bv);
+    WF_CHECK_LAUNCH();
+    return WF_OK;
+}
+
+int do_vel_precompute(wf_solver* h) {
+    wf::launch_vel_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->pr, h->eddy, h->face,
+                              h->P.les ? h->bv : nullptr, h->Dv, h->bv);
+    WF_CHECK_LAUNCH();
+    return WF_OK;
+}
+
+int read_residual(wf_solver* h, double* out) {
+    WF_CUDA(cudaMemcpyAsync(h->hsum, h->dsum, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    WF_TRY(sync(h));
+    *out = h->hsum[0];
+    return WF_OK;
+}
+
+// VelPredict loop (FvmSolverGpu.cs:1244-1279) with n sweeps.
+int do_vel_sweeps(wf_solver* h, int n, bool allow_fast) {
+    const Params& P = h->P;
+    const bool resid = h->cfg.calc_residual != 0;
+    int k = 0;
+    if (allow_fast && h->fast && !resid && n > 0) {
+        // Multi-sweep path: same buffer roles, several sweeps per launch.
+        WF_TRY(wf::vel_sweeps_fast(h, n));
+        return WF_OK;
+    }
+    for (; k < n; ++k) {
+        const float* src = h->iter_alias ? h->vb[h->iT] : h->vb[h->iI];
+        wf::launch_vel_sweep(P, h->st, h->fl, src, h->vb[h->iT], h->eddy, h->face, h->Dv, h->bv, h->vb[h->iF]);
+        WF_CHECK_LAUNCH();
+        if (resid && k % h->cfg.vel_res_interval == 0) {
+            wf::launch_vel_residual(P, h->st, h->Dv, h->vb[h->iF], src, h->part, h->dsum);
+            double s = 0.0;
+            WF_TRY(read_residual(h, &s));
+            h->res_vel = (float)std::sqrt(s / (3.0 * P.N));
+            if (h->res_vel < h->cfg.vel_tol) break;
+        }
+        std::swap(h->iI, h->iF);
+        h->iter_alias = false;
+    }
+    std::swap(h->iI, h->iF);
+    if (k == n && n == 0) {
+        // zero sweeps: the two swaps cancel, nothing else changes
+    }
+    return WF_OK;
+}
+
+int do_pres_precompute(wf_solver* h) {
+    wf::launch_pres_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iF], h->pr, h->Dv, h->Dp, h->bp);
+    WF_CHECK_LAUNCH();
+    return WF_OK;
+}
+
+// PresCorrect loop (FvmSolverGpu.cs:1372-1415) with n sweeps.
+int do_pres_sweeps(wf_solver* h, int n, bool allow_fast) {
+    const Params& P = h->P;
+    const bool resid = h->cfg.calc_residual != 0;
+    if (allow_fast && h->fast && !resid && n > 0) {
+        WF_TRY(wf::pres_sweeps_fast(h, n, /*piso=*/false));
+        return WF_OK;
+    }
+    for (int k = 0; k < n; ++k) {
+        const float* src = h->pc_zero ? nullptr : h->pcb[h->iPCL];
+        wf::launch_pres_sweep(P, h->st, h->fl, src, h->Dv, h->Dp, h->bp, h->pcb[h->iPC]);
+        WF_CHECK_LAUNCH();
+        h->pc_zero = false;
+        if (resid && k % h->cfg.pres_res_interval == 0) {
+            wf::launch_pres_residual(P, h->st, h->Dp, h->pcb[h->iPC], src, h->part, h->dsum);
+            double s = 0.0;
+            WF_TRY(read_residual(h, &s));
+            h->res_pres = (float)std::sqrt(s / double(P.N));
+            if (h->res_pres < h->cfg.pres_tol) break;
+        }
+        std::swap(h->iPCL, h->iPC);
+    }
+    std::swap(h->iPCL, h->iPC);
+    return WF_OK;
+}
+
+const float* pc_cur(const wf_solver* h) { return h->pc_zero ? nullptr : h->pcb[h->iPC]; }
+
+int do_apply_pres(wf_solver* h) {
+    wf::launch_apply_pres(h->P, h->st, h->fl, pc_cur(h), h->pr);
+    WF_CHECK_LAUNCH();
+    return WF_OK;
+}
+int do_normalize(wf_solver* h) {
+    wf::launch_normalize(h->P, h->st, h->fl, h->pr, h->dref);
+    WF_CHECK_LAUNCH();
+    return WF_OK;
+}
+int do_apply_vel(wf_solver* h) {
+    wf::launch_apply_vel(h->P, h->st, h->fl, pc_cur(h), h->Dv, h->uc, h->vb[h->iF]);
+    WF_CHECK_LAUNCH();
+    return WF_OK;
+}
+
+// PisoCorrection (FvmSolverGpu.cs:1482-1533) with n pressure sweeps; p'
+// starts from the zero state.
+int do_piso(wf_solver* h, int n, bool allow_fast) {
+    const Params& P = h->P;
+    wf::launch_piso_aodu(P, h->st, h->fl, h->uc, h->vb[h->iT], h->eddy, h->face, h->aodu);
+    WF_CHECK_LAUNCH();
+    if (allow_fast && h->fast && n > 0) {
+        WF_TRY(wf::pres_sweeps_fast(h, n, /*piso=*/true));
+    } else {
+        for (int k = 0; k < n; ++k) {
+            const float* src = h->pc_zero ? nullptr : h->pcb[h->iPCL];
+            wf::launch_piso_pres_sweep(P, h->st, h->fl, src, h->Dv, h->aodu, h->pcb[h->iPC]);
+            WF_CHECK_LAUNCH();
+            h->pc_zero = false;
+            std::swap(h->iPCL, h->iPC);
+        }
+        std::swap(h->iPCL, h->iPC);
+    }
+    wf::launch_apply_pres(P, h->st, h->fl, pc_cur(h), h->pr);
+    const float* pc = pc_cur(h);
+    if (pc) {
+        wf::launch_piso_vel(P, h->st, h->fl, pc, h->Dv, h->aodu, h->uc, h->vb[h->iF]);
+    } else {
+        // p'' == 0: PisoVelCorrection with a zero field still applies -D^-1 AodU
+        WF_TRY(materialize_pc(h));
+        wf::launch_piso_vel(P, h->st, h->fl, h->pcb[h->iPC], h->Dv, h->aodu, h->uc, h->vb[h->iF]);
+    }
+    WF_CHECK_LAUNCH();
+    h->pc_zero = true;  // SetPresCorrectFieldtoZero (:1532)
+    return WF_OK;
+}
+
+int do_end_step(wf_solver* h) {
+    std::swap(h->iT, h->iF);
+    h->iter_alias = true;  // CopyVelField(velFieldLastIter <- velFieldLastTime)
+    h->step += 1;
+    return WF_OK;
+}
+
+// One complete Step() (FvmSolverGpu.cs:1050-1121) with fixed counts.
+int enqueue_step(wf_solver* h) {
+    const wf_config& c = h->cfg;
+    if (h->P.les) WF_TRY(do_les(h));
+    WF_TRY(do_vel_precompute(h));
+    WF_TRY(do_vel_sweeps(h, c.vel_iters, true));
+    WF_TRY(do_pres_precompute(h));
+    WF_TRY(do_pres_sweeps(h, c.pres_iters, true));
+    WF_TRY(do_apply_pres(h));
+    if (!any_fixed_pres(c)) WF_TRY(do_normalize(h));
+    WF_TRY(do_apply_vel(h));
+    h->pc_zero = true;  // SetPresCorrectFieldtoZero (:1088)
+    if (c.solver_type == WF_SOLVER_PISO)
+        for (int n = 0; n < c.piso_correctors; ++n) WF_TRY(do_piso(h, c.pres_iters, true));
+    return do_end_step(h);
+}
+
+wf_solver::RoleKey role_key(const wf_solver* h) { return {h->iT, h->iF, h->iI, h->iPC, h->iPCL}; }
+void set_roles(wf_solver* h, const wf_solver::RoleKey& k) {
+    h->iT = std::get<0>(k);
+    h->iF = std::get<1>(k);
+    h->iI = std::get<2>(k);
+    h->iPC = std::get<3>(k);
+    h->iPCL = std::get<4>(k);
+}
+
+// Runs one step, replaying a cached CUDA graph when the handle is in its
+// steady state (iter_alias and pc_zero set, no residual reads).
+int run_step(wf_solver* h) {
+    const bool graphable = h->cfg.use_graph && !h->cfg.calc_residual && h->iter_alias && h->pc_zero;
+    if (!graphable) {
+        const long long l0 = wf::g_launches;
+        const int s = enqueue_step(h);
+        h->launches += wf::g_launches - l0;
+        return s;
+    }
+    const auto key = role_key(h);
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        WF_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        const int64_t step0 = h->step;
+        const long long l0 = wf::g_launches;
+        int s = enqueue_step(h);
+        const long long nk = wf::g_launches - l0;
+        cudaError_t e = cudaStreamEndCapture(h->st, &g);
+        if (s != WF_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (e != cudaSuccess) {
+            h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+            return WF_ERR_CUDA;
+        }
+        wf_solver::GraphEntry ent;
+        ent.after = role_key(h);
+        ent.kernels = nk;
+        e = cudaGraphInstantiate(&ent.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+            return WF_ERR_CUDA;
+        }
+        it = h->graphs.emplace(key, ent).first;
+        // capture only recorded the work: restore and replay it
+        set_roles(h, key);
+        h->iter_alias = true;
+        h->pc_zero = true;
+        h->step = step0;
+    }
+    WF_CUDA(cudaGraphLaunch(it->second.exec, h->st));
+    set_roles(h, it->second.after);
+    h->iter_alias = true;
+    h->pc_zero = true;
+    h->step += 1;
+    h->launches += it->second.kernels;
+    return WF_OK;
+}
+
+int check_finite(wf_solver* h) {
+    WF_CUDA(cudaMemsetAsync(h->dbad, 0, sizeof(int), h->st));
+    wf::launch_check_finite(h->st, h->vb[h->iT], 3LL * h->P.N, h->dbad);
+    wf::launch_check_finite(h->st, h->pr, h->P.N, h->dbad);
+    WF_CHECK_LAUNCH();
+    int bad = 0;
+    WF_CUDA(cudaMemcpyAsync(&bad, h->dbad, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    WF_TRY(sync(h));
+    if (bad) return set_err(h, WF_ERR_NONFINITE, "non-finite value in velocity or pressure");
+    return WF_OK;
+}
+
+// Resolves a field id to its device pointer and size.
+float* field_ptr(wf_solver* h, int field, size_t* points, int* comps) {
+    const Params& P = h->P;
+    *points = (size_t)P.N;
+    *comps = 3;
+    switch (field) {
+        case WF_FIELD_VEL: return h->vb[h->iF];
+        case WF_FIELD_VEL_LAST_TIME: return h->vb[h->iT];
+        case WF_FIELD_VEL_LAST_ITER: return h->iter_alias ? h->vb[h->iT] : h->vb[h->iI];
+        case WF_FIELD_VEL_CORRECT: return h->uc;
+        case WF_FIELD_D: return h->Dv;
+        case WF_FIELD_B: return h->bv;
+        case WF_FIELD_AODU: return h->aodu;
+        case WF_FIELD_FACE_EDDY_VIS: return h->face;
+        default: break;
+    }
+    *comps = 1;
+    switch (field) {
+        case WF_FIELD_PRES: return h->pr;
+        case WF_FIELD_PRES_CORRECT: return h->pcb[h->iPC];
+        case WF_FIELD_PRES_CORRECT_LAST_ITER: return h->pcb[h->iPCL];
+        case WF_FIELD_DP: return h->Dp;
+        case WF_FIELD_BP: return h->bp;
+        case WF_FIELD_EDDY_VIS: return h->eddy;
+        default: break;
+    }
+    if (field >= WF_FIELD_BND_X0 && field <= WF_FIELD_BND_ZN) {
+        const int f = field - WF_FIELD_BND_X0;
+        *points = (size_t)P.plane[f];
+        *comps = 3;
+        return h->bnd[f];
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+// =====================================================================
+extern "C" {
+
+void wf_config_default(wf_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->struct_size = sizeof(wf_config);
+    // FluidSimConfig.cs:113-178 defaults
+    c->nx = 100; c->ny = 50; c->nz = 100;   // physDomainSize (10,5,10), gridResX 100
+    c->dx = 0.1f;
+    c->dt = 0.1f;
+    c->mu = 0.005f;
+    c->den = 1.0f;
+    // canonical urban boundary set (Assets/Code/Config/AijBuilding0.asset)
+    c->vel_bc[WF_FACE_X0] = WF_BND_FIXED_VALUE;
+    c->vel_bc[WF_FACE_XN] = WF_BND_ZERO_GRAD;
+    c->vel_bc[WF_FACE_Y0] = WF_BND_FIXED_VALUE;
+    c->vel_bc[WF_FACE_YN] = WF_BND_SYMMETRY;
+    c->vel_bc[WF_FACE_Z0] = WF_BND_SYMMETRY;
+    c->vel_bc[WF_FACE_ZN] = WF_BND_SYMMETRY;
+    c->pres_bc[WF_FACE_X0] = WF_BND_ZERO_GRAD;
+    c->pres_bc[WF_FACE_XN] = WF_BND_FIXED_VALUE;
+    c->pres_bc[WF_FACE_Y0] = WF_BND_ZERO_GRAD;
+    c->pres_bc[WF_FACE_YN] = WF_BND_SYMMETRY;
+    c->pres_bc[WF_FACE_Z0] = WF_BND_SYMMETRY;
+    c->pres_bc[WF_FACE_ZN] = WF_BND_SYMMETRY;
+    c->solver_type = WF_SOLVER_SIMPLE;
+    c->piso_correctors = 2;
+    c->turbulence = WF_TURB_NONE;
+    c->cs = 0.15f;
+    c->vel_iters = 50;
+    c->pres_iters = 400;
+    c->inflow_type = WF_INFLOW_CONSTANT;
+    c->wind_speed = 10.0f;   // RuntimeConfig.windSpeed default
+    c->inflow_ustar = 0.f;
+    c->inflow_z0 = 1.0f;     // FvmSolverGpu.cs:818
+    c->inflow_kappa = 0.4f;  // :817
+    c->inflow_href = 10.0f;  // :819
+    c->calc_residual = 0;
+    c->vel_res_interval = 10;
+    c->pres_res_interval = 20;
+    c->vel_tol = 1e-15f;
+    c->pres_tol = 1e-3f;
+    c->compat_flags = 0;
+    c->check_finite = 0;
+    c->use_graph = 1;
+}
+
+int wf_create(const wf_config* cfg, int device, wf_solver** out) {
+    if (!out) return WF_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (const char* why = validate(cfg)) {
+        (void)why;
+        return WF_ERR_INVALID_ARG;
+    }
+    // Host-side fault injection for failure-path tests: no GPU work is done.
+    if (const char* fi = std::getenv("WF_FAULT_INJECT")) {
+        if (std::strcmp(fi, "oom") == 0) return WF_ERR_OOM;
+        if (std::strcmp(fi, "cuda") == 0) return WF_ERR_CUDA;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return WF_ERR_CUDA;
+    if (device < 0 || device >= ndev) return WF_ERR_INVALID_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return WF_ERR_CUDA;
+
+    auto* h = new (std::nothrow) wf_solver;
+    if (!h) return WF_ERR_OOM;
+    h->cfg = *cfg;
+    h->device = device;
+    h->wind = cfg->wind_speed;
+    if (const char* fe = std::getenv("WF_FAST")) h->fast = std::atoi(fe);
+
+    Params& P = h->P;
+    P.nx = cfg->nx; P.ny = cfg->ny; P.nz = cfg->nz;
+    P.N = cfg->nx * cfg->ny * cfg->nz;
+    P.plane[WF_FACE_X0] = P.plane[WF_FACE_XN] = P.ny * P.nz;
+    P.plane[WF_FACE_Y0] = P.plane[WF_FACE_YN] = P.nx * P.nz;
+    P.plane[WF_FACE_Z0] = P.plane[WF_FACE_ZN] = P.nx * P.ny;
+    P.dx = cfg->dx;
+    P.ds = cfg->dx * cfg->dx;             // FluidSimConfig.cs:326
+    P.dv = cfg->dx * cfg->dx * cfg->dx;   // :327
+    P.dt = cfg->dt;
+    P.nu = cfg->mu / cfg->den;            // :339
+    P.den = cfg->den;
+    P.cs = cfg->cs;
+    for (int i = 0; i < 3; ++i) P.force[i] = cfg->ext_force[i];
+    for (int f = 0; f < 6; ++f) { P.vbc[f] = cfg->vel_bc[f]; P.pbc[f] = cfg->pres_bc[f]; }
+    P.les = cfg->turbulence == WF_TURB_SMAGORINSKY;
+    P.compat = cfg->compat_flags;
+
+    int s = WF_OK;
+    auto fail = [&](int code) {
+        free_all(h);
+        delete h;
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(WF_ERR_CUDA);
+    if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) return fail(WF_ERR_CUDA);
+    const size_t N = P.N, v = 3 * sizeof(float) * N, sc = sizeof(float) * N;
+    size_t planes = 0;
+    for (int f = 0; f < 6; ++f) planes += 3 * (size_t)P.plane[f];
+    const int nblk = wf::cell_grid_blocks(P);
+    if ((s = alloc(h, (void**)&h->fl, N)) ||
+        (s = alloc(h, (void**)&h->vb[0], v)) || (s = alloc(h, (void**)&h->vb[1], v)) ||
+        (s = alloc(h, (void**)&h->vb[2], v)) || (s = alloc(h, (void**)&h->uc, v)) ||
+        (s = alloc(h, (void**)&h->Dv, v)) || (s = alloc(h, (void**)&h->bv, v)) ||
+        (s = alloc(h, (void**)&h->aodu, v)) || (s = alloc(h, (void**)&h->face, v)) ||
+        (s = alloc(h, (void**)&h->pr, sc)) || (s = alloc(h, (void**)&h->pcb[0], sc)) ||
+        (s = alloc(h, (void**)&h->pcb[1], sc)) || (s = alloc(h, (void**)&h->Dp, sc)) ||
+        (s = alloc(h, (void**)&h->bp, sc)) || (s = alloc(h, (void**)&h->eddy, sc)) ||
+        (s = alloc(h, (void**)&h->pcoef, 5 * sc)) || (s = alloc(h, (void**)&h->vcoef, 9 * sc)) ||
+        (s = alloc(h, (void**)&h->part, sizeof(double) * (size_t)std::max(nblk, 1))) ||
+        (s = alloc(h, (void**)&h->dsum, 4 * sizeof(double))) || (s = alloc(h, (void**)&h->dref, sizeof(float) * 4)) ||
+        (s = alloc(h, (void**)&h->dbad, sizeof(int) * 4)) || (s = alloc(h, (void**)&h->bnd[0], sizeof(float) * planes)))
+        return fail(s);
+    for (int f = 1; f < 6; ++f) h->bnd[f] = h->bnd[f - 1] + 3 * (size_t)P.plane[f - 1];
+    for (int f = 0; f < 6; ++f) h->B.p[f] = h->bnd[f];
+    if (cudaMallocHost((void**)&h->hsum, 4 * sizeof(double)) != cudaSuccess) return fail(WF_ERR_OOM);
+
+    // Constructor sequence, FvmSolverGpu.cs:207-221.  Flags start all fluid
+    // (zeroed allocation = CELL_FLUID); faceEddyVis starts at 0 because
+    // InitFaceEddyVisField dispatches kernel 0 (:941-945).
+    if ((s = wf_init_vel_pres_fields(h)) != WF_OK) return fail(s);
+    if ((s = wf_set_fixed_value_vel_bnd_cond(h, h->wind)) != WF_OK) return fail(s);
+    if ((s = sync(h)) != WF_OK) return fail(s);
+    *out = h;
+    return WF_OK;
+}
+
+int wf_destroy(wf_solver* h) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->st);
+    free_all(h);
+    delete h;
+    return WF_OK;
+}
+
+int wf_init_flags(wf_solver* h, const int32_t* flags, size_t n) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!flags || n != (size_t)h->P.N) return set_err(h, WF_ERR_INVALID_ARG, "flags must hold nx*ny*nz int32");
+    WF_CUDA(cudaSetDevice(h->device));
+    if (!h->stage) WF_TRY(alloc(h, &h->stage, 4 * sizeof(float) * (size_t)h->P.N));
+    WF_CUDA(cudaMemcpyAsync(h->stage, flags, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->st));
+    wf::launch_init_flags(h->P, h->st, (const int32_t*)h->stage, h->fl, h->vb[0], h->vb[1], h->vb[2]);
+    WF_CHECK_LAUNCH();
+    return sync(h);
+}
+
+int wf_init_vel_pres_fields(wf_solver* h) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    WF_CUDA(cudaSetDevice(h->device));
+    const wf_config& c = h->cfg;
+    const int logp = c.inflow_type == WF_INFLOW_LOG;
+    const float fric = logp ? fric_vel(h) : 0.f;
+    const int centre = (c.compat_flags & WF_COMPAT_INIT_PROFILE_CELL_CENTRE) != 0;
+    wf::launch_init_fields(h->P, h->st, logp, h->wind, fric, c.inflow_kappa, c.inflow_z0, centre, h->vb[0],
+                           h->vb[1], h->vb[2], h->uc, h->pr);
+    WF_CHECK_LAUNCH();
+    WF_CUDA(cudaMemsetAsync(h->pcb[0], 0, sizeof(float) * h->P.N, h->st));
+    WF_CUDA(cudaMemsetAsync(h->pcb[1], 0, sizeof(float) * h->P.N, h->st));
+    h->iter_alias = false;
+    h->pc_zero = true;
+    return sync(h);
+}
+
+int wf_set_fixed_value_vel_bnd_cond(wf_solver* h, float wind_speed) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!std::isfinite(wind_speed)) return set_err(h, WF_ERR_INVALID_ARG, "wind speed must be finite");
+    WF_CUDA(cudaSetDevice(h->device));
+    h->wind = wind_speed;
+    const wf_config& c = h->cfg;
+    if (c.inflow_type == WF_INFLOW_LOG) {
+        wf::launch_set_log_inlet(h->P, h->st, fric_vel(h), c.inflow_kappa, c.inflow_z0, h->bnd[WF_FACE_X0]);
+    } else {
+        wf::launch_fill3(h->st, h->bnd[WF_FACE_X0], h->P.plane[WF_FACE_X0], wind_speed, 0.f, 0.f);
+        wf::launch_fill3(h->st, h->bnd[WF_FACE_ZN], h->P.plane[WF_FACE_ZN], c.vel_zn[0], c.vel_zn[1], c.vel_zn[2]);
+    }
+    WF_CHECK_LAUNCH();
+    return sync(h);
+}
+
+int wf_change_phys_field_pos(wf_solver* h) { return wf_init_vel_pres_fields(h); }
+
+int wf_set_inflow_plane(wf_solver* h, const float* pl) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!pl) return set_err(h, WF_ERR_INVALID_ARG, "plane is NULL");
+    WF_CUDA(cudaSetDevice(h->device));
+    const int n = h->P.plane[WF_FACE_X0];
+    std::vector<float> soa(3 * (size_t)n);
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) soa[(size_t)c * n + i] = pl[3 * (size_t)i + c];
+    WF_CUDA(cudaMemcpyAsync(h->bnd[WF_FACE_X0], soa.data(), soa.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    return sync(h);
+}
+
+int wf_step(wf_solver* h, int n_steps, int* ready) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (n_steps < 0) return set_err(h, WF_ERR_INVALID_ARG, "n_steps must be >= 0");
+    WF_CUDA(cudaSetDevice(h->device));
+    WF_CUDA(cudaEventRecord(h->ev0, h->st));
+    for (int i = 0; i < n_steps; ++i) WF_TRY(run_step(h));
+    WF_CUDA(cudaEventRecord(h->ev1, h->st));
+    WF_TRY(sync(h));
+    WF_CUDA(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+    if (h->cfg.check_finite) WF_TRY(check_finite(h));
+    if (ready) *ready = 1;
+    return WF_OK;
+}
+
+int wf_get_vel(wf_solver* h, float* out, int layout) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!out || layout < 0 || layout > 2) return set_err(h, WF_ERR_INVALID_ARG, "bad output or layout");
+    WF_CUDA(cudaSetDevice(h->device));
+    const size_t N = h->P.N;
+    const float* src = h->vb[h->iT];
+    if (layout == WF_LAYOUT_SOA) {
+        WF_CUDA(cudaMemcpyAsync(out, src, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+        return sync(h);
+    }
+    if (!h->stage) WF_TRY(alloc(h, &h->stage, 4 * sizeof(float) * N));
+    wf::launch_soa_to_interleaved(h->st, src, (int)N, (float*)h->stage, layout == WF_LAYOUT_XYZW);
+    WF_CHECK_LAUNCH();
+    const size_t per = layout == WF_LAYOUT_XYZW ? 4 : 3;
+    WF_CUDA(cudaMemcpyAsync(out, h->stage, per * N * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    return sync(h);
+}
+
+int wf_get_pres(wf_solver* h, float* out) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!out) return set_err(h, WF_ERR_INVALID_ARG, "out is NULL");
+    WF_CUDA(cudaSetDevice(h->device));
+    WF_CUDA(cudaMemcpyAsync(out, h->pr, h->P.N * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    return sync(h);
+}
+
+int wf_get_flags(wf_solver* h, int32_t* out) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!out) return set_err(h, WF_ERR_INVALID_ARG, "out is NULL");
+    WF_CUDA(cudaSetDevice(h->device));
+    if (!h->stage) WF_TRY(alloc(h, &h->stage, 4 * sizeof(float) * (size_t)h->P.N));
+    wf::launch_flags_to_i32(h->st, h->fl, h->P.N, (int32_t*)h->stage);
+    WF_CHECK_LAUNCH();
+    WF_CUDA(cudaMemcpyAsync(out, h->stage, h->P.N * sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+    return sync(h);
+}
+
+int wf_get_state(wf_solver* h, float* vel, float* pres, int64_t* step) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (vel) WF_TRY(wf_get_vel(h, vel, WF_LAYOUT_SOA));
+    if (pres) WF_TRY(wf_get_pres(h, pres));
+    if (step) *step = h->step;
+    return WF_OK;
+}
+
+int wf_set_state(wf_solver* h, const float* vel, const float* pres, int64_t step) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    WF_CUDA(cudaSetDevice(h->device));
+    const size_t N = h->P.N;
+    if (vel) {
+        // velFieldLastTime and velFieldLastIter both take the state, as after
+        // a completed step (FvmSolverGpu.cs:1105-1106).
+        WF_CUDA(cudaMemcpyAsync(h->vb[h->iT], vel, 3 * N * sizeof(float), cudaMemcpyHostToDevice, h->st));
+        h->iter_alias = true;
+    }
+    if (pres) WF_CUDA(cudaMemcpyAsync(h->pr, pres, N * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    h->pc_zero = true;
+    WF_CUDA(cudaMemsetAsync(h->pcb[0], 0, sizeof(float) * N, h->st));
+    WF_CUDA(cudaMemsetAsync(h->pcb[1], 0, sizeof(float) * N, h->st));
+    h->step = step;
+    return sync(h);
+}
+
+int wf_field_size(const wf_solver* hc, int field, size_t* points, int* comps) {
+    wf_solver* h = const_cast<wf_solver*>(hc);
+    if (!h || !points || !comps) return WF_ERR_INVALID_ARG;
+    if (!field_ptr(h, field, points, comps)) return WF_ERR_INVALID_ARG;
+    return WF_OK;
+}
+
+int wf_get_field(wf_solver* h, int field, float* out) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!out) return set_err(h, WF_ERR_INVALID_ARG, "out is NULL");
+    WF_CUDA(cudaSetDevice(h->device));
+    if ((field == WF_FIELD_PRES_CORRECT || field == WF_FIELD_PRES_CORRECT_LAST_ITER) && h->pc_zero)
+        WF_TRY(materialize_pc(h));
+    size_t n = 0;
+    int comps = 0;
+    float* p = field_ptr(h, field, &n, &comps);
+    if (!p) return set_err(h, WF_ERR_INVALID_ARG, "unknown field id");
+    WF_CUDA(cudaMemcpyAsync(out, p, n * comps * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    return sync(h);
+}
+
+int wf_set_field(wf_solver* h, int field, const float* in) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!in) return set_err(h, WF_ERR_INVALID_ARG, "in is NULL");
+    WF_CUDA(cudaSetDevice(h->device));
+    if (field == WF_FIELD_VEL_LAST_TIME || field == WF_FIELD_VEL_LAST_ITER) WF_TRY(materialize_iter(h));
+    if (field == WF_FIELD_PRES_CORRECT || field == WF_FIELD_PRES_CORRECT_LAST_ITER) WF_TRY(materialize_pc(h));
+    size_t n = 0;
+    int comps = 0;
+    float* p = field_ptr(h, field, &n, &comps);
+    if (!p) return set_err(h, WF_ERR_INVALID_ARG, "unknown field id");
+    WF_CUDA(cudaMemcpyAsync(p, in, n * comps * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    return sync(h);
+}
+
+int wf_get_device_fields(wf_solver* h, wf_device_fields* out) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!out) return set_err(h, WF_ERR_INVALID_ARG, "out is NULL");
+    const size_t N = h->P.N;
+    for (int c = 0; c < 3; ++c) out->vel[c] = h->vb[h->iT] + c * N;
+    out->pres = h->pr;
+    out->flags = h->fl;
+    out->n_cells = (int64_t)N;
+    out->stream = (void*)h->st;
+    return WF_OK;
+}
+
+int wf_residuals(wf_solver* h, float* vel, float* pres, float* mass) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (vel) *vel = h->res_vel;
+    if (pres) *pres = h->res_pres;
+    if (mass) {
+        if (!h->cfg.calc_residual) {
+            *mass = -1.f;
+        } else {
+            double m = 0.0;
+            WF_TRY(wf_mass_imbalance(h, &m));
+            *mass = (float)m;
+        }
+    }
+    return WF_OK;
+}
+
+int wf_mass_imbalance(wf_solver* h, double* out) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!out) return set_err(h, WF_ERR_INVALID_ARG, "out is NULL");
+    WF_CUDA(cudaSetDevice(h->device));
+    wf::launch_mass_imbalance(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->part, h->dsum);
+    WF_CHECK_LAUNCH();
+    return read_residual(h, out);
+}
+
+int wf_check_finite(wf_solver* h) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    WF_CUDA(cudaSetDevice(h->device));
+    return check_finite(h);
+}
+
+// ------------------------------------------------------------- per-kernel ops
+#define WF_OP_BEGIN()                       \
+    if (!h) return WF_ERR_INVALID_ARG;      \
+    WF_CUDA(cudaSetDevice(h->device))
+
+int wf_op_wallfunc(wf_solver* h) {
+    WF_OP_BEGIN();
+    wf::launch_wallfunc(h->P, h->st, h->fl, h->vb[h->iT], h->face);
+    WF_CHECK_LAUNCH();
+    return sync(h);
+}
+int wf_op_eddy_vis(wf_solver* h) {
+    WF_OP_BEGIN();
+    wf::launch_eddy_vis(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->eddy);
+    WF_CHECK_LAUNCH();
+    return sync(h);
+}
+int wf_op_les_term(wf_solver* h) {
+    WF_OP_BEGIN();
+    wf::launch_les_term(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->eddy, h->face, h->bv);
+    WF_CHECK_LAUNCH();
+    return sync(h);
+}
+int wf_op_vel_precompute(wf_solver* h) {
+    WF_OP_BEGIN();
+    WF_TRY(do_vel_precompute(h));
+    return sync(h);
+}
+int wf_op_vel_sweeps(wf_solver* h, int n) {
+    WF_OP_BEGIN();
+    if (n < 0) return set_err(h, WF_ERR_INVALID_ARG, "n must be >= 0");
+    WF_TRY(do_vel_sweeps(h, n, true));
+    return sync(h);
+}
+int wf_op_pres_precompute(wf_solver* h) {
+    WF_OP_BEGIN();
+    WF_TRY(do_pres_precompute(h));
+    return sync(h);
+}
+int wf_op_pres_sweeps(wf_solver* h, int n) {
+    WF_OP_BEGIN();
+    if (n < 0) return set_err(h, WF_ERR_INVALID_ARG, "n must be >= 0");
+    WF_TRY(do_pres_sweeps(h, n, true));
+    return sync(h);
+}
+int wf_op_apply_pres(wf_solver* h) {
+    WF_OP_BEGIN();
+    WF_TRY(do_apply_pres(h));
+    return sync(h);
+}
+int wf_op_normalize(wf_solver* h) {
+    WF_OP_BEGIN();
+    WF_TRY(do_normalize(h));
+    return sync(h);
+}
+int wf_op_apply_vel(wf_solver* h) {
+    WF_OP_BEGIN();
+    WF_TRY(do_apply_vel(h));
+    return sync(h);
+}
+int wf_op_zero_pres_correct(wf_solver* h) {
+    WF_OP_BEGIN();
+    h->pc_zero = true;
+    WF_TRY(materialize_pc(h));
+    h->pc_zero = true;
+    return sync(h);
+}
+int wf_op_piso(wf_solver* h, int n) {
+    WF_OP_BEGIN();
+    if (n < 0) return set_err(h, WF_ERR_INVALID_ARG, "n must be >= 0");
+    WF_TRY(do_piso(h, n, true));
+    return sync(h);
+}
+int wf_op_end_step(wf_solver* h) {
+    WF_OP_BEGIN();
+    WF_TRY(do_end_step(h));
+    return sync(h);
+}
+int wf_op_vel_residual(wf_solver* h, float* out) {
+    WF_OP_BEGIN();
+    if (!out) return set_err(h, WF_ERR_INVALID_ARG, "out is NULL");
+    const float* uI = h->iter_alias ? h->vb[h->iT] : h->vb[h->iI];
+    wf::launch_vel_residual(h->P, h->st, h->Dv, h->vb[h->iF], uI, h->part, h->dsum);
+    WF_CHECK_LAUNCH();
+    double s = 0.0;
+    WF_TRY(read_residual(h, &s));
+    *out = (float)std::sqrt(s / (3.0 * h->P.N));
+    return WF_OK;
+}
+int wf_op_pres_residual(wf_solver* h, float* out) {
+    WF_OP_BEGIN();
+    if (!out) return set_err(h, WF_ERR_INVALID_ARG, "out is NULL");
+    wf::launch_pres_residual(h->P, h->st, h->Dp, pc_cur(h), h->pc_zero ? nullptr : h->pcb[h->iPCL], h->part,
+                             h->dsum);
+    WF_CHECK_LAUNCH();
+    double s = 0.0;
+    WF_TRY(read_residual(h, &s));
+    *out = (float)std::sqrt(s / double(h->P.N));
+    return WF_OK;
+}
+
+const char* wf_last_error(const wf_solver* h) { return h ? h->err.c_str() : "null handle"; }
+
+const char* wf_strerror(int s) {
+    switch (s) {
+        case WF_OK: return "ok";
+        case WF_ERR_INVALID_ARG: return "invalid argument";
+        case WF_ERR_CUDA: return "CUDA runtime error";
+        case WF_ERR_OOM: return "out of device memory";
+        case WF_ERR_NONFINITE: return "non-finite value in the solution";
+        case WF_ERR_TIMEOUT: return "bounded device wait timed out";
+        case WF_ERR_UNSUPPORTED: return "unsupported option";
+        case WF_NOT_FINISHED: return "step not finished";
+        case WF_ERR_STATE: return "invalid handle state";
+        default: return "unknown status";
+    }
+}
+
+int wf_version(void) { return WF_ABI_VERSION; }
+
+int wf_last_step_ms(const wf_solver* h, float* ms) {
+    if (!h || !ms) return WF_ERR_INVALID_ARG;
+    *ms = h->last_ms;
+    return WF_OK;
+}
+
+int wf_kernel_launches(const wf_solver* h, int64_t* total) {
+    if (!h || !total) return WF_ERR_INVALID_ARG;
+    *total = h->launches;
+    return WF_OK;
+}
+
+int wf_time_kernel(wf_solver* h, int kernel, int reps, int flush_l2, float* ms_per_launch,
+                   double* alg_bytes_per_launch, int* sweeps_per_launch) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!ms_per_launch || !alg_bytes_per_launch || !sweeps_per_launch || reps <= 0 ||
+        (kernel != WF_KERNEL_PRES_SWEEP && kernel != WF_KERNEL_VEL_SWEEP))
+        return set_err(h, WF_ERR_INVALID_ARG, "bad kernel id, reps or output pointer");
+    WF_CUDA(cudaSetDevice(h->device));
+    const int s = wf::time_kernel(h, kernel, reps, flush_l2 != 0, ms_per_launch, alg_bytes_per_launch,
+                                  sweeps_per_launch);
+    if (s != WF_OK) return set_err(h, s, "kernel timing failed");
+    return WF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+// wf_common.cuh - shared device definitions of the windfvm CUDA library.
+//
+// Device layout (private to the library): every scalar field is one plane of
+// N = nx*ny*nz FP32 values, x fastest (index (z*ny + y)*nx + x, the reference's
+// host layout, InitShaderColl.compute:353).  A vector field is three such
+// planes back to back (SoA: component c at base + c*N).  Flags are one byte
+// per cell (0 fluid, 1 solid).  Boundary planes are SoA too: X planes ny*nz
+// (index z*ny+y), Y planes nx*nz (z*nx+x), Z planes nx*ny (y*nx+x), matching
+// the reference's Texture2D addressing bndFieldX0[int2(y, z)] etc.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/windfvm.h"
+
+namespace wf {
+
+// Kernels launched by this thread through the library (counted by every
+// launch site; wf_step reports the per-step total).
+extern thread_local long long g_launches;
+#define WF_COUNT_LAUNCH() (++::wf::g_launches)
+
+// Scalars and switches of one solver, passed by value to every kernel.
+struct Params {
+    int nx, ny, nz;
+    int N;          // nx*ny*nz (checked < 2^31 / 4 at create)
+    int plane[6];   // point count of each boundary plane
+    float dx, ds, dv, dt, nu, den, cs;
+    float force[3];
+    int vbc[6], pbc[6];
+    int les;
+    unsigned compat;
+};
+
+// Boundary planes: base pointer of each plane (3 SoA components of
+// plane[f] points each).
+struct Bnd {
+    const float* p[6];
+};
+
+// Face f in {E, W, N, S, U, D} = {0..5}: the order every reference kernel
+// accumulates its face terms in.
+__host__ __device__ __forceinline__ constexpr int face_ox(int f) { return f == 0 ? 1 : (f == 1 ? -1 : 0); }
+__host__ __device__ __forceinline__ constexpr int face_oy(int f) { return f == 2 ? 1 : (f == 3 ? -1 : 0); }
+__host__ __device__ __forceinline__ constexpr int face_oz(int f) { return f == 4 ? 1 : (f == 5 ? -1 : 0); }
+__host__ __device__ __forceinline__ constexpr int face_axis(int f) { return f >> 1; }
+__host__ __device__ __forceinline__ constexpr int face_sign(int f) { return (f & 1) ? -1 : 1; }
+// Domain face crossed by face f of a boundary cell.
+__host__ __device__ __forceinline__ constexpr int face_bc(int f) {
+    return f == 0 ? WF_FACE_XN : f == 1 ? WF_FACE_X0 : f == 2 ? WF_FACE_YN
+         : f == 3 ? WF_FACE_Y0 : f == 4 ? WF_FACE_ZN : WF_FACE_Z0;
+}
+
+__device__ __forceinline__ bool in_region(const Params& P, int x, int y, int z) {
+    return (unsigned)x < (unsigned)P.nx && (unsigned)y < (unsigned)P.ny && (unsigned)z < (unsigned)P.nz;
+}
+__device__ __forceinline__ int cidx(const Params& P, int x, int y, int z) {
+    return (z * P.ny + y) * P.nx + x;
+}
+__device__ __forceinline__ int plane_idx(const Params& P, int bc, int x, int y, int z) {
+    return bc <= WF_FACE_XN ? z * P.ny + y : (bc <= WF_FACE_YN ? z * P.nx + x : y * P.nx + x);
+}
+__device__ __forceinline__ float bnd_comp(const Params& P, const Bnd& B, int bc, int x, int y, int z, int c) {
+    return __ldg(B.p[bc] + (size_t)c * P.plane[bc] + plane_idx(P, bc, x, y, z));
+}
+
+}  // namespace wf

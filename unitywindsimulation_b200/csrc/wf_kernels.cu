@@ -1,0 +1,905 @@
+// wf_kernels.cu - per-operation CUDA kernels of the collocated SIMPLE/PISO LES
+// step (one thread per cell).  Each kernel restates one HLSL kernel of
+// puppy2333/UnityWindSimulation (file:line given on each) with the same face
+// order and operand order, on the SoA device layout of wf_common.cuh.
+//
+// These are the building blocks of the step and of the per-kernel parity
+// entry points (wf_op_*).  The hot Jacobi loops have faster multi-sweep
+// kernels in wf_sweeps.cu; these single-sweep kernels remain the reference
+// form they are checked against.
+#include <cuda_runtime.h>
+
+#include "wf_common.cuh"
+#include "wf_kernels.cuh"
+
+namespace wf {
+
+namespace {
+
+__device__ __forceinline__ float ld(const float* p, size_t i) { return __ldg(p + i); }
+__device__ __forceinline__ bool fluid_at(const uint8_t* fl, int i) { return __ldg(fl + i) == WF_CELL_FLUID; }
+
+struct Cell {
+    int x, y, z, i;
+};
+__device__ __forceinline__ bool cell_of_thread(const Params& P, Cell& c) {
+    c.x = blockIdx.x * blockDim.x + threadIdx.x;
+    c.y = blockIdx.y * blockDim.y + threadIdx.y;
+    c.z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (c.x >= P.nx || c.y >= P.ny || c.z >= P.nz) return false;
+    c.i = cidx(P, c.x, c.y, c.z);
+    return true;
+}
+
+// faceEddyVisField read; single channel under WF_COMPAT_RFLOAT_FACE_EDDY_VIS
+// (FvmSolverGpu.cs:304 allocates it RFloat).
+__device__ __forceinline__ float face_read(const Params& P, const float* face, int i, int axis) {
+    if ((P.compat & WF_COMPAT_RFLOAT_FACE_EDDY_VIS) && axis != 0) return 0.f;
+    return ld(face, (size_t)axis * P.N + i);
+}
+
+// Face viscosity nu + nu_t, FvmColl.compute:1596-1635 (also :1962-2001 and
+// LES.compute:643-679).
+__device__ __forceinline__ float vis_face(const Params& P, const uint8_t* fl, const float* eddy,
+                                          const float* face, const Cell& c, int f) {
+    if (!P.les) return P.nu;
+    const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+    const float eP = ld(eddy, c.i);
+    float v = P.nu + eP;
+    if (in_region(P, X, Y, Z)) {
+        const int q = cidx(P, X, Y, Z);
+        if (fluid_at(fl, q)) {
+            v = P.nu + 0.5f * (eP + ld(eddy, q));
+        } else {
+            v = P.nu + face_read(P, face, face_sign(f) > 0 ? q : c.i, face_axis(f));
+        }
+    } else if (f == 3 && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE) {
+        v = P.nu + face_read(P, face, c.i, 1);
+    }
+    return v;
+}
+
+// LogLawWallFunc, WallFunc.compute:77-123
+__device__ float log_law(float uP, float dx, float nu, float den) {
+    const float E = 9.8f, k = 0.41f;
+    const float C = E * (dx / 2.0f) / nu;
+    float eddyVis = 0.f;
+    float uTau = 1.0f;
+    uP = fabsf(uP);
+    if (uP < 1e-5f) {
+        uTau = 0.f;
+    } else {
+        for (int it = 0; it < 10; ++it) {
+            const float lg = logf(C * uTau);
+            const float f = __fsub_rn(__fmul_rn(uTau, lg), __fmul_rn(k, uP));
+            const float df = lg + 1.0f;
+            if (fabsf(df) < 1e-6f) break;
+            uTau = uTau - f / df;
+            if (uTau < 1e-5f) uTau = 1e-5f;
+        }
+        const float tauWall = uTau * uTau * den;
+        const float strainRate = uP / (dx / 2.0f);
+        eddyVis = tauWall / (strainRate * den) - nu;
+        if (eddyVis < 0.f) eddyVis = 0.f;
+    }
+    return eddyVis;
+}
+
+__device__ __forceinline__ float hypot2(float a, float b) { return sqrtf(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b))); }
+
+// Get{E,W,N,S,U,D}FaceVelLastTime, LES.compute:104-258
+__device__ __forceinline__ void face_vel(const Params& P, const Bnd& B, const uint8_t* fl, const float* uT,
+                                         int x, int y, int z, int f, float r[3]) {
+    const int X = x + face_ox(f), Y = y + face_oy(f), Z = z + face_oz(f);
+    const int i = cidx(P, x, y, z);
+    r[0] = r[1] = r[2] = 0.f;
+    if (in_region(P, X, Y, Z)) {
+        const int q = cidx(P, X, Y, Z);
+        if (fluid_at(fl, q)) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[k] = 0.5f * (ld(uT, (size_t)k * P.N + i) + ld(uT, (size_t)k * P.N + q));
+        }
+    } else {
+        const int bc = face_bc(f), bt = P.vbc[bc];
+        if (bt == WF_BND_FIXED_VALUE) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[k] = bnd_comp(P, B, bc, x, y, z, k);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[k] = ld(uT, (size_t)k * P.N + i);
+            if (bt == WF_BND_SYMMETRY) r[face_axis(f)] = 0.f;
+        }
+    }
+}
+// g[i][j] = d u_i / d x_j at a cell centre, LES.compute:296-306
+__device__ __forceinline__ void cell_grad(const Params& P, const Bnd& B, const uint8_t* fl, const float* uT,
+                                          int x, int y, int z, float g[3][3]) {
+    float fv[6][3];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) face_vel(P, B, fl, uT, x, y, z, f, fv[f]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) / P.dx;
+}
+
+// ------------------------------------------------------------ wall function
+// CSCalLogLawWallFunc, WallFunc.compute:128-190.  Writes the W/S/D face
+// slots of every cell.
+__global__ void k_wallfunc(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                           const float* __restrict__ uT, float* __restrict__ face) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    float fe0 = 0.f, fe1 = 0.f, fe2 = 0.f;
+    const size_t N = P.N;
+    auto u = [&](int i, int k) { return ld(uT, (size_t)k * N + i); };
+    const bool me_fluid = fluid_at(fl, c.i);
+    const bool w_in = c.x > 0, s_in = c.y > 0, d_in = c.z > 0;
+    const int iw = c.i - 1, is = c.i - P.nx, id = c.i - P.nx * P.ny;
+    if (me_fluid) {
+        if (w_in && !fluid_at(fl, iw)) fe0 += log_law(hypot2(u(c.i, 1), u(c.i, 2)), P.dx, P.nu, P.den);
+        if ((s_in && !fluid_at(fl, is)) || (!s_in && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE))
+            fe1 += log_law(hypot2(u(c.i, 0), u(c.i, 2)), P.dx, P.nu, P.den);
+        if (d_in && !fluid_at(fl, id)) fe2 += log_law(hypot2(u(c.i, 0), u(c.i, 1)), P.dx, P.nu, P.den);
+    } else {
+        if (w_in && fluid_at(fl, iw)) fe0 += log_law(hypot2(u(iw, 1), u(iw, 2)), P.dx, P.nu, P.den);
+        if (s_in && fluid_at(fl, is)) fe1 += log_law(hypot2(u(is, 0), u(is, 2)), P.dx, P.nu, P.den);
+        if (d_in && fluid_at(fl, id)) fe2 += log_law(hypot2(u(id, 0), u(id, 1)), P.dx, P.nu, P.den);
+    }
+    face[c.i] = fe0;
+    face[N + c.i] = fe1;
+    face[2 * N + c.i] = fe2;
+}
+
+// ------------------------------------------------------------------- LES
+// CSCalEddyVis, LES.compute:268-324
+__global__ void k_eddy_vis(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
+                           const float* __restrict__ uT, float* __restrict__ eddy) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    float g[3][3];
+    cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
+    const float Sxx = g[0][0], Syy = g[1][1], Szz = g[2][2];
+    const float Sxy = 0.5f * (g[0][1] + g[1][0]);
+    const float Syz = 0.5f * (g[1][2] + g[2][1]);
+    const float Szx = 0.5f * (g[2][0] + g[0][2]);
+    const float Sabs = sqrtf(2.0f * (Sxx * Sxx + Syy * Syy + Szz * Szz + 2.0f * Sxy * Sxy + 2.0f * Syz * Syz +
+                                     2.0f * Szx * Szx));
+    eddy[c.i] = (P.cs * P.cs) * (P.dx * P.dx) * Sabs;
+}
+
+// CSCalLesDeferCorrectTerm, LES.compute:327-687.  Output: the explicit LES
+// term per momentum component (bField on the reference).
+__global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
+                           const float* __restrict__ uT, const float* __restrict__ eddy,
+                           const float* __restrict__ face, float* __restrict__ bles) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    float g[3][3];
+    cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
+    float fg[6][3];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        fg[f][0] = fg[f][1] = fg[f][2] = 0.f;
+        const int a = face_axis(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (in_region(P, X, Y, Z)) {
+            if (fluid_at(fl, cidx(P, X, Y, Z))) {
+                float gn[3][3];
+                cell_grad(P, B, fl, uT, X, Y, Z, gn);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + gn[a][j]);
+            } else {
+                const float v = ld(uT, (size_t)a * N + c.i) / (0.5f * P.dx);
+                fg[f][a] = face_sign(f) > 0 ? -v : v;
+            }
+        } else {
+            const int bc = face_bc(f), bt = P.vbc[bc];
+            if (bt == WF_BND_FIXED_VALUE) {
+                const float b = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
+                const float u = ld(uT, (size_t)a * N + c.i);
+                fg[f][a] = face_sign(f) > 0 ? (b - u) / (0.5f * P.dx) : (u - b) / (0.5f * P.dx);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    if (j != a) fg[f][j] = g[a][j];
+            }
+        }
+    }
+    float vis[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) vis[f] = vis_face(P, fl, eddy, face, c, f);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float t = vis[0] * fg[0][j] - vis[1] * fg[1][j] + vis[2] * fg[2][j] - vis[3] * fg[3][j] +
+                        vis[4] * fg[4][j] - vis[5] * fg[5][j];
+        bles[(size_t)j * N + c.i] = P.ds * t;
+    }
+}
+
+// ------------------------------------------------------- momentum predictor
+// CSVelPredictPreCompute, FvmColl.compute:1292-1859.  bles (may be null when
+// LES is off) holds the LES term; D and b are written.  bles may alias b.
+__global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
+                                 const float* __restrict__ uT, const float* __restrict__ pr,
+                                 const float* __restrict__ eddy, const float* __restrict__ face,
+                                 const float* bles, float* __restrict__ Dv, float* bv) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    float uP[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) uP[k] = ld(uT, k * N + c.i);
+    const float dvdt = P.dv / P.dt;
+    float D[3] = {dvdt, dvdt, dvdt};
+    float b[3] = {0.f, 0.f, 0.f};
+    // advection, :1314-1482
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            if (fluid_at(fl, q)) {
+                const float t = P.ds * 0.25f * (uP[a] + ld(uT, a * N + q));
+#pragma unroll
+                for (int k = 0; k < 3; ++k) D[k] = face_sign(f) > 0 ? D[k] + t : D[k] - t;
+            }
+        } else {
+            const int bc = face_bc(f), bt = P.vbc[bc];
+            if (bt == WF_BND_FIXED_VALUE) {
+                const float ba = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float t = P.ds * bnd_comp(P, B, bc, c.x, c.y, c.z, k) * ba;
+                    b[k] = face_sign(f) > 0 ? b[k] - t : b[k] + t;
+                }
+            } else if (bt == WF_BND_ZERO_GRAD) {
+                const float t = P.ds * uP[a];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) D[k] = face_sign(f) > 0 ? D[k] + t : D[k] - t;
+            }
+        }
+    }
+    // pressure, :1484-1591
+    const float pP = ld(pr, c.i);
+    float pf[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            pf[f] = fluid_at(fl, q) ? 0.5f * (pP + ld(pr, q)) : pP;
+        } else {
+            pf[f] = P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE ? 0.f : pP;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) b[a] += -(1.0f / P.den) * P.ds * (pf[2 * a] - pf[2 * a + 1]);
+    // diffusion, :1593-1836
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        const float vis = vis_face(P, fl, eddy, face, c, f);
+        if (in_region(P, X, Y, Z)) {
+            const float t = fluid_at(fl, cidx(P, X, Y, Z)) ? vis * P.ds / P.dx : 2.f * vis * P.ds / P.dx;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) D[k] += t;
+        } else {
+            const int bc = face_bc(f), bt = P.vbc[bc];
+            const float t = 2.f * vis * P.ds / P.dx;
+            if (bt == WF_BND_FIXED_VALUE) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) b[k] += t * bnd_comp(P, B, bc, c.x, c.y, c.z, k);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) D[k] += t;
+            } else if (bt == WF_BND_SYMMETRY) {
+                D[face_axis(f)] += t;
+            }
+        }
+    }
+    // time, force, LES, :1838-1854
+#pragma unroll
+    for (int k = 0; k < 3; ++k) b[k] += dvdt * uP[k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) b[k] += P.dv * P.force[k];
+    if (P.les && bles) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) b[k] += bles[k * N + c.i];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        Dv[k * N + c.i] = D[k];
+        bv[k * N + c.i] = b[k];
+    }
+}
+
+// CSVelPredict, FvmColl.compute:1863-2069.  uI == nullptr is not allowed
+// here (the sweep always reads a previous iterate).
+__global__ void k_vel_sweep(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                            const float* __restrict__ uI, const float* __restrict__ uT,
+                            const float* __restrict__ eddy, const float* __restrict__ face,
+                            const float* __restrict__ Dv, const float* __restrict__ bv, float* __restrict__ uo) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    float adv[3] = {0.f, 0.f, 0.f}, dif[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float sum = ld(uT, a * N + c.i) + ld(uT, a * N + q);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float t = P.ds * 0.25f * ld(uI, k * N + q) * sum;
+            adv[k] = face_sign(f) > 0 ? adv[k] - t : adv[k] + t;
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float vis = vis_face(P, fl, eddy, face, c, f);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) dif[k] += vis * P.ds / P.dx * ld(uI, k * N + q);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) uo[k * N + c.i] = 1.0f / ld(Dv, k * N + c.i) * (adv[k] + dif[k] + ld(bv, k * N + c.i));
+}
+
+// ----------------------------------------------------- pressure correction
+// CSPresCorrectRhieChowPreCompute, FvmColl.compute:2481-2787
+__global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
+                                  const float* __restrict__ u, const float* __restrict__ pr,
+                                  const float* __restrict__ Dv, float* __restrict__ Dp, float* __restrict__ bp) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float dx2 = 2.f * P.dx;
+    float DP = 0.f, bP = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f), s = face_sign(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            if (!fluid_at(fl, q)) continue;
+            const float DInv = 0.5f * (1.f / ld(Dv, a * N + c.i) + 1.f / ld(Dv, a * N + q));
+            DP -= (P.dv / P.den) * DInv / P.dx;
+            const float fl_ = 0.5f * (ld(u, a * N + c.i) + ld(u, a * N + q));
+            bP = s > 0 ? bP + fl_ : bP - fl_;
+            // Rhie-Chow over the face between low cell L and high cell H
+            const int L = s > 0 ? c.i : q, H = s > 0 ? q : c.i;
+            const int lx = s > 0 ? c.x : X, ly = s > 0 ? c.y : Y, lz = s > 0 ? c.z : Z;
+            const int hx = s > 0 ? X : c.x, hy = s > 0 ? Y : c.y, hz = s > 0 ? Z : c.z;
+            const int ex = (a == 0), ey = (a == 1), ez = (a == 2);
+            const bool hh = in_region(P, hx + ex, hy + ey, hz + ez) && fluid_at(fl, cidx(P, hx + ex, hy + ey, hz + ez));
+            const bool ll = in_region(P, lx - ex, ly - ey, lz - ez) && fluid_at(fl, cidx(P, lx - ex, ly - ey, lz - ez));
+            const float pL = ld(pr, L), pH = ld(pr, H);
+            const float presGrad = (pH - pL) / P.dx;
+            float ave = presGrad;
+            if (hh || ll) {
+                const float gH = hh ? (ld(pr, cidx(P, hx + ex, hy + ey, hz + ez)) - pL) / dx2 : (pH - pL) / dx2;
+                const float gL = ll ? (pH - ld(pr, cidx(P, lx - ex, ly - ey, lz - ez))) / dx2 : (pH - pL) / dx2;
+                ave = 0.5f * (gH + gL);
+            }
+            const float vct = -(P.dv * DInv) / P.den * (presGrad - ave);
+            bP = s > 0 ? bP + vct : bP - vct;
+        } else {
+            const int bc = face_bc(f), vb = P.vbc[bc];
+            if (vb == WF_BND_FIXED_VALUE) {
+                const float t = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
+                bP = s > 0 ? bP + t : bP - t;
+            } else if (vb == WF_BND_ZERO_GRAD) {
+                const float t = ld(u, a * N + c.i);
+                bP = s > 0 ? bP + t : bP - t;
+            }
+            if (P.pbc[bc] == WF_BND_FIXED_VALUE) {
+                const float DInv = 1.f / ld(Dv, a * N + c.i);
+                DP -= 2.f * (P.dv / P.den) * DInv / P.dx;
+            }
+        }
+    }
+    Dp[c.i] = DP;
+    bp[c.i] = bP;
+}
+
+// CSPresCorrectRhieChow, FvmColl.compute:2790-2848.  pin == nullptr reads as
+// an all-zero previous iterate.
+__global__ void k_pres_sweep(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                             const float* __restrict__ pin, const float* __restrict__ Dv,
+                             const float* __restrict__ Dp, const float* __restrict__ bp, float* __restrict__ pout) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    float t = 0.f;
+    if (pin) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            const int a = face_axis(f);
+            const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+            if (!in_region(P, X, Y, Z)) continue;
+            const int q = cidx(P, X, Y, Z);
+            if (!fluid_at(fl, q)) continue;
+            const float DInv = 0.5f * (1.f / ld(Dv, a * N + c.i) + 1.f / ld(Dv, a * N + q));
+            t -= (P.dv / P.den) * DInv / P.dx * ld(pin, q);
+        }
+    }
+    pout[c.i] = (1.f / ld(Dp, c.i)) * (t + ld(bp, c.i));
+}
+
+// CSApplyPresCorrection, FvmColl.compute:2851-2862 (non-solid cells) and
+// CSPisoApplyPresCorrection, PisoColl.compute:259-267 (fluid cells).  With
+// flags restricted to {fluid, solid} both select the fluid cells.
+__global__ void k_apply_pres(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                             const float* __restrict__ pc, float* __restrict__ pr) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (__ldg(fl + c.i) == WF_CELL_SOLID) return;
+    pr[c.i] += pc ? ld(pc, c.i) : 0.f;
+}
+
+// CSPresNormalization, FvmColl.compute:2865-2880, split in two launches so
+// the reference value is read before any cell is updated.
+__global__ void k_norm_read(const __grid_constant__ Params P, const float* __restrict__ pr, float* __restrict__ ref) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *ref = pr[cidx(P, 2, P.ny / 2, 2)];
+}
+__global__ void k_norm_apply(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                             const float* __restrict__ ref, float* __restrict__ pr) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (__ldg(fl + c.i) == WF_CELL_SOLID) return;
+    pr[c.i] -= __ldg(ref);
+}
+
+// CSApplyVelCorrectionDivergenceTheorem, FvmColl.compute:2951-3121.
+// pc == nullptr reads as zero.
+__global__ void k_apply_vel(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                            const float* __restrict__ pc, const float* __restrict__ Dv,
+                            float* __restrict__ uc, float* __restrict__ u) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float pP = pc ? ld(pc, c.i) : 0.f;
+    float pf[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            pf[f] = fluid_at(fl, q) ? 0.5f * (pP + (pc ? ld(pc, q) : 0.f)) : pP;
+        } else {
+            pf[f] = P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE ? 0.f : pP;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float corr = -(P.dv / P.den) * (1.f / ld(Dv, a * N + c.i)) * (pf[2 * a] - pf[2 * a + 1]) / P.dx;
+        uc[a * N + c.i] = corr;
+        u[a * N + c.i] += corr;
+    }
+}
+
+// ------------------------------------------------------------------ PISO
+// CSPisoCalAodUCorrect, PisoColl.compute:71-178
+__global__ void k_piso_aodu(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                            const float* __restrict__ uc, const float* __restrict__ uT,
+                            const float* __restrict__ eddy, const float* __restrict__ face,
+                            float* __restrict__ aodu) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const bool consistent = (P.compat & WF_COMPAT_PISO_CONSISTENT) != 0;
+    float adv[3] = {0.f, 0.f, 0.f}, dif[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float sum = ld(uT, a * N + c.i) + ld(uT, a * N + q);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float t = P.ds * 0.25f * ld(uc, k * N + q) * sum;
+            adv[k] = face_sign(f) > 0 ? adv[k] + t : adv[k] - t;
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float vis = consistent ? vis_face(P, fl, eddy, face, c, f) : P.nu;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) dif[k] -= vis * P.ds / P.dx * ld(uc, k * N + q);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) aodu[k * N + c.i] = adv[k] + dif[k];
+}
+
+// CSPisoPresCorrection, PisoColl.compute:181-256.  pin == nullptr reads as 0.
+__global__ void k_piso_pres_sweep(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                                  const float* __restrict__ pin, const float* __restrict__ Dv,
+                                  const float* __restrict__ aodu, float* __restrict__ pout) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const bool consistent = (P.compat & WF_COMPAT_PISO_CONSISTENT) != 0;
+    float coeff = 0.f, pt = 0.f, vt = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) {
+            if (consistent && P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE) {
+                const float DInv = 1.f / ld(Dv, a * N + c.i);
+                coeff -= 2.f * (P.dv / P.den) * DInv / P.dx;
+            }
+            continue;
+        }
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float AdInv = 0.5f * (1.f / ld(Dv, a * N + c.i) + 1.f / ld(Dv, a * N + q));
+        const float Aod = 0.5f * (ld(aodu, a * N + c.i) + ld(aodu, a * N + q));
+        const float pq = pin ? ld(pin, q) : 0.f;
+        if (a == 0) {
+            coeff -= (P.dv / P.den) * (AdInv / P.dx);
+            pt -= (P.dv / P.den) * (AdInv / P.dx) * pq;
+        } else {
+            coeff -= (P.dv / P.den) * AdInv / P.dx;
+            pt -= (P.dv / P.den) * AdInv / P.dx * pq;
+        }
+        vt = face_sign(f) > 0 ? vt - AdInv * Aod : vt + AdInv * Aod;
+    }
+    pout[c.i] = (1.f / coeff) * (pt + vt);
+}
+
+// CSPisoVelCorrection, PisoColl.compute:270-337
+__global__ void k_piso_vel(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                           const float* __restrict__ pc, const float* __restrict__ Dv,
+                           const float* __restrict__ aodu, float* __restrict__ uc, float* __restrict__ u) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float pP = ld(pc, c.i);
+    float pf[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        pf[f] = pP;
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            if (fluid_at(fl, q)) pf[f] = 0.5f * (pP + ld(pc, q));
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float grad = (pf[2 * a] - pf[2 * a + 1]) / P.dx;
+        const float DInv = 1.f / ld(Dv, a * N + c.i);
+        const float corr = -DInv * (ld(aodu, a * N + c.i) + P.dv / P.den * grad);
+        uc[a * N + c.i] = corr;
+        u[a * N + c.i] += corr;
+    }
+}
+
+// --------------------------------------------------------------- residuals
+// Block partial sums of squared residuals (FvmColl.compute:3124-3199): warp
+// shuffles, then one value per block; a second pass adds the partials in
+// block order, so the result is deterministic.
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, warp = tid >> 5;
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    double r = 0.0;
+    if (warp == 0) {
+        r = lane < nw ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    return r;
+}
+__device__ __forceinline__ int block_linear() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+__device__ __forceinline__ bool block_leader() { return threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0; }
+
+__global__ void k_vel_residual(const __grid_constant__ Params P, const float* __restrict__ Dv,
+                               const float* __restrict__ u, const float* __restrict__ uI, double* __restrict__ part) {
+    Cell c;
+    double s = 0.0;
+    if (cell_of_thread(P, c)) {
+        const size_t N = P.N;
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float l = ld(Dv, k * N + c.i) * (ld(u, k * N + c.i) - ld(uI, k * N + c.i));
+            acc += l * l;
+        }
+        s = acc;
+    }
+    s = block_sum(s);
+    if (block_leader()) part[block_linear()] = s;
+}
+__global__ void k_pres_residual(const __grid_constant__ Params P, const float* __restrict__ Dp,
+                                const float* __restrict__ pc, const float* __restrict__ pcL,
+                                double* __restrict__ part) {
+    Cell c;
+    double s = 0.0;
+    if (cell_of_thread(P, c)) {
+        const float a = pc ? ld(pc, c.i) : 0.f, b = pcL ? ld(pcL, c.i) : 0.f;
+        const float l = ld(Dp, c.i) * (a - b);
+        s = l * l;
+    }
+    s = block_sum(s);
+    if (block_leader()) part[block_linear()] = s;
+}
+__global__ void k_sum_partials(const double* __restrict__ part, int n, double* __restrict__ out) {
+    __shared__ double sh[1024];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+// Sum over fluid cells of |net face flux| of u (BC-aware, no Rhie-Chow).
+__global__ void k_mass_imbalance(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
+                                 const float* __restrict__ u, double* __restrict__ part) {
+    Cell c;
+    double s = 0.0;
+    if (cell_of_thread(P, c) && fluid_at(fl, c.i)) {
+        const size_t N = P.N;
+        double div = 0.0;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            const int a = face_axis(f);
+            const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+            double uf = 0.0;
+            if (in_region(P, X, Y, Z)) {
+                const int q = cidx(P, X, Y, Z);
+                if (fluid_at(fl, q)) uf = 0.5 * ((double)ld(u, a * N + c.i) + (double)ld(u, a * N + q));
+            } else {
+                const int bc = face_bc(f), vb = P.vbc[bc];
+                if (vb == WF_BND_FIXED_VALUE) uf = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
+                else if (vb == WF_BND_ZERO_GRAD) uf = ld(u, a * N + c.i);
+            }
+            div += face_sign(f) * uf;
+        }
+        s = fabs(div) * (double)P.ds;
+    }
+    s = block_sum(s);
+    if (block_leader()) part[block_linear()] = s;
+}
+
+// Non-finite scan: sets *bad = 1 when any value is NaN/Inf.
+__global__ void k_check_finite(const float* __restrict__ a, long long n, int* __restrict__ bad) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int b = 0;
+    for (; i < n; i += stride) b |= !isfinite(__ldg(a + i));
+    if (__syncthreads_or(b) && threadIdx.x == 0) atomicOr(bad, 1);
+}
+
+// ------------------------------------------------------------------ set-up
+// CSInitVelPresFields / CSInitLogVelPresFields, InitShaderColl.compute:95-132:
+// every cell of the three velocity buffers gets the profile, velCorrect and
+// pressures are zeroed.  fric_vel <= 0 selects the constant profile.
+__global__ void k_init_fields(const __grid_constant__ Params P, int logp, float wind, float fric, float kappa,
+                              float z0, int centre, float* u0, float* u1, float* u2, float* uc, float* pr) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    const size_t N = P.N;
+    float vx = wind;
+    if (logp) {
+        const float yPhys = centre ? ((float)c.y + 0.5f) * P.dx : (float)c.y * P.dx;
+        vx = fric / kappa * logf((yPhys + z0) / z0);
+    }
+    float* bufs[3] = {u0, u1, u2};
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        if (!bufs[b]) continue;
+        bufs[b][c.i] = vx;
+        bufs[b][N + c.i] = 0.f;
+        bufs[b][2 * N + c.i] = 0.f;
+    }
+    uc[c.i] = 0.f;
+    uc[N + c.i] = 0.f;
+    uc[2 * N + c.i] = 0.f;
+    pr[c.i] = 0.f;
+}
+
+// CSInitModelFlag, InitShaderColl.compute:346-364
+__global__ void k_init_flags(const __grid_constant__ Params P, const int32_t* __restrict__ src,
+                             uint8_t* __restrict__ fl, float* u0, float* u1, float* u2) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    const size_t N = P.N;
+    if ((double)src[c.i] > 0.5) {
+        fl[c.i] = WF_CELL_SOLID;
+        float* bufs[3] = {u0, u1, u2};
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            if (!bufs[b]) continue;
+            bufs[b][c.i] = 0.f;
+            bufs[b][N + c.i] = 0.f;
+            bufs[b][2 * N + c.i] = 0.f;
+        }
+    } else {
+        fl[c.i] = WF_CELL_FLUID;
+    }
+}
+
+// CSSetLogVelBndCond, InitShaderColl.compute:273-285 (X0 plane, ny*nz points)
+__global__ void k_set_log_inlet(int ny, int nz, float dx, float fric, float kappa, float z0, float* x0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = ny * nz;
+    if (i >= n) return;
+    const int y = i % ny;
+    const float yPhys = ((float)y + 0.5f) * dx;
+    x0[i] = fric / kappa * logf((yPhys + z0) / z0);
+    x0[n + i] = 0.f;
+    x0[2 * n + i] = 0.f;
+}
+__global__ void k_fill3(float* a, int n, float v0, float v1, float v2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    a[i] = v0;
+    a[n + i] = v1;
+    a[2 * n + i] = v2;
+}
+
+// Layout conversion for host I/O.
+__global__ void k_soa_to_xyzw(const float* __restrict__ s, int n, float* __restrict__ d, int w4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (w4) {
+        reinterpret_cast<float4*>(d)[i] = make_float4(s[i], s[n + i], s[2 * (size_t)n + i], 0.f);
+    } else {
+        d[3 * (size_t)i] = s[i];
+        d[3 * (size_t)i + 1] = s[n + i];
+        d[3 * (size_t)i + 2] = s[2 * (size_t)n + i];
+    }
+}
+__global__ void k_flags_to_i32(const uint8_t* __restrict__ f, int n, int32_t* __restrict__ o) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = f[i];
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- launchers
+thread_local long long g_launches = 0;
+
+static dim3 cell_block() { return dim3(32, 4, 2); }
+static dim3 cell_grid(const Params& P) {
+    dim3 b = cell_block();
+    return dim3((P.nx + b.x - 1) / b.x, (P.ny + b.y - 1) / b.y, (P.nz + b.z - 1) / b.z);
+}
+int cell_grid_blocks(const Params& P) {
+    dim3 g = cell_grid(P);
+    return (int)(g.x * g.y * g.z);
+}
+
+#define WF_LAUNCH(kernel, ...) \
+    (WF_COUNT_LAUNCH(), kernel<<<cell_grid(P), cell_block(), 0, st>>>(P, __VA_ARGS__))
+
+void launch_wallfunc(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, float* face) {
+    WF_LAUNCH(k_wallfunc, fl, uT, face);
+}
+void launch_eddy_vis(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT, float* eddy) {
+    WF_LAUNCH(k_eddy_vis, B, fl, uT, eddy);
+}
+void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
+                     const float* eddy, const float* face, float* bles) {
+    WF_LAUNCH(k_les_term, B, fl, uT, eddy, face, bles);
+}
+void launch_vel_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
+                           const float* pr, const float* eddy, const float* face, const float* bles, float* Dv,
+                           float* bv) {
+    WF_LAUNCH(k_vel_precompute, B, fl, uT, pr, eddy, face, bles, Dv, bv);
+}
+void launch_vel_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uI, const float* uT,
+                      const float* eddy, const float* face, const float* Dv, const float* bv, float* uo) {
+    WF_LAUNCH(k_vel_sweep, fl, uI, uT, eddy, face, Dv, bv, uo);
+}
+void launch_pres_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* u,
+                            const float* pr, const float* Dv, float* Dp, float* bp) {
+    WF_LAUNCH(k_pres_precompute, B, fl, u, pr, Dv, Dp, bp);
+}
+void launch_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pin, const float* Dv,
+                       const float* Dp, const float* bp, float* pout) {
+    WF_LAUNCH(k_pres_sweep, fl, pin, Dv, Dp, bp, pout);
+}
+void launch_apply_pres(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, float* pr) {
+    WF_LAUNCH(k_apply_pres, fl, pc, pr);
+}
+void launch_normalize(const Params& P, cudaStream_t st, const uint8_t* fl, float* pr, float* ref) {
+    WF_COUNT_LAUNCH();
+    k_norm_read<<<1, 32, 0, st>>>(P, pr, ref);
+    WF_LAUNCH(k_norm_apply, fl, ref, pr);
+}
+void launch_apply_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
+                      float* uc, float* u) {
+    WF_LAUNCH(k_apply_vel, fl, pc, Dv, uc, u);
+}
+void launch_piso_aodu(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uc, const float* uT,
+                      const float* eddy, const float* face, float* aodu) {
+    WF_LAUNCH(k_piso_aodu, fl, uc, uT, eddy, face, aodu);
+}
+void launch_piso_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pin, const float* Dv,
+                            const float* aodu, float* pout) {
+    WF_LAUNCH(k_piso_pres_sweep, fl, pin, Dv, aodu, pout);
+}
+void launch_piso_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
+                     const float* aodu, float* uc, float* u) {
+    WF_LAUNCH(k_piso_vel, fl, pc, Dv, aodu, uc, u);
+}
+void launch_vel_residual(const Params& P, cudaStream_t st, const float* Dv, const float* u, const float* uI,
+                         double* part, double* out) {
+    WF_LAUNCH(k_vel_residual, Dv, u, uI, part);
+    WF_COUNT_LAUNCH();
+    k_sum_partials<<<1, 1024, 0, st>>>(part, cell_grid_blocks(P), out);
+}
+void launch_pres_residual(const Params& P, cudaStream_t st, const float* Dp, const float* pc, const float* pcL,
+                          double* part, double* out) {
+    WF_LAUNCH(k_pres_residual, Dp, pc, pcL, part);
+    WF_COUNT_LAUNCH();
+    k_sum_partials<<<1, 1024, 0, st>>>(part, cell_grid_blocks(P), out);
+}
+void launch_mass_imbalance(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* u,
+                           double* part, double* out) {
+    WF_LAUNCH(k_mass_imbalance, B, fl, u, part);
+    WF_COUNT_LAUNCH();
+    k_sum_partials<<<1, 1024, 0, st>>>(part, cell_grid_blocks(P), out);
+}
+void launch_check_finite(cudaStream_t st, const float* a, long long n, int* bad) {
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+    if (blocks < 1) blocks = 1;
+    k_check_finite<<<blocks, 256, 0, st>>>(a, n, bad);
+}
+void launch_init_fields(const Params& P, cudaStream_t st, int logp, float wind, float fric, float kappa, float z0,
+                        int centre, float* u0, float* u1, float* u2, float* uc, float* pr) {
+    WF_LAUNCH(k_init_fields, logp, wind, fric, kappa, z0, centre, u0, u1, u2, uc, pr);
+}
+void launch_init_flags(const Params& P, cudaStream_t st, const int32_t* src, uint8_t* fl, float* u0, float* u1,
+                       float* u2) {
+    WF_LAUNCH(k_init_flags, src, fl, u0, u1, u2);
+}
+void launch_set_log_inlet(const Params& P, cudaStream_t st, float fric, float kappa, float z0, float* x0) {
+    const int n = P.ny * P.nz;
+    k_set_log_inlet<<<(n + 255) / 256, 256, 0, st>>>(P.ny, P.nz, P.dx, fric, kappa, z0, x0);
+}
+void launch_fill3(cudaStream_t st, float* a, int n, float v0, float v1, float v2) {
+    k_fill3<<<(n + 255) / 256, 256, 0, st>>>(a, n, v0, v1, v2);
+}
+void launch_soa_to_interleaved(cudaStream_t st, const float* s, int n, float* d, int w4) {
+    k_soa_to_xyzw<<<(n + 255) / 256, 256, 0, st>>>(s, n, d, w4);
+}
+void launch_flags_to_i32(cudaStream_t st, const uint8_t* f, int n, int32_t* o) {
+    k_flags_to_i32<<<(n + 255) / 256, 256, 0, st>>>(f, n, o);
+}
+
+}  // namespace wf

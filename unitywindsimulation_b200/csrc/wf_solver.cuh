@@ -1,0 +1,66 @@
+// wf_solver.cuh - the solver handle behind the C ABI (private).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+
+#include "wf_common.cuh"
+
+struct wf_solver {
+    wf_config cfg{};
+    wf::Params P{};
+    wf::Bnd B{};
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    // ---- device fields (see wf_common.cuh for the layout) ----
+    uint8_t* fl = nullptr;
+    // Three velocity buffers rotated by role like the reference's
+    // velField / velFieldLastTime / velFieldLastIter textures.  When
+    // iter_alias is set, velFieldLastIter is logically equal to
+    // velFieldLastTime and buffer vb[iI] holds no meaningful fluid values
+    // (this replaces the end-of-step copy, FvmSolverGpu.cs:1106).
+    float* vb[3] = {nullptr, nullptr, nullptr};
+    int iT = 0, iF = 1, iI = 2;
+    bool iter_alias = false;
+    float *uc = nullptr, *Dv = nullptr, *bv = nullptr, *aodu = nullptr, *face = nullptr;
+    float* pr = nullptr;
+    // presCorrectField / presCorrectFieldLastIter.  When pc_zero is set both
+    // are logically all-zero (replaces SetPresCorrectFieldtoZero,
+    // FvmSolverGpu.cs:1545-1554; the first sweep then reads no input).
+    float* pcb[2] = {nullptr, nullptr};
+    int iPC = 0, iPCL = 1;
+    bool pc_zero = true;
+    float *Dp = nullptr, *bp = nullptr, *eddy = nullptr;
+    float* bnd[6] = {};
+    // sweep coefficient caches of the fast path (wf_sweeps.cu)
+    float* pcoef = nullptr;   // pressure: c_E, c_N, c_U, 1/Dp, PISO rhs (5 planes)
+    float* vcoef = nullptr;   // momentum: A_E..A_D, 1/D (9 planes)
+    // scratch
+    double* part = nullptr;
+    double* dsum = nullptr;   // 4 doubles
+    float* dref = nullptr;
+    int* dbad = nullptr;
+    void* stage = nullptr;    // 4N floats of device staging for host I/O
+    double* hsum = nullptr;   // pinned
+
+    float wind = 0.f;
+    int64_t step = 0;
+    float res_vel = -1.f, res_pres = -1.f;
+    float last_ms = 0.f;
+    int fast = 1;             // use the fast Jacobi kernels (wf_sweeps.cu)
+    long long launches = 0;   // kernels launched by wf_step
+    std::string err;
+
+    // CUDA-graph cache of one step, keyed by the buffer roles before the step.
+    using RoleKey = std::tuple<int, int, int, int, int>;
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        RoleKey after{};
+        long long kernels = 0;
+    };
+    std::map<RoleKey, GraphEntry> graphs;
+};

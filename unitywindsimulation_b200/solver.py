@@ -1,0 +1,219 @@
+"""Host-side mirror of the reference's ``IFvmSolver`` over the C ABI.
+
+``FvmSolverCuda`` exposes the operations of ``IFvmSolver``
+(Assets/Code/FvmSolver/IFvmSolver.cs:3-24) with the reference's names and
+argument meaning -- ``Step``, ``InitFlags``, ``InitVelPresFields``,
+``SetFixedValueVelBndCond``, ``ChangePhysFieldPos``, ``ChangePhysDomainSize``,
+``GetVelField``, ``GetPresField``, ``GetFlagField`` -- plus snake_case aliases,
+field access for parity checks and the per-kernel operations.
+
+All compute runs in libwindfvm.so on the GPU; a missing library or device
+raises ``WindFvmError``.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, byref, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
+
+import numpy as np
+
+from . import _lib
+from ._lib import WfConfig, WfDeviceFields, WindFvmError, check
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_float))
+
+
+class FvmSolverCuda:
+    """One solver handle on one GPU (FvmSolverGpu equivalent)."""
+
+    def __init__(self, cfg: WfConfig, device: int = 0):
+        self._lib = _lib.load()
+        self.cfg = cfg.copy()
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)  # numpy order of the flat x-fastest arrays
+        self.n_cells = cfg.nx * cfg.ny * cfg.nz
+        h = c_void_p()
+        st = self._lib.wf_create(byref(self.cfg), device, byref(h))
+        if st != _lib.WF_OK:
+            raise WindFvmError(st, f"wf_create failed: {self._lib.wf_strerror(st).decode()}")
+        self._h = h
+        self.wind_speed = cfg.wind_speed
+
+    # ---- lifecycle ----
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.wf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int):
+        check(st, self._h)
+
+    # ---- IFvmSolver ----
+    def Step(self, n_steps: int = 1) -> bool:
+        ready = c_int(0)
+        self._check(self._lib.wf_step(self._h, int(n_steps), byref(ready)))
+        return bool(ready.value)
+
+    def InitFlags(self, flags) -> None:
+        f = np.ascontiguousarray(np.asarray(flags, dtype=np.int32).reshape(-1))
+        if f.size != self.n_cells:
+            raise ValueError(f"flags must hold {self.n_cells} values")
+        self._check(self._lib.wf_init_flags(self._h, f.ctypes.data_as(POINTER(c_int32)), f.size))
+
+    def InitVelPresFields(self) -> None:
+        self._check(self._lib.wf_init_vel_pres_fields(self._h))
+
+    def SetFixedValueVelBndCond(self, wind_speed: float | None = None) -> None:
+        if wind_speed is not None:
+            self.wind_speed = float(wind_speed)
+        self._check(self._lib.wf_set_fixed_value_vel_bnd_cond(self._h, c_float(self.wind_speed)))
+
+    def ChangePhysFieldPos(self) -> None:
+        self._check(self._lib.wf_change_phys_field_pos(self._h))
+
+    def ChangePhysDomainSize(self, cfg: WfConfig | None = None, device: int = 0) -> None:
+        """Re-creates the handle for a new grid (the reference re-reads gridRes
+        and re-initialises the fields, FvmSolverGpu.cs:1034-1046)."""
+        new = (cfg or self.cfg).copy()
+        self.close()
+        self.__init__(new, device)
+
+    def GetVelField(self, layout: int = _lib.LAYOUT_SOA, out: np.ndarray | None = None) -> np.ndarray:
+        """Current velocity.  SOA -> (3, nz, ny, nx); XYZW -> (nz, ny, nx, 4).
+        `out` (float32, contiguous, right size) may be a pinned host buffer."""
+        n = self.n_cells
+        per = {_lib.LAYOUT_SOA: 3, _lib.LAYOUT_XYZW: 4, _lib.LAYOUT_XYZ: 3}[layout]
+        if out is None:
+            out = np.empty(per * n, dtype=np.float32)
+        elif out.dtype != np.float32 or out.size != per * n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 array of the field's size")
+        self._check(self._lib.wf_get_vel(self._h, _fptr(out), layout))
+        if layout == _lib.LAYOUT_SOA:
+            return out.reshape((3,) + self.shape)
+        return out.reshape(self.shape + (per,))
+
+    def GetPresField(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.n_cells, dtype=np.float32)
+        elif out.dtype != np.float32 or out.size != self.n_cells or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 array of the field's size")
+        self._check(self._lib.wf_get_pres(self._h, _fptr(out)))
+        return out.reshape(self.shape)
+
+    def GetFlagField(self) -> np.ndarray:
+        out = np.empty(self.n_cells, dtype=np.int32)
+        self._check(self._lib.wf_get_flags(self._h, out.ctypes.data_as(POINTER(c_int32))))
+        return out.reshape(self.shape)
+
+    # snake_case aliases
+    step = Step
+    init_flags = InitFlags
+    init_vel_pres_fields = InitVelPresFields
+    set_fixed_value_vel_bnd_cond = SetFixedValueVelBndCond
+    get_vel = GetVelField
+    get_pres = GetPresField
+    get_flags = GetFlagField
+
+    # ---- extras ----
+    def set_inflow_plane(self, plane_xyz: np.ndarray) -> None:
+        """X0 inlet plane, shape (nz, ny, 3)."""
+        a = np.ascontiguousarray(plane_xyz, dtype=np.float32).reshape(-1)
+        if a.size != 3 * self.cfg.ny * self.cfg.nz:
+            raise ValueError("inlet plane must be (nz, ny, 3)")
+        self._check(self._lib.wf_set_inflow_plane(self._h, _fptr(a)))
+
+    def get_state(self):
+        vel = np.empty(3 * self.n_cells, dtype=np.float32)
+        pres = np.empty(self.n_cells, dtype=np.float32)
+        step = c_int64(0)
+        self._check(self._lib.wf_get_state(self._h, _fptr(vel), _fptr(pres), byref(step)))
+        return vel.reshape((3,) + self.shape), pres.reshape(self.shape), step.value
+
+    def set_state(self, vel: np.ndarray, pres: np.ndarray, step: int = 0) -> None:
+        v = np.ascontiguousarray(vel, dtype=np.float32).reshape(-1)
+        p = np.ascontiguousarray(pres, dtype=np.float32).reshape(-1)
+        self._check(self._lib.wf_set_state(self._h, _fptr(v), _fptr(p), int(step)))
+
+    def field_size(self, field: int):
+        pts, comps = c_size_t(0), c_int(0)
+        self._check(self._lib.wf_field_size(self._h, field, byref(pts), byref(comps)))
+        return pts.value, comps.value
+
+    def get_field(self, field: int) -> np.ndarray:
+        pts, comps = self.field_size(field)
+        out = np.empty(pts * comps, dtype=np.float32)
+        self._check(self._lib.wf_get_field(self._h, field, _fptr(out)))
+        return out.reshape((comps, pts)) if comps > 1 else out
+
+    def set_field(self, field: int, data: np.ndarray) -> None:
+        pts, comps = self.field_size(field)
+        a = np.ascontiguousarray(data, dtype=np.float32).reshape(-1)
+        if a.size != pts * comps:
+            raise ValueError(f"field {field} needs {pts * comps} floats")
+        self._check(self._lib.wf_set_field(self._h, field, _fptr(a)))
+
+    def device_fields(self) -> WfDeviceFields:
+        d = WfDeviceFields()
+        self._check(self._lib.wf_get_device_fields(self._h, byref(d)))
+        return d
+
+    def residuals(self):
+        v, p, m = c_float(0), c_float(0), c_float(0)
+        self._check(self._lib.wf_residuals(self._h, byref(v), byref(p), byref(m)))
+        return v.value, p.value, m.value
+
+    def mass_imbalance(self) -> float:
+        m = c_double(0)
+        self._check(self._lib.wf_mass_imbalance(self._h, byref(m)))
+        return m.value
+
+    def check_finite(self) -> None:
+        self._check(self._lib.wf_check_finite(self._h))
+
+    def last_step_ms(self) -> float:
+        ms = c_float(0)
+        self._check(self._lib.wf_last_step_ms(self._h, byref(ms)))
+        return ms.value
+
+    def kernel_launches(self) -> int:
+        n = c_int64(0)
+        self._check(self._lib.wf_kernel_launches(self._h, byref(n)))
+        return n.value
+
+    def time_kernel(self, kernel: int, reps: int = 20, flush_l2: bool = True):
+        """(ms per launch, algorithmic bytes per launch, sweeps per launch)."""
+        ms, by, sw = c_float(0), c_double(0), c_int(0)
+        self._check(self._lib.wf_time_kernel(self._h, kernel, reps, int(flush_l2), byref(ms), byref(by), byref(sw)))
+        return ms.value, by.value, sw.value
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.device_fields().stream or 0)
+
+    # ---- per-kernel operations ----
+    def op(self, name: str, *args) -> None:
+        fn = getattr(self._lib, f"wf_op_{name}")
+        self._check(fn(self._h, *[int(a) for a in args]))
+
+    def op_residual(self, which: str) -> float:
+        out = c_float(0)
+        fn = getattr(self._lib, f"wf_op_{which}_residual")
+        self._check(fn(self._h, byref(out)))
+        return out.value
+
+
+# Reference-style name for the solver class.
+FvmSolverGpu = FvmSolverCuda
