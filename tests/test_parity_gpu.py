@@ -99,6 +99,33 @@ def test_pres_sweeps_parity(small, n):
     assert_fields(g, o, [_lib.FIELD_PRES_CORRECT], label=f"pres_sweeps({n})")
 
 
+@pytest.mark.parametrize("pk,vk", [(1, 1), (2, 3), (3, 2), (4, 1)])
+@pytest.mark.parametrize("n", [1, 2, 5, 9])
+def test_sweep_blocking_depths(built, monkeypatch, pk, vk, n):
+    """Every temporal-blocking depth (sweeps per pass) and every remainder
+    pattern gives the reference's iterates n and n-1 in velField /
+    velFieldLastIter and presCorrectField / presCorrectFieldLastIter."""
+    monkeypatch.setenv("WF_PRES_K", str(pk))
+    monkeypatch.setenv("WF_VEL_K", str(vk))
+    case = cases.small_case(nx=40, ny=20, nz=30, seed=21)
+    g, o = make_pair(case)
+    for s in (g, o):
+        s.op("vel_precompute")
+    copy_state(o, g)
+    g.op("vel_sweeps", n)
+    o.op("vel_sweeps", n)
+    assert_fields(g, o, [_lib.FIELD_VEL, _lib.FIELD_VEL_LAST_ITER], label=f"vel k={vk} n={n}")
+    o.op("pres_precompute")
+    copy_state(o, g)
+    g.op("pres_sweeps", n)
+    o.op("pres_sweeps", n)
+    assert_fields(g, o, [_lib.FIELD_PRES_CORRECT, _lib.FIELD_PRES_CORRECT_LAST_ITER],
+                  label=f"pres k={pk} n={n}")
+    g.Step(2)
+    o.Step(2)
+    assert_fields(g, o, [_lib.FIELD_VEL_LAST_TIME, _lib.FIELD_PRES], tol=2 * REL_TOL, label="steps")
+
+
 @pytest.mark.parametrize("n", [1, 5])
 def test_piso_parity(small, n):
     g, o = make_pair(small)

@@ -114,8 +114,8 @@ void free_all(wf_solver* h) {
     for (auto& kv : h->graphs)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     h->graphs.clear();
-    void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
-                    h->pcb[0], h->pcb[1], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->part, h->dsum, h->dref,
+    void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->vb[3], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
+                    h->pcb[0], h->pcb[1], h->pcb[2], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->part, h->dsum, h->dref,
                     h->dbad, h->stage, h->bnd[0]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -140,8 +140,8 @@ int materialize_iter(wf_solver* h) {
 // Makes both pressure-correction buffers real zeros again.
 int materialize_pc(wf_solver* h) {
     if (!h->pc_zero) return WF_OK;
-    WF_CUDA(cudaMemsetAsync(h->pcb[0], 0, sizeof(float) * h->P.N, h->st));
-    WF_CUDA(cudaMemsetAsync(h->pcb[1], 0, sizeof(float) * h->P.N, h->st));
+    WF_CUDA(cudaMemsetAsync(h->pcb[h->iPC], 0, sizeof(float) * h->P.N, h->st));
+    WF_CUDA(cudaMemsetAsync(h->pcb[h->iPCL], 0, sizeof(float) * h->P.N, h->st));
     h->pc_zero = false;
     return WF_OK;
 }
@@ -295,7 +295,16 @@ int do_end_step(wf_solver* h) {
 }
 
 // One complete Step() (FvmSolverGpu.cs:1050-1121) with fixed counts.
+int enqueue_step_body(wf_solver* h);
+
 int enqueue_step(wf_solver* h) {
+    h->in_step = true;
+    const int s = enqueue_step_body(h);
+    h->in_step = false;
+    return s;
+}
+
+int enqueue_step_body(wf_solver* h) {
     const wf_config& c = h->cfg;
     if (h->P.les) WF_TRY(do_les(h));
     WF_TRY(do_vel_precompute(h));
@@ -493,6 +502,8 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     h->device = device;
     h->wind = cfg->wind_speed;
     if (const char* fe = std::getenv("WF_FAST")) h->fast = std::atoi(fe);
+    if (const char* pk = std::getenv("WF_PRES_K")) h->pres_k = std::min(std::max(std::atoi(pk), 1), 4);
+    if (const char* vk = std::getenv("WF_VEL_K")) h->vel_k = std::min(std::max(std::atoi(vk), 1), 3);
 
     Params& P = h->P;
     P.nx = cfg->nx; P.ny = cfg->ny; P.nz = cfg->nz;
@@ -526,11 +537,13 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     const int nblk = wf::cell_grid_blocks(P);
     if ((s = alloc(h, (void**)&h->fl, N)) ||
         (s = alloc(h, (void**)&h->vb[0], v)) || (s = alloc(h, (void**)&h->vb[1], v)) ||
-        (s = alloc(h, (void**)&h->vb[2], v)) || (s = alloc(h, (void**)&h->uc, v)) ||
+        (s = alloc(h, (void**)&h->vb[2], v)) || (s = alloc(h, (void**)&h->vb[3], v)) ||
+        (s = alloc(h, (void**)&h->uc, v)) ||
         (s = alloc(h, (void**)&h->Dv, v)) || (s = alloc(h, (void**)&h->bv, v)) ||
         (s = alloc(h, (void**)&h->aodu, v)) || (s = alloc(h, (void**)&h->face, v)) ||
         (s = alloc(h, (void**)&h->pr, sc)) || (s = alloc(h, (void**)&h->pcb[0], sc)) ||
-        (s = alloc(h, (void**)&h->pcb[1], sc)) || (s = alloc(h, (void**)&h->Dp, sc)) ||
+        (s = alloc(h, (void**)&h->pcb[1], sc)) || (s = alloc(h, (void**)&h->pcb[2], sc)) ||
+        (s = alloc(h, (void**)&h->Dp, sc)) ||
         (s = alloc(h, (void**)&h->bp, sc)) || (s = alloc(h, (void**)&h->eddy, sc)) ||
         (s = alloc(h, (void**)&h->pcoef, 5 * sc)) || (s = alloc(h, (void**)&h->vcoef, 9 * sc)) ||
         (s = alloc(h, (void**)&h->part, sizeof(double) * (size_t)std::max(nblk, 1))) ||
@@ -567,6 +580,7 @@ int wf_init_flags(wf_solver* h, const int32_t* flags, size_t n) {
     if (!h->stage) WF_TRY(alloc(h, &h->stage, 4 * sizeof(float) * (size_t)h->P.N));
     WF_CUDA(cudaMemcpyAsync(h->stage, flags, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->st));
     wf::launch_init_flags(h->P, h->st, (const int32_t*)h->stage, h->fl, h->vb[0], h->vb[1], h->vb[2]);
+    wf::launch_init_flags(h->P, h->st, (const int32_t*)h->stage, h->fl, h->vb[3], nullptr, nullptr);
     WF_CHECK_LAUNCH();
     return sync(h);
 }
@@ -581,8 +595,8 @@ int wf_init_vel_pres_fields(wf_solver* h) {
     wf::launch_init_fields(h->P, h->st, logp, h->wind, fric, c.inflow_kappa, c.inflow_z0, centre, h->vb[0],
                            h->vb[1], h->vb[2], h->uc, h->pr);
     WF_CHECK_LAUNCH();
-    WF_CUDA(cudaMemsetAsync(h->pcb[0], 0, sizeof(float) * h->P.N, h->st));
-    WF_CUDA(cudaMemsetAsync(h->pcb[1], 0, sizeof(float) * h->P.N, h->st));
+    WF_CUDA(cudaMemcpyAsync(h->vb[3], h->vb[0], 3 * sizeof(float) * h->P.N, cudaMemcpyDeviceToDevice, h->st));
+    for (int b = 0; b < 3; ++b) WF_CUDA(cudaMemsetAsync(h->pcb[b], 0, sizeof(float) * h->P.N, h->st));
     h->iter_alias = false;
     h->pc_zero = true;
     return sync(h);
@@ -689,8 +703,7 @@ int wf_set_state(wf_solver* h, const float* vel, const float* pres, int64_t step
     }
     if (pres) WF_CUDA(cudaMemcpyAsync(h->pr, pres, N * sizeof(float), cudaMemcpyHostToDevice, h->st));
     h->pc_zero = true;
-    WF_CUDA(cudaMemsetAsync(h->pcb[0], 0, sizeof(float) * N, h->st));
-    WF_CUDA(cudaMemsetAsync(h->pcb[1], 0, sizeof(float) * N, h->st));
+    for (int b = 0; b < 3; ++b) WF_CUDA(cudaMemsetAsync(h->pcb[b], 0, sizeof(float) * N, h->st));
     h->step = step;
     return sync(h);
 }

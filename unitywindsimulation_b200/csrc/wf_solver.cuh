@@ -23,7 +23,10 @@ struct wf_solver {
     // iter_alias is set, velFieldLastIter is logically equal to
     // velFieldLastTime and buffer vb[iI] holds no meaningful fluid values
     // (this replaces the end-of-step copy, FvmSolverGpu.cs:1106).
-    float* vb[3] = {nullptr, nullptr, nullptr};
+    // A fourth, spare buffer lets the multi-sweep kernels write iterates n
+    // and n-1 while velFieldLastTime and the pass input stay intact.  Solid
+    // cells hold the same values in all four (no kernel writes them).
+    float* vb[4] = {nullptr, nullptr, nullptr, nullptr};
     int iT = 0, iF = 1, iI = 2;
     bool iter_alias = false;
     float *uc = nullptr, *Dv = nullptr, *bv = nullptr, *aodu = nullptr, *face = nullptr;
@@ -31,7 +34,9 @@ struct wf_solver {
     // presCorrectField / presCorrectFieldLastIter.  When pc_zero is set both
     // are logically all-zero (replaces SetPresCorrectFieldtoZero,
     // FvmSolverGpu.cs:1545-1554; the first sweep then reads no input).
-    float* pcb[2] = {nullptr, nullptr};
+    // Three physical buffers: the multi-sweep kernels need a third one to
+    // materialise iterate n-1 next to iterate n.
+    float* pcb[3] = {nullptr, nullptr, nullptr};
     int iPC = 0, iPCL = 1;
     bool pc_zero = true;
     float *Dp = nullptr, *bp = nullptr, *eddy = nullptr;
@@ -52,6 +57,9 @@ struct wf_solver {
     float res_vel = -1.f, res_pres = -1.f;
     float last_ms = 0.f;
     int fast = 1;             // use the fast Jacobi kernels (wf_sweeps.cu)
+    int pres_k = 3;           // pressure sweeps per multi-sweep pass (1..4)
+    int vel_k = 2;            // momentum sweeps per multi-sweep pass (1..3)
+    bool in_step = false;     // inside wf_step: skip iterates no later kernel reads
     long long launches = 0;   // kernels launched by wf_step
     std::string err;
 
