@@ -232,25 +232,37 @@ __global__ void __launch_bounds__(256) k_pres_sweep1(const __grid_constant__ Par
 // A block owns a 32 x 32 column tile of the x-y plane, K cells wider than
 // its output tile on every side, and streams a chunk of z planes.  Level 0
 // is the input iterate; level s (1..K) is sweep s.  At pipeline step t the
-// block loads input plane zs + t and level s computes plane zs + t - s from
+// block pushes input plane zs + t and level s computes plane zs + t - s from
 // level s-1's planes zs+t-s-1 .. zs+t-s+1: the own column's three planes sit
 // in registers, the x/y neighbours in a double-buffered shared plane per
-// level.  One __syncthreads per pipeline step.  The valid region shrinks by
-// one cell per level on every side, so level K is exact on the output tile
-// and z chunk.  Cells outside the domain hold 0 at every level, which with
-// their zero coefficients reproduces the reference's InRegion tests.
+// level.  Coefficients are read from DRAM once per pass: the own column's
+// c_U, 1/Dp and rhs ride in register queues, c_E and c_N (needed by the x/y
+// neighbours) in a shared ring of K+1 planes.  Every load of step t+1 is
+// issued at the top of step t, so its latency hides behind step t's
+// arithmetic; one __syncthreads per step.  The valid region shrinks by one
+// cell per level on every side, so level K is exact on the output tile and
+// z chunk.  Cells outside the domain carry zero values and coefficients,
+// which reproduces the reference's InRegion tests without branches, and
+// non-fluid cells have 1/Dp = 0, so they stay 0 inside the pass and are
+// never written.
 //
-// DRAM traffic per pass and cell: the coefficients (c_E, c_N, c_U, 1/Dp,
-// rhs: 20 B) and the input iterate (4 B) once, the output iterate (4 B)
-// once, against 28 B per sweep for one sweep per launch.
+// DRAM traffic per pass and cell: coefficients (c_E, c_N, c_U, 1/Dp, rhs:
+// 20 B) and the input iterate (4 B) once, the output iterate (4 B) once,
+// against 28 B per sweep for one sweep per launch.
 constexpr int MS_TX = 32, MS_TY = 32;
+constexpr size_t pres_msweep_smem(int K) { return sizeof(float) * MS_TX * MS_TY * (2 * K + 2 * (K + 1)); }
 
 template <int K>
 __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
     k_pres_msweep(const __grid_constant__ Params P, const float* __restrict__ c3, const float* __restrict__ ainv,
                   const float* __restrict__ rhs, const float* __restrict__ pin, float* __restrict__ pout,
                   float* __restrict__ pprev, int zchunk) {
-    __shared__ float S[K][2][MS_TY][MS_TX];
+    // dynamic shared memory (above the 48 KB static limit for K >= 3):
+    // V[K][2][TY][TX] level planes, CE/CN[K+1][TY][TX] coefficient rings
+    extern __shared__ float msm[];
+    float(*V)[2][MS_TY][MS_TX] = reinterpret_cast<float(*)[2][MS_TY][MS_TX]>(msm);
+    float(*CE)[MS_TY][MS_TX] = reinterpret_cast<float(*)[MS_TY][MS_TX]>(msm + K * 2 * MS_TY * MS_TX);
+    float(*CN)[MS_TY][MS_TX] = CE + (K + 1);
     const int tx = threadIdx.x, ty = threadIdx.y;
     constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
     const int x = blockIdx.x * OX - K + tx;
@@ -261,67 +273,95 @@ __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
     const bool out_col = inxy && tx >= K && tx < MS_TX - K && ty >= K && ty < MS_TY - K;
     const size_t N = P.N;
     const int sxy = P.nx * P.ny;
-    const int col = y * P.nx + x;  // only used when inxy
-    const float* cE = c3;
-    const float* cN = c3 + N;
-    const float* cU = c3 + 2 * N;
+    const int col = inxy ? y * P.nx + x : 0;
+    const float* cEg = c3;
+    const float* cNg = c3 + N;
+    const float* cUg = c3 + 2 * N;
     const int xe = min(tx + 1, MS_TX - 1), xw = max(tx - 1, 0);
     const int yn = min(ty + 1, MS_TY - 1), ys = max(ty - 1, 0);
 
-    float h[K + 1][3];
 #pragma unroll
-    for (int s = 0; s <= K; ++s) h[s][0] = h[s][1] = h[s][2] = 0.f;
+    for (int s = 0; s < K; ++s) V[s][0][ty][tx] = V[s][1][ty][tx] = 0.f;
+#pragma unroll
+    for (int s = 0; s <= K; ++s) CE[s][ty][tx] = CN[s][ty][tx] = 0.f;
+    float h[K + 1][3];
+    float qa[K + 1], qr[K + 1], qu[K + 2];
+#pragma unroll
+    for (int s = 0; s <= K; ++s) h[s][0] = h[s][1] = h[s][2] = qa[s] = qr[s] = 0.f;
+#pragma unroll
+    for (int s = 0; s < K + 2; ++s) qu[s] = 0.f;
 
     const int zs = z0 - K;
     const int T = (z1 - z0) + 2 * K;
+    float pv = 0.f, pe = 0.f, pn = 0.f, pu = 0.f, pa = 0.f, pr = 0.f;
+    {
+        const int p = zs;
+        if (inxy && p >= 0 && p < P.nz) {
+            const int i = p * sxy + col;
+            pv = pin ? __ldg(pin + i) : 0.f;
+            pe = __ldg(cEg + i); pn = __ldg(cNg + i); pu = __ldg(cUg + i);
+            pa = __ldg(ainv + i); pr = __ldg(rhs + i);
+        }
+    }
+    __syncthreads();
     for (int t = 0; t < T; ++t) {
         const int cur = t & 1, prv = cur ^ 1;
-        {  // level 0: input plane zs + t
-            const int p = zs + t;
-            float v = 0.f;
-            if (pin && inxy && p >= 0 && p < P.nz) v = __ldg(pin + (size_t)p * sxy + col);
-            h[0][0] = h[0][1];
-            h[0][1] = h[0][2];
-            h[0][2] = v;
-            S[0][cur][ty][tx] = v;
+        // prefetch step t+1
+        float nv = 0.f, ne = 0.f, nn = 0.f, nu = 0.f, na = 0.f, nr = 0.f;
+        {
+            const int p = zs + t + 1;
+            if (inxy && p >= 0 && p < P.nz && t + 1 < T) {
+                const int i = p * sxy + col;
+                nv = pin ? __ldg(pin + i) : 0.f;
+                ne = __ldg(cEg + i); nn = __ldg(cNg + i); nu = __ldg(cUg + i);
+                na = __ldg(ainv + i); nr = __ldg(rhs + i);
+            }
         }
+        // level 0 and the coefficients of plane zs + t
+        h[0][0] = h[0][1]; h[0][1] = h[0][2]; h[0][2] = pv;
+        V[0][cur][ty][tx] = pv;
+        const int cw = t % (K + 1);
+        CE[cw][ty][tx] = pe;
+        CN[cw][ty][tx] = pn;
+#pragma unroll
+        for (int s = K; s > 0; --s) { qa[s] = qa[s - 1]; qr[s] = qr[s - 1]; }
+        qa[0] = pa; qr[0] = pr;
+#pragma unroll
+        for (int s = K + 1; s > 0; --s) qu[s] = qu[s - 1];
+        qu[0] = pu;
 #pragma unroll
         for (int s = 1; s <= K; ++s) {
-            const int p = zs + t - s;
-            float v = 0.f;
-            if (t >= s && inxy && p >= 0 && p < P.nz) {
-                const int i = p * sxy + col;
-                const float ai = __ldg(ainv + i);
-                if (ai != 0.f) {
-                    const float(*L)[MS_TX] = S[s - 1][prv];
-                    float acc = 0.f;
-                    acc -= __ldg(cE + i) * L[ty][xe];
-                    acc -= (x > 0 ? __ldg(cE + i - 1) : 0.f) * L[ty][xw];
-                    acc -= __ldg(cN + i) * L[yn][tx];
-                    acc -= (y > 0 ? __ldg(cN + i - P.nx) : 0.f) * L[ys][tx];
-                    acc -= __ldg(cU + i) * h[s - 1][2];
-                    acc -= (p > 0 ? __ldg(cU + i - sxy) : 0.f) * h[s - 1][0];
-                    v = ai * (acc + __ldg(rhs + i));
-                    if (s == K && out_col && p >= z0 && p < z1) {
-                        pout[i] = v;
-                        if (pprev) pprev[i] = h[K - 1][1];
-                    }
+            const int rs = (t - s + K + 1) % (K + 1);
+            const float(*L)[MS_TX] = V[s - 1][prv];
+            float acc = -(CE[rs][ty][tx] * L[ty][xe]);
+            acc -= CE[rs][ty][xw] * L[ty][xw];
+            acc -= CN[rs][ty][tx] * L[yn][tx];
+            acc -= CN[rs][ys][tx] * L[ys][tx];
+            acc -= qu[s] * h[s - 1][2];
+            acc -= qu[s + 1] * h[s - 1][0];
+            const float v = qa[s] * (acc + qr[s]);
+            if (s == K) {
+                const int p = zs + t - K;
+                if (out_col && p >= z0 && p < z1 && qa[K] != 0.f) {
+                    const int i = p * sxy + col;
+                    pout[i] = v;
+                    if (pprev) pprev[i] = h[K - 1][1];
                 }
             }
-            h[s][0] = h[s][1];
-            h[s][1] = h[s][2];
-            h[s][2] = v;
-            if (s < K) S[s][cur][ty][tx] = v;
+            h[s][0] = h[s][1]; h[s][1] = h[s][2]; h[s][2] = v;
+            if (s < K) V[s][cur][ty][tx] = v;
         }
         __syncthreads();
+        pv = nv; pe = ne; pn = nn; pu = nu; pa = na; pr = nr;
     }
 }
 
-// K momentum sweeps per pass: the same wavefront as k_pres_msweep for the
-// three velocity components, on a 32 x 16 tile (three components need
-// three times the registers per level).  Per pass and cell the 12
-// coefficient planes (A_E..A_D, 1/D, b: 48 B) and the input iterate (12 B)
-// are read once and the output iterate (12 B) written once.
+// K momentum sweeps per pass: the same wavefront for the three velocity
+// components on a 32 x 16 tile (three components need three times the
+// registers per level).  All 12 coefficient planes (A_E..A_D, 1/D, b) are
+// the own column's, so they ride in register queues.  Per pass and cell the
+// coefficients (48 B) and the input iterate (12 B) are read once and the
+// output iterate (12 B) written once.
 constexpr int MV_TX = 32, MV_TY = 16;
 
 template <int K>
@@ -329,7 +369,7 @@ __global__ void __launch_bounds__(MV_TX* MV_TY, 1)
     k_vel_msweep(const __grid_constant__ Params P, const float* __restrict__ A, const float* __restrict__ iD,
                  const float* __restrict__ bv, const float* __restrict__ uin, float* __restrict__ uout,
                  float* __restrict__ uprev, int zchunk) {
-    __shared__ float S[K][2][3][MV_TY][MV_TX];
+    __shared__ float V[K][2][3][MV_TY][MV_TX];
     const int tx = threadIdx.x, ty = threadIdx.y;
     constexpr int OX = MV_TX - 2 * K, OY = MV_TY - 2 * K;
     const int x = blockIdx.x * OX - K + tx;
@@ -340,72 +380,97 @@ __global__ void __launch_bounds__(MV_TX* MV_TY, 1)
     const bool out_col = inxy && tx >= K && tx < MV_TX - K && ty >= K && ty < MV_TY - K;
     const size_t N = P.N;
     const int sxy = P.nx * P.ny;
-    const int col = y * P.nx + x;
+    const int col = inxy ? y * P.nx + x : 0;
     const int xe = min(tx + 1, MV_TX - 1), xw = max(tx - 1, 0);
     const int yn = min(ty + 1, MV_TY - 1), ys = max(ty - 1, 0);
 
-    float h[K + 1][3][3];  // [level][component][plane z-1, z, z+1]
 #pragma unroll
-    for (int s = 0; s <= K; ++s)
+    for (int s = 0; s < K; ++s)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) V[s][0][c][ty][tx] = V[s][1][c][ty][tx] = 0.f;
+    float h[K + 1][3][3];
+    float qc[K + 1][12];  // A_E..A_D, 1/D x3, b x3 of planes zs+t, zs+t-1, ...
+#pragma unroll
+    for (int s = 0; s <= K; ++s) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) h[s][c][0] = h[s][c][1] = h[s][c][2] = 0.f;
-
+#pragma unroll
+        for (int j = 0; j < 12; ++j) qc[s][j] = 0.f;
+    }
     const int zs = z0 - K;
     const int T = (z1 - z0) + 2 * K;
+    float pv[3], pc[12];
+    auto load = [&](int p, bool ok, float v[3], float c[12]) {
+        if (ok && inxy && p >= 0 && p < P.nz) {
+            const int i = p * sxy + col;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) v[k] = __ldg(uin + k * N + i);
+#pragma unroll
+            for (int f = 0; f < 6; ++f) c[f] = __ldg(A + f * N + i);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) c[6 + k] = __ldg(iD + k * N + i);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) c[9 + k] = __ldg(bv + k * N + i);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) v[k] = 0.f;
+#pragma unroll
+            for (int j = 0; j < 12; ++j) c[j] = 0.f;
+        }
+    };
+    load(zs, true, pv, pc);
+    __syncthreads();
     for (int t = 0; t < T; ++t) {
         const int cur = t & 1, prv = cur ^ 1;
-        {
-            const int p = zs + t;
-            const bool ok = inxy && p >= 0 && p < P.nz;
+        float nv[3], nc[12];
+        load(zs + t + 1, t + 1 < T, nv, nc);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const float v = ok ? __ldg(uin + c * N + (size_t)p * sxy + col) : 0.f;
-                h[0][c][0] = h[0][c][1];
-                h[0][c][1] = h[0][c][2];
-                h[0][c][2] = v;
-                S[0][cur][c][ty][tx] = v;
-            }
+        for (int c = 0; c < 3; ++c) {
+            h[0][c][0] = h[0][c][1]; h[0][c][1] = h[0][c][2]; h[0][c][2] = pv[c];
+            V[0][cur][c][ty][tx] = pv[c];
         }
 #pragma unroll
+        for (int s = K; s > 0; --s)
+#pragma unroll
+            for (int j = 0; j < 12; ++j) qc[s][j] = qc[s - 1][j];
+#pragma unroll
+        for (int j = 0; j < 12; ++j) qc[0][j] = pc[j];
+#pragma unroll
         for (int s = 1; s <= K; ++s) {
-            const int p = zs + t - s;
-            float v[3] = {0.f, 0.f, 0.f};
-            if (t >= s && inxy && p >= 0 && p < P.nz) {
-                const int i = p * sxy + col;
-                const float d0 = __ldg(iD + i);
-                if (d0 != 0.f) {
-                    const float aE = __ldg(A + i), aW = __ldg(A + N + i), aN = __ldg(A + 2 * N + i);
-                    const float aS = __ldg(A + 3 * N + i), aU = __ldg(A + 4 * N + i), aD = __ldg(A + 5 * N + i);
+            float v[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float(*L)[MV_TX] = V[s - 1][prv][c];
+                float acc = qc[s][0] * L[ty][xe];
+                acc += qc[s][1] * L[ty][xw];
+                acc += qc[s][2] * L[yn][tx];
+                acc += qc[s][3] * L[ys][tx];
+                acc += qc[s][4] * h[s - 1][c][2];
+                acc += qc[s][5] * h[s - 1][c][0];
+                v[c] = qc[s][6 + c] * (acc + qc[s][9 + c]);
+            }
+            if (s == K) {
+                const int p = zs + t - K;
+                if (out_col && p >= z0 && p < z1 && qc[K][6] != 0.f) {
+                    const int i = p * sxy + col;
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        const float(*L)[MV_TX] = S[s - 1][prv][c];
-                        float acc = aE * L[ty][xe];
-                        acc += aW * L[ty][xw];
-                        acc += aN * L[yn][tx];
-                        acc += aS * L[ys][tx];
-                        acc += aU * h[s - 1][c][2];
-                        acc += aD * h[s - 1][c][0];
-                        const float dk = c == 0 ? d0 : __ldg(iD + c * N + i);
-                        v[c] = dk * (acc + __ldg(bv + c * N + i));
-                    }
-                    if (s == K && out_col && p >= z0 && p < z1) {
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            uout[c * N + i] = v[c];
-                            if (uprev) uprev[c * N + i] = h[K - 1][c][1];
-                        }
+                        uout[c * N + i] = v[c];
+                        if (uprev) uprev[c * N + i] = h[K - 1][c][1];
                     }
                 }
             }
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                h[s][c][0] = h[s][c][1];
-                h[s][c][1] = h[s][c][2];
-                h[s][c][2] = v[c];
-                if (s < K) S[s][cur][c][ty][tx] = v[c];
+                h[s][c][0] = h[s][c][1]; h[s][c][1] = h[s][c][2]; h[s][c][2] = v[c];
+                if (s < K) V[s][cur][c][ty][tx] = v[c];
             }
         }
         __syncthreads();
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pv[c] = nv[c];
+#pragma unroll
+        for (int j = 0; j < 12; ++j) pc[j] = nc[j];
     }
 }
 
@@ -496,6 +561,19 @@ void launch_vmsweep(wf_solver* h, int k, const float* in, float* out, float* pre
 
 }  // namespace
 
+int sweeps_setup() {
+    // dynamic shared memory above 48 KB needs the opt-in, per device
+    cudaError_t e = cudaSuccess;
+    e = cudaFuncSetAttribute(k_pres_msweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(1));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_pres_msweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(2));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_pres_msweep<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(3));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_pres_msweep<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(4));
+    return e == cudaSuccess ? WF_OK : WF_ERR_CUDA;
+}
+
 int vel_sweeps_fast(wf_solver* h, int n) {
     vel_coef(h);
     const int kmax = std::min(std::max(h->vel_k, 1), 3);
@@ -560,9 +638,10 @@ void launch_msweep_k(wf_solver* h, const float* rhs, const float* in, float* out
     int nchunk = std::max(1, (2 * 148 + gx * gy - 1) / (gx * gy));
     int zchunk = std::max(8, (P.nz + nchunk - 1) / nchunk);
     nchunk = (P.nz + zchunk - 1) / zchunk;
+    const size_t smem = pres_msweep_smem(K);
     WF_COUNT_LAUNCH();
-    k_pres_msweep<K><<<dim3(gx, gy, nchunk), dim3(MS_TX, MS_TY), 0, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
-                                                                           in, out, prev, zchunk);
+    k_pres_msweep<K><<<dim3(gx, gy, nchunk), dim3(MS_TX, MS_TY), smem, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
+                                                                              in, out, prev, zchunk);
 }
 
 void launch_msweep(wf_solver* h, int k, const float* rhs, const float* in, float* out, float* prev) {

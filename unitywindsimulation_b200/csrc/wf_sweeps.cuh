@@ -5,6 +5,10 @@
 
 namespace wf {
 
+// Per-device kernel attributes of the sweep kernels; call once per device
+// before the first launch.
+int sweeps_setup();
+
 // n sweeps of CSVelPredict with the VelPredict buffer rotation
 // (FvmSolverGpu.cs:1244-1279): on return vb[iF] holds iterate n and vb[iI]
 // iterate n-1, exactly as after the reference loop.
