@@ -531,6 +531,7 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     };
     if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(WF_ERR_CUDA);
     if (wf::sweeps_setup() != WF_OK) return fail(WF_ERR_CUDA);
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) return fail(WF_ERR_CUDA);
     const size_t N = P.N, v = 3 * sizeof(float) * N, sc = sizeof(float) * N;
     size_t planes = 0;

@@ -537,15 +537,24 @@ void launch_pres_sweep_fast(wf_solver* h, const float* rhs, const float* src, fl
 
 namespace {
 
+// z chunking of the wavefront kernels (one resident block per SM): as many
+// chunks as fit one wave of blocks on the device's SMs, so no SM runs a
+// second, partly empty wave; each chunk re-reads 2K halo planes.
+void wave_chunks(const wf_solver* h, int blocks_xy, int K, int& zchunk, int& nchunk) {
+    const int sms = h->num_sms > 0 ? h->num_sms : 148;
+    nchunk = std::max(1, sms / std::max(blocks_xy, 1));
+    zchunk = std::max(2 * K + 2, (h->P.nz + nchunk - 1) / nchunk);
+    nchunk = (h->P.nz + zchunk - 1) / zchunk;
+}
+
 template <int K>
 void launch_vmsweep_k(wf_solver* h, const float* in, float* out, float* prev) {
     const Params& P = h->P;
     const size_t N = P.N;
     constexpr int OX = MV_TX - 2 * K, OY = MV_TY - 2 * K;
     const int gx = (P.nx + OX - 1) / OX, gy = (P.ny + OY - 1) / OY;
-    int nchunk = std::max(1, (2 * 148 + gx * gy - 1) / (gx * gy));
-    int zchunk = std::max(8, (P.nz + nchunk - 1) / nchunk);
-    nchunk = (P.nz + zchunk - 1) / zchunk;
+    int zchunk = 0, nchunk = 0;
+    wave_chunks(h, gx * gy, K, zchunk, nchunk);
     WF_COUNT_LAUNCH();
     k_vel_msweep<K><<<dim3(gx, gy, nchunk), dim3(MV_TX, MV_TY), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv,
                                                                           in, out, prev, zchunk);
@@ -635,9 +644,8 @@ void launch_msweep_k(wf_solver* h, const float* rhs, const float* in, float* out
     const size_t N = P.N;
     constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
     const int gx = (P.nx + OX - 1) / OX, gy = (P.ny + OY - 1) / OY;
-    int nchunk = std::max(1, (2 * 148 + gx * gy - 1) / (gx * gy));
-    int zchunk = std::max(8, (P.nz + nchunk - 1) / nchunk);
-    nchunk = (P.nz + zchunk - 1) / zchunk;
+    int zchunk = 0, nchunk = 0;
+    wave_chunks(h, gx * gy, K, zchunk, nchunk);
     const size_t smem = pres_msweep_smem(K);
     WF_COUNT_LAUNCH();
     k_pres_msweep<K><<<dim3(gx, gy, nchunk), dim3(MS_TX, MS_TY), smem, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
