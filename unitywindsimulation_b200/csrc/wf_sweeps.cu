@@ -250,227 +250,297 @@ __global__ void __launch_bounds__(256) k_pres_sweep1(const __grid_constant__ Par
 // 20 B) and the input iterate (4 B) once, the output iterate (4 B) once,
 // against 28 B per sweep for one sweep per launch.
 constexpr int MS_TX = 32, MS_TY = 32;
-constexpr size_t pres_msweep_smem(int K) { return sizeof(float) * MS_TX * MS_TY * (2 * K + 2 * (K + 1)); }
+constexpr size_t pres_msweep_smem(int K) { return sizeof(float) * MS_TX * MS_TY * (2 * K + 2 * 6); }
+
+template <int K>
+struct PresWave {
+    static_assert(K >= 1 && K <= 4, "ring of 6 planes holds K <= 4");
+    static constexpr int R = 6;  // ring period: unrolled z steps per loop trip
+    float (*V)[2][MS_TY][MS_TX];
+    float (*CE)[MS_TY][MS_TX];
+    float (*CN)[MS_TY][MS_TX];
+    const float* __restrict__ pin;
+    const float* __restrict__ cE;
+    const float* __restrict__ cN;
+    const float* __restrict__ cU;
+    const float* __restrict__ ai;
+    const float* __restrict__ rh;
+    float* __restrict__ pout;
+    float* __restrict__ pprev;
+    int tx, ty, xe, xw, yn, ys, col, sxy, nz, zs, z0, z1, T;
+    bool inxy, out_col;
+    float h[K + 1][3];           // level values, ring of the last 3 planes
+    float qa[R], qr[R], qu[R];   // 1/Dp, rhs, c_U of the last R planes
+    float pv, pe, pn, pu;        // prefetched input value and c_E, c_N, c_U
+
+    __device__ __forceinline__ void fetch(int p, float& a, float& r) {
+        if (inxy && p >= 0 && p < nz) {
+            const int i = p * sxy + col;
+            pv = pin ? __ldg(pin + i) : 0.f;
+            pe = __ldg(cE + i);
+            pn = __ldg(cN + i);
+            pu = __ldg(cU + i);
+            a = __ldg(ai + i);
+            r = __ldg(rh + i);
+        } else {
+            pv = pe = pn = pu = a = r = 0.f;
+        }
+    }
+
+    template <int PH>
+    __device__ __forceinline__ void step(int t) {
+        if (t >= T) return;  // uniform over the block
+        constexpr int cur = PH & 1, prv = cur ^ 1;
+        constexpr int h0 = PH % 3, hm1 = (PH + 2) % 3, hm2 = (PH + 1) % 3;
+        // plane zs + t (fetched one step ago) enters level 0 and the rings
+        h[0][h0] = pv;
+        V[0][cur][ty][tx] = pv;
+        CE[PH][ty][tx] = pe;
+        CN[PH][ty][tx] = pn;
+        qu[PH] = pu;
+        // prefetch plane zs + t + 1
+        fetch(zs + t + 1, qa[(PH + 1) % R], qr[(PH + 1) % R]);
+#pragma unroll
+        for (int s = 1; s <= K; ++s) {
+            if (ty >= s && ty < MS_TY - s) {  // rows this level must produce
+                const int rs = (PH - s + 2 * R) % R;
+                const int rd = (PH - s - 1 + 2 * R) % R;
+                const float(*L)[MS_TX] = V[s - 1][prv];
+                float acc = -(CE[rs][ty][tx] * L[ty][xe]);
+                acc -= CE[rs][ty][xw] * L[ty][xw];
+                acc -= CN[rs][ty][tx] * L[yn][tx];
+                acc -= CN[rs][ys][tx] * L[ys][tx];
+                acc -= qu[rs] * h[s - 1][h0];
+                acc -= qu[rd] * h[s - 1][hm2];
+                const float v = qa[rs] * (acc + qr[rs]);
+                if (s == K) {
+                    const int p = zs + t - K;
+                    if (out_col && p >= z0 && p < z1 && qa[rs] != 0.f) {
+                        const int i = p * sxy + col;
+                        pout[i] = v;
+                        if (pprev) pprev[i] = h[K - 1][hm1];
+                    }
+                }
+                h[s][h0] = v;
+                if (s < K) V[s][cur][ty][tx] = v;
+            }
+        }
+        __syncthreads();
+    }
+};
 
 template <int K>
 __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
     k_pres_msweep(const __grid_constant__ Params P, const float* __restrict__ c3, const float* __restrict__ ainv,
                   const float* __restrict__ rhs, const float* __restrict__ pin, float* __restrict__ pout,
                   float* __restrict__ pprev, int zchunk) {
-    // dynamic shared memory (above the 48 KB static limit for K >= 3):
-    // V[K][2][TY][TX] level planes, CE/CN[K+1][TY][TX] coefficient rings
+    // dynamic shared memory: V[K][2][TY][TX] level planes, CE/CN[6][TY][TX]
+    // coefficient rings
     extern __shared__ float msm[];
-    float(*V)[2][MS_TY][MS_TX] = reinterpret_cast<float(*)[2][MS_TY][MS_TX]>(msm);
-    float(*CE)[MS_TY][MS_TX] = reinterpret_cast<float(*)[MS_TY][MS_TX]>(msm + K * 2 * MS_TY * MS_TX);
-    float(*CN)[MS_TY][MS_TX] = CE + (K + 1);
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    PresWave<K> w;
+    w.V = reinterpret_cast<float(*)[2][MS_TY][MS_TX]>(msm);
+    w.CE = reinterpret_cast<float(*)[MS_TY][MS_TX]>(msm + K * 2 * MS_TY * MS_TX);
+    w.CN = w.CE + PresWave<K>::R;
+    w.tx = threadIdx.x;
+    w.ty = threadIdx.y;
     constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
-    const int x = blockIdx.x * OX - K + tx;
-    const int y = blockIdx.y * OY - K + ty;
-    const int z0 = blockIdx.z * zchunk;
-    const int z1 = min(z0 + zchunk, P.nz);
-    const bool inxy = x >= 0 && x < P.nx && y >= 0 && y < P.ny;
-    const bool out_col = inxy && tx >= K && tx < MS_TX - K && ty >= K && ty < MS_TY - K;
-    const size_t N = P.N;
-    const int sxy = P.nx * P.ny;
-    const int col = inxy ? y * P.nx + x : 0;
-    const float* cEg = c3;
-    const float* cNg = c3 + N;
-    const float* cUg = c3 + 2 * N;
-    const int xe = min(tx + 1, MS_TX - 1), xw = max(tx - 1, 0);
-    const int yn = min(ty + 1, MS_TY - 1), ys = max(ty - 1, 0);
-
+    const int x = blockIdx.x * OX - K + w.tx;
+    const int y = blockIdx.y * OY - K + w.ty;
+    w.z0 = blockIdx.z * zchunk;
+    w.z1 = min(w.z0 + zchunk, P.nz);
+    w.nz = P.nz;
+    w.inxy = x >= 0 && x < P.nx && y >= 0 && y < P.ny;
+    w.out_col = w.inxy && w.tx >= K && w.tx < MS_TX - K && w.ty >= K && w.ty < MS_TY - K;
+    w.sxy = P.nx * P.ny;
+    w.col = w.inxy ? y * P.nx + x : 0;
+    w.cE = c3;
+    w.cN = c3 + P.N;
+    w.cU = c3 + 2 * (size_t)P.N;
+    w.ai = ainv;
+    w.rh = rhs;
+    w.pin = pin;
+    w.pout = pout;
+    w.pprev = pprev;
+    w.xe = min(w.tx + 1, MS_TX - 1);
+    w.xw = max(w.tx - 1, 0);
+    w.yn = min(w.ty + 1, MS_TY - 1);
+    w.ys = max(w.ty - 1, 0);
 #pragma unroll
-    for (int s = 0; s < K; ++s) V[s][0][ty][tx] = V[s][1][ty][tx] = 0.f;
+    for (int s = 0; s < K; ++s) w.V[s][0][w.ty][w.tx] = w.V[s][1][w.ty][w.tx] = 0.f;
 #pragma unroll
-    for (int s = 0; s <= K; ++s) CE[s][ty][tx] = CN[s][ty][tx] = 0.f;
-    float h[K + 1][3];
-    float qa[K + 1], qr[K + 1], qu[K + 2];
-#pragma unroll
-    for (int s = 0; s <= K; ++s) h[s][0] = h[s][1] = h[s][2] = qa[s] = qr[s] = 0.f;
-#pragma unroll
-    for (int s = 0; s < K + 2; ++s) qu[s] = 0.f;
-
-    const int zs = z0 - K;
-    const int T = (z1 - z0) + 2 * K;
-    float pv = 0.f, pe = 0.f, pn = 0.f, pu = 0.f, pa = 0.f, pr = 0.f;
-    {
-        const int p = zs;
-        if (inxy && p >= 0 && p < P.nz) {
-            const int i = p * sxy + col;
-            pv = pin ? __ldg(pin + i) : 0.f;
-            pe = __ldg(cEg + i); pn = __ldg(cNg + i); pu = __ldg(cUg + i);
-            pa = __ldg(ainv + i); pr = __ldg(rhs + i);
-        }
+    for (int r = 0; r < PresWave<K>::R; ++r) {
+        w.CE[r][w.ty][w.tx] = w.CN[r][w.ty][w.tx] = 0.f;
+        w.qa[r] = w.qr[r] = w.qu[r] = 0.f;
     }
+#pragma unroll
+    for (int s = 0; s <= K; ++s) w.h[s][0] = w.h[s][1] = w.h[s][2] = 0.f;
+    w.zs = w.z0 - K;
+    w.T = (w.z1 - w.z0) + 2 * K;
+    w.fetch(w.zs, w.qa[0], w.qr[0]);
     __syncthreads();
-    for (int t = 0; t < T; ++t) {
-        const int cur = t & 1, prv = cur ^ 1;
-        // prefetch step t+1
-        float nv = 0.f, ne = 0.f, nn = 0.f, nu = 0.f, na = 0.f, nr = 0.f;
-        {
-            const int p = zs + t + 1;
-            if (inxy && p >= 0 && p < P.nz && t + 1 < T) {
-                const int i = p * sxy + col;
-                nv = pin ? __ldg(pin + i) : 0.f;
-                ne = __ldg(cEg + i); nn = __ldg(cNg + i); nu = __ldg(cUg + i);
-                na = __ldg(ainv + i); nr = __ldg(rhs + i);
-            }
-        }
-        // level 0 and the coefficients of plane zs + t
-        h[0][0] = h[0][1]; h[0][1] = h[0][2]; h[0][2] = pv;
-        V[0][cur][ty][tx] = pv;
-        const int cw = t % (K + 1);
-        CE[cw][ty][tx] = pe;
-        CN[cw][ty][tx] = pn;
-#pragma unroll
-        for (int s = K; s > 0; --s) { qa[s] = qa[s - 1]; qr[s] = qr[s - 1]; }
-        qa[0] = pa; qr[0] = pr;
-#pragma unroll
-        for (int s = K + 1; s > 0; --s) qu[s] = qu[s - 1];
-        qu[0] = pu;
-#pragma unroll
-        for (int s = 1; s <= K; ++s) {
-            const int rs = (t - s + K + 1) % (K + 1);
-            const float(*L)[MS_TX] = V[s - 1][prv];
-            float acc = -(CE[rs][ty][tx] * L[ty][xe]);
-            acc -= CE[rs][ty][xw] * L[ty][xw];
-            acc -= CN[rs][ty][tx] * L[yn][tx];
-            acc -= CN[rs][ys][tx] * L[ys][tx];
-            acc -= qu[s] * h[s - 1][2];
-            acc -= qu[s + 1] * h[s - 1][0];
-            const float v = qa[s] * (acc + qr[s]);
-            if (s == K) {
-                const int p = zs + t - K;
-                if (out_col && p >= z0 && p < z1 && qa[K] != 0.f) {
-                    const int i = p * sxy + col;
-                    pout[i] = v;
-                    if (pprev) pprev[i] = h[K - 1][1];
-                }
-            }
-            h[s][0] = h[s][1]; h[s][1] = h[s][2]; h[s][2] = v;
-            if (s < K) V[s][cur][ty][tx] = v;
-        }
-        __syncthreads();
-        pv = nv; pe = ne; pn = nn; pu = nu; pa = na; pr = nr;
+    for (int t = 0; t < w.T; t += PresWave<K>::R) {
+        w.template step<0>(t);
+        w.template step<1>(t + 1);
+        w.template step<2>(t + 2);
+        w.template step<3>(t + 3);
+        w.template step<4>(t + 4);
+        w.template step<5>(t + 5);
     }
 }
 
 // K momentum sweeps per pass: the same wavefront for the three velocity
-// components on a 32 x 16 tile (three components need three times the
-// registers per level).  All 12 coefficient planes (A_E..A_D, 1/D, b) are
-// the own column's, so they ride in register queues.  Per pass and cell the
-// coefficients (48 B) and the input iterate (12 B) are read once and the
-// output iterate (12 B) written once.
-constexpr int MV_TX = 32, MV_TY = 16;
+// components on a 32 x 32 tile.  Level planes are float4 (u, v, w, -) so a
+// neighbour costs one 128-bit shared load; the own column's 12 coefficients
+// (A_E..A_D, 1/D, b) ride in a shared ring of 3 planes as three float4.  Per
+// pass and cell the coefficients (48 B) and the input iterate (12 B) are
+// read once and the output iterate (12 B) written once.
+constexpr int MV_TX = 32, MV_TY = 32;
+constexpr int MV_RING = 3;
+constexpr size_t vel_msweep_smem(int K) {
+    return sizeof(float4) * MV_TX * MV_TY * (2 * K + 3 * MV_RING);
+}
+
+template <int K>
+struct VelWave {
+    static_assert(K >= 1 && K <= 2, "ring of 3 planes holds K <= 2");
+    float4 (*V)[2][MV_TY][MV_TX];   // level planes
+    float4 (*C)[3][MV_TY][MV_TX];   // coefficient ring [slot][part]
+    const float* __restrict__ uin;
+    const float* __restrict__ A;
+    const float* __restrict__ iD;
+    const float* __restrict__ bv;
+    float* __restrict__ uout;
+    float* __restrict__ uprev;
+    size_t N;
+    int tx, ty, xe, xw, yn, ys, col, sxy, nz, zs, z0, z1, T;
+    bool inxy, out_col;
+    float h[K + 1][3][3];  // [level][ring of 3 planes][component]
+    float pu[3], pc[12];   // prefetched plane
+
+    __device__ __forceinline__ void fetch(int p) {
+        if (inxy && p >= 0 && p < nz) {
+            const int i = p * sxy + col;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pu[c] = __ldg(uin + c * N + i);
+#pragma unroll
+            for (int f = 0; f < 6; ++f) pc[f] = __ldg(A + f * N + i);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pc[6 + c] = __ldg(iD + c * N + i);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pc[9 + c] = __ldg(bv + c * N + i);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pu[c] = 0.f;
+#pragma unroll
+            for (int j = 0; j < 12; ++j) pc[j] = 0.f;
+        }
+    }
+
+    template <int PH>
+    __device__ __forceinline__ void step(int t) {
+        if (t >= T) return;
+        constexpr int cur = PH & 1, prv = cur ^ 1;
+        constexpr int h0 = PH % 3, hm1 = (PH + 2) % 3, hm2 = (PH + 1) % 3;
+        constexpr int slot = PH % MV_RING;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) h[0][h0][c] = pu[c];
+        V[0][cur][ty][tx] = make_float4(pu[0], pu[1], pu[2], 0.f);
+        C[slot][0][ty][tx] = make_float4(pc[0], pc[1], pc[2], pc[3]);
+        C[slot][1][ty][tx] = make_float4(pc[4], pc[5], pc[6], pc[7]);
+        C[slot][2][ty][tx] = make_float4(pc[8], pc[9], pc[10], pc[11]);
+        fetch(zs + t + 1);
+#pragma unroll
+        for (int s = 1; s <= K; ++s) {
+            if (ty >= s && ty < MV_TY - s) {
+                const int rs = (PH - s + 2 * MV_RING) % MV_RING;
+                const float4 c0 = C[rs][0][ty][tx], c1 = C[rs][1][ty][tx], c2 = C[rs][2][ty][tx];
+                const float4 e = V[s - 1][prv][ty][xe], w = V[s - 1][prv][ty][xw];
+                const float4 n = V[s - 1][prv][yn][tx], so = V[s - 1][prv][ys][tx];
+                const float eu[3] = {e.x, e.y, e.z}, wu[3] = {w.x, w.y, w.z};
+                const float nu[3] = {n.x, n.y, n.z}, su[3] = {so.x, so.y, so.z};
+                const float idg[3] = {c1.z, c1.w, c2.x}, bb[3] = {c2.y, c2.z, c2.w};
+                float v[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    float acc = c0.x * eu[c];
+                    acc += c0.y * wu[c];
+                    acc += c0.z * nu[c];
+                    acc += c0.w * su[c];
+                    acc += c1.x * h[s - 1][h0][c];
+                    acc += c1.y * h[s - 1][hm2][c];
+                    v[c] = idg[c] * (acc + bb[c]);
+                }
+                if (s == K) {
+                    const int p = zs + t - K;
+                    if (out_col && p >= z0 && p < z1 && idg[0] != 0.f) {
+                        const int i = p * sxy + col;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            uout[c * N + i] = v[c];
+                            if (uprev) uprev[c * N + i] = h[K - 1][hm1][c];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) h[s][h0][c] = v[c];
+                if (s < K) V[s][cur][ty][tx] = make_float4(v[0], v[1], v[2], 0.f);
+            }
+        }
+        __syncthreads();
+    }
+};
 
 template <int K>
 __global__ void __launch_bounds__(MV_TX* MV_TY, 1)
     k_vel_msweep(const __grid_constant__ Params P, const float* __restrict__ A, const float* __restrict__ iD,
                  const float* __restrict__ bv, const float* __restrict__ uin, float* __restrict__ uout,
                  float* __restrict__ uprev, int zchunk) {
-    __shared__ float V[K][2][3][MV_TY][MV_TX];
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    extern __shared__ float4 vsm[];
+    VelWave<K> w;
+    w.V = reinterpret_cast<float4(*)[2][MV_TY][MV_TX]>(vsm);
+    w.C = reinterpret_cast<float4(*)[3][MV_TY][MV_TX]>(vsm + K * 2 * MV_TY * MV_TX);
+    w.tx = threadIdx.x;
+    w.ty = threadIdx.y;
     constexpr int OX = MV_TX - 2 * K, OY = MV_TY - 2 * K;
-    const int x = blockIdx.x * OX - K + tx;
-    const int y = blockIdx.y * OY - K + ty;
-    const int z0 = blockIdx.z * zchunk;
-    const int z1 = min(z0 + zchunk, P.nz);
-    const bool inxy = x >= 0 && x < P.nx && y >= 0 && y < P.ny;
-    const bool out_col = inxy && tx >= K && tx < MV_TX - K && ty >= K && ty < MV_TY - K;
-    const size_t N = P.N;
-    const int sxy = P.nx * P.ny;
-    const int col = inxy ? y * P.nx + x : 0;
-    const int xe = min(tx + 1, MV_TX - 1), xw = max(tx - 1, 0);
-    const int yn = min(ty + 1, MV_TY - 1), ys = max(ty - 1, 0);
-
+    const int x = blockIdx.x * OX - K + w.tx;
+    const int y = blockIdx.y * OY - K + w.ty;
+    w.z0 = blockIdx.z * zchunk;
+    w.z1 = min(w.z0 + zchunk, P.nz);
+    w.nz = P.nz;
+    w.N = P.N;
+    w.inxy = x >= 0 && x < P.nx && y >= 0 && y < P.ny;
+    w.out_col = w.inxy && w.tx >= K && w.tx < MV_TX - K && w.ty >= K && w.ty < MV_TY - K;
+    w.sxy = P.nx * P.ny;
+    w.col = w.inxy ? y * P.nx + x : 0;
+    w.uin = uin; w.A = A; w.iD = iD; w.bv = bv; w.uout = uout; w.uprev = uprev;
+    w.xe = min(w.tx + 1, MV_TX - 1);
+    w.xw = max(w.tx - 1, 0);
+    w.yn = min(w.ty + 1, MV_TY - 1);
+    w.ys = max(w.ty - 1, 0);
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int s = 0; s < K; ++s)
+    for (int s = 0; s < K; ++s) w.V[s][0][w.ty][w.tx] = w.V[s][1][w.ty][w.tx] = z4;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) V[s][0][c][ty][tx] = V[s][1][c][ty][tx] = 0.f;
-    float h[K + 1][3][3];
-    float qc[K + 1][12];  // A_E..A_D, 1/D x3, b x3 of planes zs+t, zs+t-1, ...
+    for (int r = 0; r < MV_RING; ++r)
 #pragma unroll
-    for (int s = 0; s <= K; ++s) {
+        for (int q = 0; q < 3; ++q) w.C[r][q][w.ty][w.tx] = z4;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) h[s][c][0] = h[s][c][1] = h[s][c][2] = 0.f;
+    for (int s = 0; s <= K; ++s)
 #pragma unroll
-        for (int j = 0; j < 12; ++j) qc[s][j] = 0.f;
-    }
-    const int zs = z0 - K;
-    const int T = (z1 - z0) + 2 * K;
-    float pv[3], pc[12];
-    auto load = [&](int p, bool ok, float v[3], float c[12]) {
-        if (ok && inxy && p >= 0 && p < P.nz) {
-            const int i = p * sxy + col;
+        for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) v[k] = __ldg(uin + k * N + i);
-#pragma unroll
-            for (int f = 0; f < 6; ++f) c[f] = __ldg(A + f * N + i);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) c[6 + k] = __ldg(iD + k * N + i);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) c[9 + k] = __ldg(bv + k * N + i);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) v[k] = 0.f;
-#pragma unroll
-            for (int j = 0; j < 12; ++j) c[j] = 0.f;
-        }
-    };
-    load(zs, true, pv, pc);
+            for (int c = 0; c < 3; ++c) w.h[s][r][c] = 0.f;
+    w.zs = w.z0 - K;
+    w.T = (w.z1 - w.z0) + 2 * K;
+    w.fetch(w.zs);
     __syncthreads();
-    for (int t = 0; t < T; ++t) {
-        const int cur = t & 1, prv = cur ^ 1;
-        float nv[3], nc[12];
-        load(zs + t + 1, t + 1 < T, nv, nc);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            h[0][c][0] = h[0][c][1]; h[0][c][1] = h[0][c][2]; h[0][c][2] = pv[c];
-            V[0][cur][c][ty][tx] = pv[c];
-        }
-#pragma unroll
-        for (int s = K; s > 0; --s)
-#pragma unroll
-            for (int j = 0; j < 12; ++j) qc[s][j] = qc[s - 1][j];
-#pragma unroll
-        for (int j = 0; j < 12; ++j) qc[0][j] = pc[j];
-#pragma unroll
-        for (int s = 1; s <= K; ++s) {
-            float v[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const float(*L)[MV_TX] = V[s - 1][prv][c];
-                float acc = qc[s][0] * L[ty][xe];
-                acc += qc[s][1] * L[ty][xw];
-                acc += qc[s][2] * L[yn][tx];
-                acc += qc[s][3] * L[ys][tx];
-                acc += qc[s][4] * h[s - 1][c][2];
-                acc += qc[s][5] * h[s - 1][c][0];
-                v[c] = qc[s][6 + c] * (acc + qc[s][9 + c]);
-            }
-            if (s == K) {
-                const int p = zs + t - K;
-                if (out_col && p >= z0 && p < z1 && qc[K][6] != 0.f) {
-                    const int i = p * sxy + col;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        uout[c * N + i] = v[c];
-                        if (uprev) uprev[c * N + i] = h[K - 1][c][1];
-                    }
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                h[s][c][0] = h[s][c][1]; h[s][c][1] = h[s][c][2]; h[s][c][2] = v[c];
-                if (s < K) V[s][cur][c][ty][tx] = v[c];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < 3; ++c) pv[c] = nv[c];
-#pragma unroll
-        for (int j = 0; j < 12; ++j) pc[j] = nc[j];
+    for (int t = 0; t < w.T; t += 6) {
+        w.template step<0>(t);
+        w.template step<1>(t + 1);
+        w.template step<2>(t + 2);
+        w.template step<3>(t + 3);
+        w.template step<4>(t + 4);
+        w.template step<5>(t + 5);
     }
 }
 
@@ -556,15 +626,14 @@ void launch_vmsweep_k(wf_solver* h, const float* in, float* out, float* prev) {
     int zchunk = 0, nchunk = 0;
     wave_chunks(h, gx * gy, K, zchunk, nchunk);
     WF_COUNT_LAUNCH();
-    k_vel_msweep<K><<<dim3(gx, gy, nchunk), dim3(MV_TX, MV_TY), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv,
-                                                                          in, out, prev, zchunk);
+    k_vel_msweep<K><<<dim3(gx, gy, nchunk), dim3(MV_TX, MV_TY), vel_msweep_smem(K), h->st>>>(
+        P, h->vcoef, h->vcoef + 6 * N, h->bv, in, out, prev, zchunk);
 }
 
 void launch_vmsweep(wf_solver* h, int k, const float* in, float* out, float* prev) {
     switch (k) {
         case 1: launch_vmsweep_k<1>(h, in, out, prev); break;
-        case 2: launch_vmsweep_k<2>(h, in, out, prev); break;
-        default: launch_vmsweep_k<3>(h, in, out, prev); break;
+        default: launch_vmsweep_k<2>(h, in, out, prev); break;
     }
 }
 
@@ -580,12 +649,16 @@ int sweeps_setup() {
         e = cudaFuncSetAttribute(k_pres_msweep<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(3));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_pres_msweep<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(4));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_vel_msweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_msweep_smem(1));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_vel_msweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_msweep_smem(2));
     return e == cudaSuccess ? WF_OK : WF_ERR_CUDA;
 }
 
 int vel_sweeps_fast(wf_solver* h, int n) {
     vel_coef(h);
-    const int kmax = std::min(std::max(h->vel_k, 1), 3);
+    const int kmax = std::min(std::max(h->vel_k, 1), 2);
     if (kmax > 1) {
         // Passes of up to kmax sweeps over buffers other than velFieldLastTime;
         // the last pass also writes iterate n-1 (the reference's
@@ -741,7 +814,7 @@ int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float total = 0.f;
-    const int kv = std::min(std::max(h->vel_k, 1), 3), kp = std::min(std::max(h->pres_k, 1), 4);
+    const int kv = std::min(std::max(h->vel_k, 1), 2), kp = std::min(std::max(h->pres_k, 1), 4);
     for (int r = 0; r < reps; ++r) {
         if (flush) k_flush_read<<<148 * 4, 512, 0, h->st>>>((const float4*)fbuf, flush_bytes / 16, (float*)fbuf);
         cudaEventRecord(e0, h->st);
