@@ -57,8 +57,8 @@ struct wf_solver {
     float res_vel = -1.f, res_pres = -1.f;
     float last_ms = 0.f;
     int fast = 1;             // use the fast Jacobi kernels (wf_sweeps.cu)
-    int pres_k = 3;           // pressure sweeps per multi-sweep pass (1..4)
-    int vel_k = 2;            // momentum sweeps per multi-sweep pass (1..2)
+    int pres_k = 4;           // pressure sweeps per multi-sweep pass (1..4)
+    int vel_k = 1;            // momentum sweeps per multi-sweep pass (1..2)
     int num_sms = 148;        // multiprocessors of the device
     bool in_step = false;     // inside wf_step: skip iterates no later kernel reads
     long long launches = 0;   // kernels launched by wf_step
