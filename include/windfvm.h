@@ -278,6 +278,34 @@ enum { WF_KERNEL_PRES_SWEEP = 0, WF_KERNEL_VEL_SWEEP = 1 };
 int wf_time_kernel(wf_solver* h, int kernel, int reps, int flush_l2, float* ms_per_launch,
                    double* alg_bytes_per_launch, int* sweeps_per_launch);
 
+/* ---- allocation-free residual --------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory: an engine or visualiser plugin whose GPU memory belongs to
+ * the host application, a real-time loop that cannot afford cudaMalloc's
+ * implicit device synchronisation, a process with a locked-down allocator.
+ *
+ * Computes the reference's continuity residual, sqrt(sum (Dp*(p'-p'_last))^2
+ * / n) (CSComputePresCorrectResidual + host normalisation), of caller-owned
+ * device arrays of n_cells floats; d_pc_last may be NULL (all-zero iterate).
+ * `stream` is a cudaStream_t (NULL: the legacy default stream); the call
+ * returns after that stream has finished the reduction, with the norm in
+ * *out (host memory).
+ *
+ * Scratch: a fixed array of WF_NOALLOC_BLOCKS + 1 doubles (32 KiB + 8 B)
+ * compiled into the library; every GPU that loads the library holds it
+ * until the process exits.  The call makes no cudaMalloc/cudaFree or other
+ * allocating call.  Every call shares that array and overwrites what the
+ * previous call left there, so calls that overlap on the GPU (different
+ * streams or threads) race and must be serialised by the caller.  The first
+ * call on each device looks up the array's device address (with that device
+ * current); make that first call before any stream capture.
+ * Returns WF_ERR_INVALID_ARG for NULL inputs or when n_cells is < 1 or larger
+ * than WF_NOALLOC_MAX_CELLS, WF_ERR_CUDA when a CUDA call fails. */
+#define WF_NOALLOC_BLOCKS 4096
+#define WF_NOALLOC_MAX_CELLS (WF_NOALLOC_BLOCKS * 256 * 64) /* 67,108,864 */
+int wf_pres_residual_noalloc(const float* d_dp, const float* d_pc, const float* d_pc_last, int64_t n_cells,
+                             void* stream, float* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -161,7 +161,11 @@ _SIGNATURES = {
     "wf_last_step_ms": (c_int, [c_void_p, POINTER(c_float)]),
     "wf_kernel_launches": (c_int, [c_void_p, POINTER(c_int64)]),
     "wf_time_kernel": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_float), POINTER(c_double), POINTER(c_int)]),
+    "wf_pres_residual_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, POINTER(c_float)]),
 }
+
+NOALLOC_BLOCKS = 4096
+NOALLOC_MAX_CELLS = NOALLOC_BLOCKS * 256 * 64
 
 KERNEL_PRES_SWEEP = 0
 KERNEL_VEL_SWEEP = 1
