@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--workload", default="urban_block")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     return ap.parse_args()
 
@@ -156,6 +157,49 @@ def cpu_baseline(case, steps: int):
     return {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
             "sample": f"{steps} full steps of {case.name} ({case.n_cells} cells) after 1 warm-up step, "
                       f"FP32 oracle, OpenMP {cores} threads"}
+
+
+def batched_section(steps: int, local: int):
+    """Batched form on the 16-case direction sweep (uneven grids 96..192 x
+    48..80(up) x 96..160, wind rotated by 22.5 degree steps): the same
+    cases stepped one after another (plain form) and together in one graph
+    launch per step (batched form), both after autotuning the blocking
+    depths per grid size.  Device time from CUDA events."""
+    from unitywindsimulation_b200 import FvmSolverCuda, autotune, cases
+    from unitywindsimulation_b200.solver import BatchSolver
+
+    cs = cases.batch_directions()
+    solvers = [FvmSolverCuda(c.cfg, device=local) for c in cs]
+    for s, c in zip(solvers, cs):
+        cases.apply_case(s, c)
+    cache = os.path.join(tempfile.gettempdir(), "windfvm_autotune.json")
+    tuned = []
+    for s in solvers:
+        s.Step(1)
+        tuned.append(autotune.tune(s, cache, reps=3))
+    cells = sum(c.n_cells for c in cs)
+    for s in solvers:
+        s.Step(2)  # graph capture + warm-up
+    plain_ms = 0.0
+    for s in solvers:
+        s.Step(steps)
+        plain_ms += s.last_step_ms()
+    b = BatchSolver(solvers)
+    b.step(2)
+    l0 = b.kernel_launches()
+    b.step(steps)
+    batched_ms = b.last_step_ms()
+    launches = b.kernel_launches() - l0
+    b.close()
+    for s in solvers:
+        s.close()
+    plain = cells * steps / (plain_ms / 1e3) / 1e6
+    batched = cells * steps / (batched_ms / 1e3) / 1e6
+    return {"workload": f"batch_directions: {len(cs)} cases, {cells} cells total, grids "
+                        f"{min(c.n_cells for c in cs)}..{max(c.n_cells for c in cs)} cells, nV=50 nP=30 nC=2",
+            "plain_mcell_steps_s": plain, "batched_mcell_steps_s": batched, "batched_over_plain": batched / plain,
+            "steps": steps, "gpu_launches": launches,
+            "depths": sorted({(t["pres_k"], t["vel_k"]) for t in tuned})}
 
 
 def run_reference(args):
@@ -290,6 +334,11 @@ def run_windfvm(args):
     v_ms, v_bytes, v_sweeps = solver.time_kernel(_lib.KERNEL_VEL_SWEEP, reps=10, flush_l2=True)
     step_gbs = value / world * b_alg(cfg.vel_iters, cfg.pres_iters, cfg.piso_correctors) / 1e3
 
+    solver.close()
+    batched = None
+    if world == 1 and not args.no_batched:
+        batched = batched_section(max(3, min(args.steps, 5)), local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case, args.cpu_sample_steps)
@@ -305,9 +354,9 @@ def run_windfvm(args):
             "step_alg_gbs": step_gbs, "step_alg_frac": step_gbs / peak,
             "vel_sweep_kernel": {"ms_per_launch": v_ms, "alg_bytes_per_launch": v_bytes,
                                  "achieved_gbs": v_bytes / (v_ms / 1e3) / 1e9, "sweeps_per_launch": v_sweeps},
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

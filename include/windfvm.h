@@ -278,6 +278,32 @@ enum { WF_KERNEL_PRES_SWEEP = 0, WF_KERNEL_VEL_SWEEP = 1 };
 int wf_time_kernel(wf_solver* h, int kernel, int reps, int flush_l2, float* ms_per_launch,
                    double* alg_bytes_per_launch, int* sweeps_per_launch);
 
+/* ---- batched form ---------------------------------------------------------
+ * Several independent cases (uneven grids, wind directions, inflow speeds,
+ * building layouts) stepped together.  No counterpart in the reference,
+ * which runs one domain per solver object (a second, background domain in
+ * FvmSolverController.cs:143-151 is stepped separately, :472-480).  Every
+ * case's step graph becomes an independent branch of one CUDA graph, so one
+ * launch advances all cases by one step and the cases fill each other's idle
+ * SMs.  Results are identical to stepping each handle alone.  All handles
+ * must live on one device, use use_graph = 1 and calc_residual = 0. */
+typedef struct wf_batch wf_batch;
+int wf_batch_create(wf_solver* const* solvers, int n, wf_batch** out);
+int wf_batch_destroy(wf_batch* b);    /* the handles stay valid */
+int wf_batch_step(wf_batch* b, int n_steps);
+/* Device time of the last wf_batch_step call (CUDA events), milliseconds. */
+int wf_batch_last_step_ms(const wf_batch* b, float* ms);
+int wf_batch_kernel_launches(const wf_batch* b, int64_t* total);
+const char* wf_batch_last_error(const wf_batch* b);
+
+/* Temporal-blocking depths of the Jacobi loops: pressure sweeps per pass
+ * (1..4) and momentum sweeps per pass (1..2).  Results do not depend on
+ * them; speed does, per grid size (see the autotuner in the Python host
+ * package).  Drops the handle's captured step graphs; rebuild batches that
+ * contain the handle afterwards. */
+int wf_set_blocking(wf_solver* h, int pres_k, int vel_k);
+int wf_get_blocking(const wf_solver* h, int* pres_k, int* vel_k);
+
 /* ---- allocation-free residual --------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory: an engine or visualiser plugin whose GPU memory belongs to

@@ -88,3 +88,11 @@ def test_small_cases(seed):
     c = cases.small_case(seed=seed)
     assert cases.isolated_fluid_count(c.flags) == 0
     assert c.cfg.dt > 0
+
+
+def test_autotune_cache_roundtrip(tmp_path):
+    from unitywindsimulation_b200 import autotune
+    p = str(tmp_path / "sub" / "t.json")
+    assert autotune.load_cache(p) == {}
+    autotune.save_cache(p, {"dev|8x8x8": {"pres_k": 3, "vel_k": 1}})
+    assert autotune.load_cache(p)["dev|8x8x8"]["pres_k"] == 3

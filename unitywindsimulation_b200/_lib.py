@@ -162,6 +162,14 @@ _SIGNATURES = {
     "wf_kernel_launches": (c_int, [c_void_p, POINTER(c_int64)]),
     "wf_time_kernel": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_float), POINTER(c_double), POINTER(c_int)]),
     "wf_pres_residual_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, POINTER(c_float)]),
+    "wf_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)]),
+    "wf_batch_destroy": (c_int, [c_void_p]),
+    "wf_batch_step": (c_int, [c_void_p, c_int]),
+    "wf_batch_last_step_ms": (c_int, [c_void_p, POINTER(c_float)]),
+    "wf_batch_kernel_launches": (c_int, [c_void_p, POINTER(c_int64)]),
+    "wf_batch_last_error": (c_char_p, [c_void_p]),
+    "wf_set_blocking": (c_int, [c_void_p, c_int, c_int]),
+    "wf_get_blocking": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
 }
 
 NOALLOC_BLOCKS = 4096

@@ -111,11 +111,9 @@ int alloc(wf_solver* h, void** p, size_t bytes) {
 }
 
 void free_all(wf_solver* h) {
-    for (auto& kv : h->graphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    h->graphs.clear();
+    wf::drop_graphs(h);
     void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->vb[3], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
-                    h->pcb[0], h->pcb[1], h->pcb[2], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->part, h->dsum, h->dref,
+                    h->pcb[0], h->pcb[1], h->pcb[2], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->grad, h->part, h->dsum, h->dref,
                     h->dbad, h->stage, h->bnd[0]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -154,8 +152,8 @@ int do_les(wf_solver* h) {
     const Params& P = h->P;
     const float* uT = h->vb[h->iT];
     wf::launch_wallfunc(P, h->st, h->fl, uT, h->face);
-    wf::launch_eddy_vis(P, h->B, h->st, h->fl, uT, h->eddy);
-    wf::launch_les_term(P, h->B, h->st, h->fl, uT, h->eddy, h->face, h->bv);
+    wf::launch_eddy_vis(P, h->B, h->st, h->fl, uT, h->eddy, h->grad);
+    wf::launch_les_term(P, h->B, h->st, h->fl, uT, h->eddy, h->face, h->grad, h->bv);
     WF_CHECK_LAUNCH();
     return WF_OK;
 }
@@ -332,53 +330,11 @@ void set_roles(wf_solver* h, const wf_solver::RoleKey& k) {
 // Runs one step, replaying a cached CUDA graph when the handle is in its
 // steady state (iter_alias and pc_zero set, no residual reads).
 int run_step(wf_solver* h) {
-    const bool graphable = h->cfg.use_graph && !h->cfg.calc_residual && h->iter_alias && h->pc_zero;
-    if (!graphable) {
-        const long long l0 = wf::g_launches;
-        const int s = enqueue_step(h);
-        h->launches += wf::g_launches - l0;
-        return s;
-    }
-    const auto key = role_key(h);
-    auto it = h->graphs.find(key);
-    if (it == h->graphs.end()) {
-        cudaGraph_t g = nullptr;
-        WF_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-        const int64_t step0 = h->step;
-        const long long l0 = wf::g_launches;
-        int s = enqueue_step(h);
-        const long long nk = wf::g_launches - l0;
-        cudaError_t e = cudaStreamEndCapture(h->st, &g);
-        if (s != WF_OK) {
-            if (g) cudaGraphDestroy(g);
-            return s;
-        }
-        if (e != cudaSuccess) {
-            h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
-            return WF_ERR_CUDA;
-        }
-        wf_solver::GraphEntry ent;
-        ent.after = role_key(h);
-        ent.kernels = nk;
-        e = cudaGraphInstantiate(&ent.exec, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            h->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
-            return WF_ERR_CUDA;
-        }
-        it = h->graphs.emplace(key, ent).first;
-        // capture only recorded the work: restore and replay it
-        set_roles(h, key);
-        h->iter_alias = true;
-        h->pc_zero = true;
-        h->step = step0;
-    }
-    WF_CUDA(cudaGraphLaunch(it->second.exec, h->st));
-    set_roles(h, it->second.after);
-    h->iter_alias = true;
-    h->pc_zero = true;
-    h->step += 1;
-    h->launches += it->second.kernels;
+    if (!wf::step_graphable(h)) return wf::run_step_eager(h);
+    const wf_solver::GraphEntry* ent = nullptr;
+    WF_TRY(wf::ensure_step_graph(h, &ent));
+    WF_CUDA(cudaGraphLaunch(ent->exec, h->st));
+    wf::commit_graph_step(h, *ent);
     return WF_OK;
 }
 
@@ -430,6 +386,79 @@ float* field_ptr(wf_solver* h, int field, size_t* points, int* comps) {
 }
 
 }  // namespace
+
+namespace wf {
+
+bool step_graphable(const wf_solver* h) {
+    return h->cfg.use_graph && !h->cfg.calc_residual && h->iter_alias && h->pc_zero;
+}
+
+int run_step_eager(wf_solver* h) {
+    const long long l0 = g_launches;
+    const int s = enqueue_step(h);
+    h->launches += g_launches - l0;
+    return s;
+}
+
+int ensure_step_graph(wf_solver* h, const wf_solver::GraphEntry** out) {
+    const auto key = role_key(h);
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        WF_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        const int64_t step0 = h->step;
+        const long long l0 = g_launches;
+        const int s = enqueue_step(h);
+        const long long nk = g_launches - l0;
+        cudaError_t e = cudaStreamEndCapture(h->st, &g);
+        const auto after = role_key(h);
+        // capture only recorded the work: restore the roles it rotated
+        set_roles(h, key);
+        h->iter_alias = true;
+        h->pc_zero = true;
+        h->step = step0;
+        g_launches = l0;
+        if (s != WF_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (e != cudaSuccess) {
+            h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+            return WF_ERR_CUDA;
+        }
+        wf_solver::GraphEntry ent;
+        ent.graph = g;
+        ent.kernels = nk;
+        ent.after = after;
+        e = cudaGraphInstantiate(&ent.exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            h->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+            return WF_ERR_CUDA;
+        }
+        it = h->graphs.emplace(key, ent).first;
+    }
+    *out = &it->second;
+    return WF_OK;
+}
+
+void commit_graph_step(wf_solver* h, const wf_solver::GraphEntry& e) {
+    set_roles(h, e.after);
+    h->iter_alias = true;
+    h->pc_zero = true;
+    h->step += 1;
+    h->launches += e.kernels;
+}
+
+void drop_graphs(wf_solver* h) {
+    for (auto& kv : h->graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    h->graphs.clear();
+}
+
+}  // namespace wf
 
 // =====================================================================
 extern "C" {
@@ -548,6 +577,7 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
         (s = alloc(h, (void**)&h->Dp, sc)) ||
         (s = alloc(h, (void**)&h->bp, sc)) || (s = alloc(h, (void**)&h->eddy, sc)) ||
         (s = alloc(h, (void**)&h->pcoef, 5 * sc)) || (s = alloc(h, (void**)&h->vcoef, 9 * sc)) ||
+        (s = alloc(h, (void**)&h->grad, 9 * sc)) ||
         (s = alloc(h, (void**)&h->part, sizeof(double) * (size_t)std::max(nblk, 1))) ||
         (s = alloc(h, (void**)&h->dsum, 4 * sizeof(double))) || (s = alloc(h, (void**)&h->dref, sizeof(float) * 4)) ||
         (s = alloc(h, (void**)&h->dbad, sizeof(int) * 4)) || (s = alloc(h, (void**)&h->bnd[0], sizeof(float) * planes)))
@@ -801,13 +831,16 @@ int wf_op_wallfunc(wf_solver* h) {
 }
 int wf_op_eddy_vis(wf_solver* h) {
     WF_OP_BEGIN();
-    wf::launch_eddy_vis(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->eddy);
+    wf::launch_eddy_vis(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->eddy, nullptr);
     WF_CHECK_LAUNCH();
     return sync(h);
 }
 int wf_op_les_term(wf_solver* h) {
     WF_OP_BEGIN();
-    wf::launch_les_term(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->eddy, h->face, h->bv);
+    // the gradient tensors are rebuilt from velFieldLastTime (the eddy
+    // viscosity may have been set independently)
+    wf::launch_cell_grad(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->grad);
+    wf::launch_les_term(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->eddy, h->face, h->grad, h->bv);
     WF_CHECK_LAUNCH();
     return sync(h);
 }

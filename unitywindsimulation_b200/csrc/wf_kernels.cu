@@ -153,13 +153,22 @@ __global__ void k_wallfunc(const __grid_constant__ Params P, const uint8_t* __re
 
 // ------------------------------------------------------------------- LES
 // CSCalEddyVis, LES.compute:268-324
+// When `grad` is given, the cell-centre gradient tensor is also stored (9
+// planes, g[i][j] at plane 3i+j) for the LES term, which needs it at the cell
+// and its six neighbours.
 __global__ void k_eddy_vis(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
-                           const float* __restrict__ uT, float* __restrict__ eddy) {
+                           const float* __restrict__ uT, float* __restrict__ eddy, float* __restrict__ grad) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     if (!fluid_at(fl, c.i)) return;
     float g[3][3];
     cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
+    if (grad) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) grad[(size_t)(3 * i + j) * P.N + c.i] = g[i][j];
+    }
     const float Sxx = g[0][0], Syy = g[1][1], Szz = g[2][2];
     const float Sxy = 0.5f * (g[0][1] + g[1][0]);
     const float Syz = 0.5f * (g[1][2] + g[2][1]);
@@ -171,15 +180,41 @@ __global__ void k_eddy_vis(const __grid_constant__ Params P, const Bnd B, const 
 
 // CSCalLesDeferCorrectTerm, LES.compute:327-687.  Output: the explicit LES
 // term per momentum component (bField on the reference).
+// Gradient tensor only (for the LES term when the eddy viscosity comes from
+// elsewhere).
+__global__ void k_cell_grad(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
+                            const float* __restrict__ uT, float* __restrict__ grad) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    if (!fluid_at(fl, c.i)) return;
+    float g[3][3];
+    cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) grad[(size_t)(3 * i + j) * P.N + c.i] = g[i][j];
+}
+
+// `grad` (nullable) holds the stored gradient tensors of every fluid cell;
+// without it they are recomputed (the reference recomputes them in place,
+// LES.compute:381-616).
 __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
                            const float* __restrict__ uT, const float* __restrict__ eddy,
-                           const float* __restrict__ face, float* __restrict__ bles) {
+                           const float* __restrict__ face, const float* __restrict__ grad,
+                           float* __restrict__ bles) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     if (!fluid_at(fl, c.i)) return;
     const size_t N = P.N;
     float g[3][3];
-    cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
+    if (grad) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) g[i][j] = ld(grad, (size_t)(3 * i + j) * N + c.i);
+    } else {
+        cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
+    }
     float fg[6][3];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -187,11 +222,17 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
         const int a = face_axis(f);
         const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
         if (in_region(P, X, Y, Z)) {
-            if (fluid_at(fl, cidx(P, X, Y, Z))) {
-                float gn[3][3];
-                cell_grad(P, B, fl, uT, X, Y, Z, gn);
+            const int q = cidx(P, X, Y, Z);
+            if (fluid_at(fl, q)) {
+                if (grad) {
 #pragma unroll
-                for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + gn[a][j]);
+                    for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + ld(grad, (size_t)(3 * a + j) * N + q));
+                } else {
+                    float gn[3][3];
+                    cell_grad(P, B, fl, uT, X, Y, Z, gn);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + gn[a][j]);
+                }
             } else {
                 const float v = ld(uT, (size_t)a * N + c.i) / (0.5f * P.dx);
                 fg[f][a] = face_sign(f) > 0 ? -v : v;
@@ -809,12 +850,17 @@ int cell_grid_blocks(const Params& P) {
 void launch_wallfunc(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, float* face) {
     WF_LAUNCH(k_wallfunc, fl, uT, face);
 }
-void launch_eddy_vis(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT, float* eddy) {
-    WF_LAUNCH(k_eddy_vis, B, fl, uT, eddy);
+void launch_eddy_vis(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT, float* eddy,
+                     float* grad) {
+    WF_LAUNCH(k_eddy_vis, B, fl, uT, eddy, grad);
+}
+void launch_cell_grad(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
+                      float* grad) {
+    WF_LAUNCH(k_cell_grad, B, fl, uT, grad);
 }
 void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
-                     const float* eddy, const float* face, float* bles) {
-    WF_LAUNCH(k_les_term, B, fl, uT, eddy, face, bles);
+                     const float* eddy, const float* face, const float* grad, float* bles) {
+    WF_LAUNCH(k_les_term, B, fl, uT, eddy, face, grad, bles);
 }
 void launch_vel_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
                            const float* pr, const float* eddy, const float* face, const float* bles, float* Dv,

@@ -10,9 +10,14 @@ namespace wf {
 int cell_grid_blocks(const Params& P);
 
 void launch_wallfunc(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, float* face);
-void launch_eddy_vis(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT, float* eddy);
+// grad (nullable): 9 planes receiving / holding the cell-centre velocity
+// gradient tensors.
+void launch_eddy_vis(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT, float* eddy,
+                     float* grad);
+void launch_cell_grad(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
+                      float* grad);
 void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
-                     const float* eddy, const float* face, float* bles);
+                     const float* eddy, const float* face, const float* grad, float* bles);
 void launch_vel_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
                            const float* pr, const float* eddy, const float* face, const float* bles, float* Dv,
                            float* bv);

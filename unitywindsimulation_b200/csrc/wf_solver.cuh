@@ -44,6 +44,7 @@ struct wf_solver {
     // sweep coefficient caches of the fast path (wf_sweeps.cu)
     float* pcoef = nullptr;   // pressure: c_E, c_N, c_U, 1/Dp, PISO rhs (5 planes)
     float* vcoef = nullptr;   // momentum: A_E..A_D, 1/D (9 planes)
+    float* grad = nullptr;    // cell-centre velocity gradient tensors (9 planes)
     // scratch
     double* part = nullptr;
     double* dsum = nullptr;   // 4 doubles
@@ -67,9 +68,23 @@ struct wf_solver {
     // CUDA-graph cache of one step, keyed by the buffer roles before the step.
     using RoleKey = std::tuple<int, int, int, int, int>;
     struct GraphEntry {
+        cudaGraph_t graph = nullptr;  // kept for composition into batch graphs
         cudaGraphExec_t exec = nullptr;
         RoleKey after{};
         long long kernels = 0;
     };
     std::map<RoleKey, GraphEntry> graphs;
 };
+
+namespace wf {
+// Step-graph plumbing shared by the single-handle and the batched step.
+bool step_graphable(const wf_solver* h);
+// Captures (once per buffer-role assignment) the graph of one step from the
+// handle's current state without running it.
+int ensure_step_graph(wf_solver* h, const wf_solver::GraphEntry** out);
+// Applies the role rotation and counters of one replayed step.
+void commit_graph_step(wf_solver* h, const wf_solver::GraphEntry& e);
+// One step launched kernel by kernel on the handle's stream.
+int run_step_eager(wf_solver* h);
+void drop_graphs(wf_solver* h);
+}  // namespace wf

@@ -203,6 +203,14 @@ class FvmSolverCuda:
     def stream_ptr(self) -> int:
         return int(self.device_fields().stream or 0)
 
+    def set_blocking(self, pres_k: int, vel_k: int) -> None:
+        self._check(self._lib.wf_set_blocking(self._h, int(pres_k), int(vel_k)))
+
+    def get_blocking(self):
+        p, v = c_int(0), c_int(0)
+        self._check(self._lib.wf_get_blocking(self._h, byref(p), byref(v)))
+        return p.value, v.value
+
     # ---- per-kernel operations ----
     def op(self, name: str, *args) -> None:
         fn = getattr(self._lib, f"wf_op_{name}")
@@ -213,6 +221,53 @@ class FvmSolverCuda:
         fn = getattr(self._lib, f"wf_op_{which}_residual")
         self._check(fn(self._h, byref(out)))
         return out.value
+
+
+class BatchSolver:
+    """Several FvmSolverCuda handles stepped together by one graph launch per
+    step (wf_batch_*).  The handles stay usable on their own."""
+
+    def __init__(self, solvers):
+        self._lib = _lib.load()
+        self.solvers = list(solvers)
+        arr = (c_void_p * len(self.solvers))(*[s._h for s in self.solvers])
+        b = c_void_p()
+        st = self._lib.wf_batch_create(arr, len(self.solvers), byref(b))
+        if st != _lib.WF_OK:
+            raise WindFvmError(st, "wf_batch_create failed")
+        self._b = b
+
+    def _check(self, st):
+        if st != _lib.WF_OK:
+            raise WindFvmError(st, self._lib.wf_batch_last_error(self._b).decode())
+
+    def step(self, n_steps: int = 1) -> None:
+        self._check(self._lib.wf_batch_step(self._b, int(n_steps)))
+
+    def last_step_ms(self) -> float:
+        ms = c_float(0)
+        self._check(self._lib.wf_batch_last_step_ms(self._b, byref(ms)))
+        return ms.value
+
+    def kernel_launches(self) -> int:
+        n = c_int64(0)
+        self._check(self._lib.wf_batch_kernel_launches(self._b, byref(n)))
+        return n.value
+
+    @property
+    def n_cells(self) -> int:
+        return sum(s.n_cells for s in self.solvers)
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.wf_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # Reference-style name for the solver class.
