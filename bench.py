@@ -185,7 +185,8 @@ def batched_section(steps: int, local: int):
         s.Step(steps)
         plain_ms += s.last_step_ms()
     b = BatchSolver(solvers)
-    b.step(2)
+    width = autotune.tune_batch(b, steps=2)
+    b.step(1)
     l0 = b.kernel_launches()
     b.step(steps)
     batched_ms = b.last_step_ms()
@@ -199,7 +200,7 @@ def batched_section(steps: int, local: int):
                         f"{min(c.n_cells for c in cs)}..{max(c.n_cells for c in cs)} cells, nV=50 nP=30 nC=2",
             "plain_mcell_steps_s": plain, "batched_mcell_steps_s": batched, "batched_over_plain": batched / plain,
             "steps": steps, "gpu_launches": launches,
-            "depths": sorted({(t["pres_k"], t["vel_k"]) for t in tuned})}
+            "depths": sorted({(t["pres_k"], t["vel_k"]) for t in tuned}), "width": width}
 
 
 def run_reference(args):

@@ -295,6 +295,11 @@ int wf_batch_step(wf_batch* b, int n_steps);
 int wf_batch_last_step_ms(const wf_batch* b, float* ms);
 int wf_batch_kernel_launches(const wf_batch* b, int64_t* total);
 const char* wf_batch_last_error(const wf_batch* b);
+/* Cases are dealt round-robin onto `width` chains that run concurrently; the
+ * cases of one chain run one after another inside the same launch.  0
+ * (default) = every case its own chain; 1 = all cases in sequence (keeps
+ * each case's working set in L2 while it runs).  Speed only. */
+int wf_batch_set_width(wf_batch* b, int width);
 
 /* Temporal-blocking depths of the Jacobi loops: pressure sweeps per pass
  * (1..4) and momentum sweeps per pass (1..2).  Results do not depend on

@@ -36,6 +36,22 @@ def test_batched_step_equals_individual_steps(built):
         assert a.get_state()[2] == s.get_state()[2] == 4
 
 
+@pytest.mark.parametrize("width", [1, 2, 0])
+def test_batch_width_does_not_change_results(built, width):
+    cs = _small_batch()
+    alone = [FvmSolverCuda(c.cfg) for c in cs]
+    batch = [FvmSolverCuda(c.cfg) for c in cs]
+    for s, c in zip(alone + batch, cs + cs):
+        s.InitFlags(c.flags)
+    for s in alone:
+        s.Step(3)
+    b = BatchSolver(batch)
+    b.set_width(width)
+    b.step(3)
+    for a, s in zip(alone, batch):
+        np.testing.assert_array_equal(a.GetVelField(), s.GetVelField())
+
+
 def test_batched_cases_match_oracle(built):
     cs = _small_batch()[:2]
     gs = [FvmSolverCuda(c.cfg) for c in cs]

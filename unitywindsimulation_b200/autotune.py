@@ -49,6 +49,24 @@ def save_cache(path: str, cache: dict) -> None:
     os.replace(tmp, path)
 
 
+def tune_batch(batch, widths=(1, 2, 4, 0), steps: int = 2) -> dict:
+    """Picks the concurrency width of a BatchSolver (cases per concurrent
+    chain) by timing `steps` batched steps per candidate; leaves the batch
+    on the fastest.  The timed steps advance the cases."""
+    best = None
+    times = {}
+    for w in widths:
+        batch.set_width(w)
+        batch.step(1)  # capture
+        batch.step(steps)
+        ms = batch.last_step_ms() / steps
+        times[w] = ms
+        if best is None or ms < times[best]:
+            best = w
+    batch.set_width(best)
+    return {"width": best, "ms_per_step": times}
+
+
 def tune(solver, cache_path: str | None = DEFAULT_CACHE, reps: int = 5, device_name: str | None = None) -> dict:
     """Picks and applies the fastest blocking depths for `solver`'s grid.
     Returns {"pres_k", "vel_k", "pres_us_per_sweep", "vel_us_per_sweep",

@@ -11,6 +11,7 @@
 // No block of one case waits on another, so there are no spin barriers.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
 #include <string>
 #include <vector>
@@ -24,6 +25,7 @@ struct wf_batch {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     float last_ms = 0.f;
     long long launches = 0;  // kernels launched by batched steps
+    int width = 0;           // concurrent chains of cases (0: every case its own)
     std::string err;
     struct Entry {
         cudaGraphExec_t exec = nullptr;
@@ -57,7 +59,12 @@ int ensure_batch_graph(wf_batch* b, const wf_batch::Entry** out) {
         cudaGraph_t parent = nullptr;
         if (cudaGraphCreate(&parent, 0) != cudaSuccess) return fail(b, WF_ERR_CUDA, "cudaGraphCreate failed");
         wf_batch::Entry ent;
-        for (wf_solver* h : b->s) {
+        // Cases are dealt round-robin onto `width` chains; the chains run
+        // concurrently, the cases of one chain one after another.
+        const int width = b->width > 0 ? std::min<int>(b->width, (int)b->s.size()) : (int)b->s.size();
+        std::vector<cudaGraphNode_t> tail(width, nullptr);
+        for (size_t i = 0; i < b->s.size(); ++i) {
+            wf_solver* h = b->s[i];
             const wf_solver::GraphEntry* ge = nullptr;
             const int st = wf::ensure_step_graph(h, &ge);
             if (st != WF_OK) {
@@ -65,10 +72,13 @@ int ensure_batch_graph(wf_batch* b, const wf_batch::Entry** out) {
                 return fail(b, st, "capturing a case's step failed: " + h->err);
             }
             cudaGraphNode_t node;
-            if (cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, ge->graph) != cudaSuccess) {
+            cudaGraphNode_t& prev = tail[i % width];
+            if (cudaGraphAddChildGraphNode(&node, parent, prev ? &prev : nullptr, prev ? 1 : 0, ge->graph) !=
+                cudaSuccess) {
                 cudaGraphDestroy(parent);
                 return fail(b, WF_ERR_CUDA, "cudaGraphAddChildGraphNode failed");
             }
+            prev = node;
             ent.after.push_back(ge->after);
             ent.kernels += ge->kernels;
         }
@@ -169,6 +179,16 @@ int wf_batch_last_step_ms(const wf_batch* b, float* ms) {
 }
 
 const char* wf_batch_last_error(const wf_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int wf_batch_set_width(wf_batch* b, int width) {
+    if (!b) return WF_ERR_INVALID_ARG;
+    if (width < 0) return fail(b, WF_ERR_INVALID_ARG, "width must be >= 0");
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->st);
+    destroy_graphs(b);
+    b->width = width;
+    return WF_OK;
+}
 
 int wf_batch_kernel_launches(const wf_batch* b, int64_t* total) {
     if (!b || !total) return WF_ERR_INVALID_ARG;

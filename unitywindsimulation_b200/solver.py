@@ -249,6 +249,9 @@ class BatchSolver:
         self._check(self._lib.wf_batch_last_step_ms(self._b, byref(ms)))
         return ms.value
 
+    def set_width(self, width: int) -> None:
+        self._check(self._lib.wf_batch_set_width(self._b, int(width)))
+
     def kernel_launches(self) -> int:
         n = c_int64(0)
         self._check(self._lib.wf_batch_kernel_launches(self._b, byref(n)))
