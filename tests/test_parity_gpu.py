@@ -126,6 +126,22 @@ def test_sweep_blocking_depths(built, monkeypatch, pk, vk, n):
     assert_fields(g, o, [_lib.FIELD_VEL_LAST_TIME, _lib.FIELD_PRES], tol=2 * REL_TOL, label="steps")
 
 
+@pytest.mark.parametrize("vec4", ["0", "1"])
+@pytest.mark.parametrize("nx", [40, 42])
+def test_vel_sweep_scalar_and_vector_forms(built, monkeypatch, vec4, nx):
+    """The 4-cell vector momentum sweep (nx % 4 == 0) and the one-cell form
+    give the reference's iterates."""
+    monkeypatch.setenv("WF_VEC4", vec4)
+    case = cases.small_case(nx=nx, ny=14, nz=18, seed=22)
+    g, o = make_pair(case)
+    for s in (g, o):
+        s.op("vel_precompute")
+    copy_state(o, g)
+    g.op("vel_sweeps", 6)
+    o.op("vel_sweeps", 6)
+    assert_fields(g, o, [_lib.FIELD_VEL, _lib.FIELD_VEL_LAST_ITER], label=f"vec4={vec4} nx={nx}")
+
+
 @pytest.mark.parametrize("n", [1, 5])
 def test_piso_parity(small, n):
     g, o = make_pair(small)

@@ -121,6 +121,69 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
     }
 }
 
+// One momentum sweep, four consecutive x cells per thread (nx % 4 == 0):
+// every plane is read with 128-bit loads (A_E..A_D, 1/D, b, the own and the
+// y/z-neighbour iterates), the x neighbours beyond the thread's four cells
+// with two scalar loads.  Same arithmetic per cell as k_vel_sweep1.
+__device__ __forceinline__ float4 ld4(const float* p, size_t i) { return __ldg(reinterpret_cast<const float4*>(p + i)); }
+__device__ __forceinline__ float f4(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+
+__global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Params P, const float* __restrict__ A,
+                                                    const float* __restrict__ iD, const float* __restrict__ bv,
+                                                    const float* __restrict__ ui, float* __restrict__ uo) {
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x0 >= P.nx || y >= P.ny || z >= P.nz) return;
+    const int i = cidx(P, x0, y, z);
+    const size_t N = P.N;
+    const float4 d0 = ld4(iD, i);
+    if (d0.x == 0.f && d0.y == 0.f && d0.z == 0.f && d0.w == 0.f) return;  // four non-fluid cells
+    const float4 aE = ld4(A, i), aW = ld4(A, N + i), aN = ld4(A, 2 * N + i);
+    const float4 aS = ld4(A, 3 * N + i), aU = ld4(A, 4 * N + i), aD = ld4(A, 5 * N + i);
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const bool hn = y + 1 < P.ny, hs = y > 0, hu = z + 1 < P.nz, hd = z > 0;
+    const bool he = x0 + 4 < P.nx, hw = x0 > 0;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float* u = ui + k * N;
+        const float4 c = ld4(u, i);
+        const float4 n = hn ? ld4(u, i + sx) : zero4;
+        const float4 s = hs ? ld4(u, i - sx) : zero4;
+        const float4 up = hu ? ld4(u, i + sz) : zero4;
+        const float4 dn = hd ? ld4(u, i - sz) : zero4;
+        const float e3 = he ? __ldg(u + i + 4) : 0.f;
+        const float w0 = hw ? __ldg(u + i - 1) : 0.f;
+        const float4 dk = k == 0 ? d0 : ld4(iD, k * N + i);
+        const float4 bk = ld4(bv, k * N + i);
+        float r[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float ue = j < 3 ? f4(c, j + 1) : e3;
+            const float uw = j > 0 ? f4(c, j - 1) : w0;
+            float acc = f4(aE, j) * ue;
+            acc += f4(aW, j) * uw;
+            acc += f4(aN, j) * f4(n, j);
+            acc += f4(aS, j) * f4(s, j);
+            acc += f4(aU, j) * f4(up, j);
+            acc += f4(aD, j) * f4(dn, j);
+            r[j] = f4(dk, j) * (acc + f4(bk, j));
+        }
+        // non-fluid cells keep their value (the reference does not write them)
+        float* o = uo + k * N + i;
+        const float4 old = (f4(d0, 0) == 0.f || f4(d0, 1) == 0.f || f4(d0, 2) == 0.f || f4(d0, 3) == 0.f)
+                               ? __ldg(reinterpret_cast<const float4*>(o))
+                               : zero4;
+        float4 outv;
+        outv.x = d0.x != 0.f ? r[0] : old.x;
+        outv.y = d0.y != 0.f ? r[1] : old.y;
+        outv.z = d0.z != 0.f ? r[2] : old.z;
+        outv.w = d0.w != 0.f ? r[3] : old.w;
+        *reinterpret_cast<float4*>(o) = outv;
+    }
+}
+
 // Pressure face coefficients c_E, c_N, c_U (FvmColl.compute:2813-2814 form
 // ((dv/den) * DInv) / dx) for fluid-fluid faces, else 0.
 __global__ void k_pres_coef(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
@@ -574,7 +637,13 @@ void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
     const Params& P = h->P;
     const size_t N = P.N;
     WF_COUNT_LAUNCH();
-    k_vel_sweep1<<<grd(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
+    if (P.nx % 4 == 0 && h->vec4) {
+        const dim3 b = blk();
+        const dim3 g((P.nx / 4 + b.x - 1) / b.x, (P.ny + b.y - 1) / b.y, (P.nz + b.z - 1) / b.z);
+        k_vel_sweep4<<<g, b, 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
+    } else {
+        k_vel_sweep1<<<grd(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
+    }
 }
 
 // Pressure coefficients of the SIMPLE (piso = false) or PISO equation;
