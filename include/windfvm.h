@@ -309,6 +309,56 @@ int wf_batch_set_width(wf_batch* b, int width);
 int wf_set_blocking(wf_solver* h, int pres_k, int vel_k);
 int wf_get_blocking(const wf_solver* h, int* pres_k, int* vel_k);
 
+/* ---- discrete adjoint ------------------------------------------------------
+ * No counterpart in the reference, which computes no derivatives.  The
+ * vector-Jacobian product of the fixed-iteration step (momentum predictor,
+ * SIMPLE correction, PISO correctors) is the same composition of maps
+ * reversed: every Jacobi sweep becomes a transposed sweep, the once-per-step
+ * maps scatter their local derivatives.  The forward step is recomputed from
+ * a stored state with every Jacobi iterate kept.
+ *
+ * Supported: turbulence = 0, calc_residual = 0, at least one fixed-pressure
+ * domain face (no normalisation), compat flag WF_COMPAT_PISO_CONSISTENT off.
+ * wf_adj_create returns WF_ERR_UNSUPPORTED otherwise.  The adjoint handle
+ * keeps a reference to `h`; destroy it before the solver. */
+typedef struct wf_adjoint wf_adjoint;
+int wf_adj_create(wf_solver* h, wf_adjoint** out);
+int wf_adj_destroy(wf_adjoint* a);
+const char* wf_adj_last_error(const wf_adjoint* a);
+
+/* One step from the solver's current state (velocity and pressure), cut
+ * after `phases` parts: 1 = momentum predictor, 2 = + SIMPLE pressure
+ * correction, 3 = + PISO correctors (the whole step).  The solver does not
+ * advance.  All arrays are host memory in the SoA layout.
+ * wf_adj_step_forward: the state after the cut (u_out 3N, p_out N).
+ * wf_adj_step_vjp: given adjoints of that output (ubar_out 3N, pbar_out N),
+ * the adjoints of the input state (ubar_in 3N, pbar_in N) and, when
+ * gbar_planes is non-NULL, of the six boundary-value planes (3 * plane
+ * points each, planes in WF_FACE_* order, as wf_field_size reports them). */
+int wf_adj_step_forward(wf_adjoint* a, int phases, float* u_out, float* p_out);
+int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const float* pbar_out, float* ubar_in,
+                    float* pbar_in, float* gbar_planes);
+
+/* Pedestrian-comfort objective: the mean over the last `window` steps of the
+ * mean squared speed |u|^2 on the fluid cells of one horizontal patch
+ * (x0 <= x < x1, z0 <= z < z1 at height index y), divided by the patch's full
+ * cell count. */
+typedef struct wf_objective {
+    int32_t x0, x1, z0, z1, y;
+    int32_t window;
+} wf_objective;
+
+/* Advances the solver n_steps steps from its current state, evaluates the
+ * objective and its derivatives with respect to the log-inflow parameters
+ * (inflow_ustar, inflow_z0; needs inflow_type = WF_INFLOW_LOG with
+ * inflow_ustar > 0).  include_init != 0 also differentiates the initial
+ * interior profile of wf_init_vel_pres_fields (the current state must be that
+ * profile).  States are stored every `checkpoint_every` steps and the others
+ * recomputed.  ms_forward / ms_total (nullable): device time of the forward
+ * pass and of the whole call. */
+int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
+                    double* J, double* dJ_dustar, double* dJ_dz0, float* ms_forward, float* ms_total);
+
 /* ---- allocation-free residual --------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory: an engine or visualiser plugin whose GPU memory belongs to

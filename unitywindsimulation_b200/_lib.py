@@ -111,6 +111,11 @@ class WfDeviceFields(ctypes.Structure):
                 ("stream", c_void_p)]
 
 
+class WfObjective(ctypes.Structure):
+    _fields_ = [("x0", c_int32), ("x1", c_int32), ("z0", c_int32), ("z1", c_int32), ("y", c_int32),
+                ("window", c_int32)]
+
+
 class WindFvmError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"windfvm status {status}: {message}")
@@ -171,6 +176,13 @@ _SIGNATURES = {
     "wf_batch_set_width": (c_int, [c_void_p, c_int]),
     "wf_set_blocking": (c_int, [c_void_p, c_int, c_int]),
     "wf_get_blocking": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
+    "wf_adj_create": (c_int, [c_void_p, POINTER(c_void_p)]),
+    "wf_adj_destroy": (c_int, [c_void_p]),
+    "wf_adj_last_error": (c_char_p, [c_void_p]),
+    "wf_adj_step_forward": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "wf_adj_step_vjp": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wf_adj_gradient": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_double), POINTER(c_double),
+                                POINTER(c_double), POINTER(c_float), POINTER(c_float)]),
 }
 
 NOALLOC_BLOCKS = 4096

@@ -1,0 +1,1026 @@
+// wf_adjoint.cu - discrete adjoint of the fixed-iteration SIMPLE/PISO step.
+//
+// No counterpart in the reference (it has no derivatives).  The forward step
+// (wf_api.cu sequencing of FvmSolverGpu.Step, LES off) is a fixed
+// composition of maps; its vector-Jacobian product is the same composition
+// reversed:
+//
+//   (D, b)   = PRE(u0, p0, g)           momentum diagonal / right-hand side
+//   (A, 1/D) = VCOEF(u0, D)             Picard coefficients of the sweep
+//   u^{k+1}  = 1/D (A u^k + b)          nV sweeps, u^0 = u0        -> u*
+//   (Dp, bp) = PPRE(u*, p0, D, g)       Rhie-Chow face-flux assembly
+//   c, 1/Dp  = PCOEF(D), 1/Dp           face coefficients
+//   q^{k+1}  = 1/Dp (bp - C q^k)        nP sweeps, q^0 = 0         -> q
+//   p1 = p0 + q,  c1 = CORR(q, D),  u1 = u* + c1
+//   per PISO corrector m: a = AOD(c_m, u0); (1/coef, r) = PISOPRE(D, a);
+//   s^{k+1} = 1/coef (r - C s^k), nP sweeps; p += s; c_{m+1} = PVEL(s, D, a);
+//   u += c_{m+1}
+//
+// Linear sweeps reverse as transposed gathers (each cell collects from its
+// neighbours, no atomics); the once-per-step maps scatter their local
+// derivatives with atomicAdd.  The forward step is re-run from its input
+// state with every Jacobi iterate kept (the "tape"), using the one-sweep
+// kernels of wf_sweeps.cu.
+//
+// Supported: turbulence off, binary obstacle mask, any boundary set,
+// SIMPLE or PISO, no compat flags that change the PISO corrector.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "wf_kernels.cuh"
+#include "wf_solver.cuh"
+#include "wf_sweeps.cuh"
+
+struct wf_adjoint;
+
+namespace wf {
+namespace {
+
+__device__ __forceinline__ float ld(const float* p, size_t i) { return __ldg(p + i); }
+__device__ __forceinline__ bool fluid_at(const uint8_t* fl, int i) { return __ldg(fl + i) == WF_CELL_FLUID; }
+__device__ __forceinline__ void aadd(float* p, float v) {
+    if (v != 0.f) atomicAdd(p, v);
+}
+
+struct Cell {
+    int x, y, z, i;
+};
+__device__ __forceinline__ bool thread_cell(const Params& P, Cell& c) {
+    c.x = blockIdx.x * blockDim.x + threadIdx.x;
+    c.y = blockIdx.y * blockDim.y + threadIdx.y;
+    c.z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (c.x >= P.nx || c.y >= P.ny || c.z >= P.nz) return false;
+    c.i = cidx(P, c.x, c.y, c.z);
+    return true;
+}
+
+// Mutable boundary planes for the adjoint of the boundary values.
+struct BndBar {
+    float* p[6];
+};
+__device__ __forceinline__ float* bnd_bar(const Params& P, const BndBar& G, int bc, int x, int y, int z, int c) {
+    return G.p[bc] + (size_t)c * P.plane[bc] + plane_idx(P, bc, x, y, z);
+}
+
+// ---------------------------------------------------------------- PISO
+// VJP of PVEL: c[a] = -(1/D_a) (aod[a] + dv/den * (pf+ - pf-)/dx), face values
+// of s averaged with fluid neighbours, else the cell's own (PisoColl.compute:
+// 294-336).
+__global__ void k_adj_pvel(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                           const float* __restrict__ cbar, const float* __restrict__ ss,
+                           const float* __restrict__ Dv, const float* __restrict__ aod, float* __restrict__ abar,
+                           float* __restrict__ ssbar, float* __restrict__ Dbar) {
+    Cell c;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float pP = ld(ss, c.i);
+    float pf[6];
+    int qn[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        qn[f] = -1;
+        pf[f] = pP;
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            if (fluid_at(fl, q)) {
+                qn[f] = q;
+                pf[f] = 0.5f * (pP + ld(ss, q));
+            }
+        }
+    }
+    float pfb[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float k = P.dv / P.den;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float w = ld(cbar, a * N + c.i);
+        if (w == 0.f) continue;
+        const float Da = ld(Dv, a * N + c.i);
+        const float grad = (pf[2 * a] - pf[2 * a + 1]) / P.dx;
+        const float K = ld(aod, a * N + c.i) + k * grad;
+        aadd(Dbar + a * N + c.i, w * K / (Da * Da));
+        aadd(abar + a * N + c.i, -w / Da);
+        const float gb = -w / Da * k / P.dx;
+        pfb[2 * a] += gb;
+        pfb[2 * a + 1] -= gb;
+    }
+    float own = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (qn[f] >= 0) {
+            own += 0.5f * pfb[f];
+            aadd(ssbar + qn[f], 0.5f * pfb[f]);
+        } else {
+            own += pfb[f];
+        }
+    }
+    aadd(ssbar + c.i, own);
+}
+
+// One reversed pressure-type sweep s^{k+1} = ai (r - C s^k): sb0 = adjoint of
+// s^k, plus the adjoints of r, ai and the face coefficients (owner cell holds
+// its E/N/U faces).  s_k == nullptr is the zero start.
+__global__ void k_adj_psweep(const __grid_constant__ Params P, const float* __restrict__ sb1,
+                             const float* __restrict__ s_k, const float* __restrict__ s_k1,
+                             const float* __restrict__ ai, const float* __restrict__ c3, float* __restrict__ sb0,
+                             float* __restrict__ c3bar, float* __restrict__ aibar, float* __restrict__ rbar) {
+    Cell c;
+    if (!thread_cell(P, c)) return;
+    const size_t N = P.N;
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const float* cE = c3;
+    const float* cN = c3 + N;
+    const float* cU = c3 + 2 * N;
+    auto w_at = [&](int q) { return ld(ai, q) * ld(sb1, q); };
+    const float wP = w_at(c.i);
+    float acc = 0.f;
+    if (c.x + 1 < P.nx) acc += ld(cE, c.i) * w_at(c.i + 1);
+    if (c.x > 0) acc += ld(cE, c.i - 1) * w_at(c.i - 1);
+    if (c.y + 1 < P.ny) acc += ld(cN, c.i) * w_at(c.i + sx);
+    if (c.y > 0) acc += ld(cN, c.i - sx) * w_at(c.i - sx);
+    if (c.z + 1 < P.nz) acc += ld(cU, c.i) * w_at(c.i + sz);
+    if (c.z > 0) acc += ld(cU, c.i - sz) * w_at(c.i - sz);
+    sb0[c.i] = -acc;
+    const float aiP = ld(ai, c.i);
+    if (aiP == 0.f) return;  // non-fluid cell: no equation
+    rbar[c.i] += wP;
+    aibar[c.i] += ld(sb1, c.i) * ld(s_k1, c.i) / aiP;
+    if (s_k) {
+        const float sP = ld(s_k, c.i);
+        if (c.x + 1 < P.nx) c3bar[c.i] += -(wP * ld(s_k, c.i + 1) + w_at(c.i + 1) * sP);
+        if (c.y + 1 < P.ny) c3bar[N + c.i] += -(wP * ld(s_k, c.i + sx) + w_at(c.i + sx) * sP);
+        if (c.z + 1 < P.nz) c3bar[2 * N + c.i] += -(wP * ld(s_k, c.i + sz) + w_at(c.i + sz) * sP);
+    }
+}
+
+// VJP of PISOPRE: coef = -sum_f (dv/den) AdInv_f / dx, ai = 1/coef,
+// r = -sum_f s_f AdInv_f Aod_f (PisoColl.compute:196-255).
+__global__ void k_adj_pisopre(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                              const float* __restrict__ aibar, const float* __restrict__ rbar,
+                              const float* __restrict__ ai, const float* __restrict__ Dv,
+                              const float* __restrict__ aod, float* __restrict__ abar, float* __restrict__ Dbar) {
+    Cell c;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float aiP = ld(ai, c.i);
+    const float coefb = -ld(aibar, c.i) * aiP * aiP;
+    const float rb = ld(rbar, c.i);
+    const float k = P.dv / P.den / P.dx;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f), s = face_sign(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float DP = ld(Dv, a * N + c.i), DQ = ld(Dv, a * N + q);
+        const float AdInv = 0.5f * (1.f / DP + 1.f / DQ);
+        const float Aod = 0.5f * (ld(aod, a * N + c.i) + ld(aod, a * N + q));
+        const float adinvb = -k * coefb - s * Aod * rb;
+        const float aodb = -s * AdInv * rb;
+        aadd(abar + a * N + c.i, 0.5f * aodb);
+        aadd(abar + a * N + q, 0.5f * aodb);
+        aadd(Dbar + a * N + c.i, -0.5f * adinvb / (DP * DP));
+        aadd(Dbar + a * N + q, -0.5f * adinvb / (DQ * DQ));
+    }
+}
+
+// VJP of the face coefficients c_f = (dv/den) 0.5 (1/D_P + 1/D_Q) / dx
+// (owner cell P holds its E/N/U faces).
+__global__ void k_adj_c3(const __grid_constant__ Params P, const float* __restrict__ c3bar,
+                         const float* __restrict__ Dv, float* __restrict__ Dbar) {
+    Cell c;
+    if (!thread_cell(P, c)) return;
+    const size_t N = P.N;
+    const float k = P.dv / P.den / P.dx;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float cb = ld(c3bar, a * N + c.i);
+        if (cb == 0.f) continue;
+        const int f = 2 * a;
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        const float DP = ld(Dv, a * N + c.i), DQ = ld(Dv, a * N + q);
+        aadd(Dbar + a * N + c.i, -0.5f * k * cb / (DP * DP));
+        aadd(Dbar + a * N + q, -0.5f * k * cb / (DQ * DQ));
+    }
+}
+
+// VJP of AOD: a_P[c] = sum_fluid f (s_f ds/4 (uT_P[a] + uT_Q[a]) - nu ds/dx) cm_Q[c]
+// (PisoColl.compute:90-177, reference nu-only diffusion).
+__global__ void k_adj_aod(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                          const float* __restrict__ abar, const float* __restrict__ cm,
+                          const float* __restrict__ uT, float* __restrict__ cmbar, float* __restrict__ uTbar) {
+    Cell c;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float ab[3] = {ld(abar, c.i), ld(abar, N + c.i), ld(abar, 2 * N + c.i)};
+    if (ab[0] == 0.f && ab[1] == 0.f && ab[2] == 0.f) return;
+    const float dif = P.nu * P.ds / P.dx;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f), s = face_sign(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float sum = ld(uT, a * N + c.i) + ld(uT, a * N + q);
+        const float coef = s * (P.ds * 0.25f * sum) - dif;
+        float t = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            aadd(cmbar + k * N + q, coef * ab[k]);
+            t += ld(cm, k * N + q) * ab[k];
+        }
+        t *= s * P.ds * 0.25f;
+        aadd(uTbar + a * N + c.i, t);
+        aadd(uTbar + a * N + q, t);
+    }
+}
+
+// Face value of a pressure-type field with the SIMPLE boundary rules
+// (FvmColl.compute:2975-3113): fluid neighbour -> average, solid neighbour ->
+// own value, domain face -> 0 for fixed pressure else own value.  Returns the
+// neighbour index that shares the face (-1 if none) and whether the face is a
+// fixed-pressure domain face.
+__device__ __forceinline__ void face_rule(const Params& P, const uint8_t* fl, const Cell& c, int f, int& q,
+                                          bool& fixed0) {
+    const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+    q = -1;
+    fixed0 = false;
+    if (in_region(P, X, Y, Z)) {
+        const int n = cidx(P, X, Y, Z);
+        if (fluid_at(fl, n)) q = n;
+    } else {
+        fixed0 = P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE;
+    }
+}
+
+// VJP of CORR (CSApplyVelCorrectionDivergenceTheorem):
+// c[a] = -(dv/den) (1/D_a) (pf+ - pf-) / dx.
+__global__ void k_adj_corr(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                           const float* __restrict__ cbar, const float* __restrict__ qf,
+                           const float* __restrict__ Dv, float* __restrict__ qbar, float* __restrict__ Dbar) {
+    Cell c;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float pP = ld(qf, c.i);
+    float pf[6];
+    int qn[6];
+    bool fx[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        face_rule(P, fl, c, f, qn[f], fx[f]);
+        pf[f] = qn[f] >= 0 ? 0.5f * (pP + ld(qf, qn[f])) : (fx[f] ? 0.f : pP);
+    }
+    float pfb[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float k = P.dv / P.den;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float w = ld(cbar, a * N + c.i);
+        if (w == 0.f) continue;
+        const float Da = ld(Dv, a * N + c.i);
+        const float K = k * (pf[2 * a] - pf[2 * a + 1]) / P.dx;
+        aadd(Dbar + a * N + c.i, w * K / (Da * Da));
+        const float g = -w * k / (Da * P.dx);
+        pfb[2 * a] += g;
+        pfb[2 * a + 1] -= g;
+    }
+    float own = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (qn[f] >= 0) {
+            own += 0.5f * pfb[f];
+            aadd(qbar + qn[f], 0.5f * pfb[f]);
+        } else if (!fx[f]) {
+            own += pfb[f];
+        }
+    }
+    aadd(qbar + c.i, own);
+}
+
+// VJP of PPRE (CSPresCorrectRhieChowPreCompute, FvmColl.compute:2481-2787).
+__global__ void k_adj_ppre(const __grid_constant__ Params P, const BndBar G,
+                           const uint8_t* __restrict__ fl, const float* __restrict__ Dpbar,
+                           const float* __restrict__ bpbar, const float* __restrict__ pr,
+                           const float* __restrict__ Dv, float* __restrict__ ubar, float* __restrict__ pbar,
+                           float* __restrict__ Dbar) {
+    Cell c;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float dpb = ld(Dpbar, c.i), bpb = ld(bpbar, c.i);
+    if (dpb == 0.f && bpb == 0.f) return;
+    const float dx2 = 2.f * P.dx;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f), s = face_sign(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            if (!fluid_at(fl, q)) continue;
+            const float DP = ld(Dv, a * N + c.i), DQ = ld(Dv, a * N + q);
+            const float DInv = 0.5f * (1.f / DP + 1.f / DQ);
+            float dinvb = -(P.dv / P.den) / P.dx * dpb;
+            // face flux 0.5 (u_P + u_Q)
+            aadd(ubar + a * N + c.i, 0.5f * s * bpb);
+            aadd(ubar + a * N + q, 0.5f * s * bpb);
+            // Rhie-Chow: vct = -(dv DInv / den) (presGrad - ave), linear in p
+            const int L = s > 0 ? c.i : q, H = s > 0 ? q : c.i;
+            const int lx = s > 0 ? c.x : X, ly = s > 0 ? c.y : Y, lz = s > 0 ? c.z : Z;
+            const int hx = s > 0 ? X : c.x, hy = s > 0 ? Y : c.y, hz = s > 0 ? Z : c.z;
+            const int ex = (a == 0), ey = (a == 1), ez = (a == 2);
+            const bool hhin = in_region(P, hx + ex, hy + ey, hz + ez);
+            const bool llin = in_region(P, lx - ex, ly - ey, lz - ez);
+            const int HH = hhin ? cidx(P, hx + ex, hy + ey, hz + ez) : -1;
+            const int LL = llin ? cidx(P, lx - ex, ly - ey, lz - ez) : -1;
+            const bool hh = hhin && fluid_at(fl, HH);
+            const bool ll = llin && fluid_at(fl, LL);
+            if (hh || ll) {
+                float wL = -1.f / P.dx, wH = 1.f / P.dx, wLL = 0.f, wHH = 0.f;
+                // subtract ave = 0.5 (gH + gL)
+                if (hh) { wHH -= 0.5f / dx2; wL += 0.5f / dx2; }
+                else { wH -= 0.5f / dx2; wL += 0.5f / dx2; }
+                if (ll) { wH -= 0.5f / dx2; wLL += 0.5f / dx2; }
+                else { wH -= 0.5f / dx2; wL += 0.5f / dx2; }
+                const float pL = ld(pr, L), pH = ld(pr, H);
+                float diff = wL * pL + wH * pH;
+                if (hh) diff += wHH * ld(pr, HH);
+                if (ll) diff += wLL * ld(pr, LL);
+                const float vctb = s * bpb;
+                dinvb += -(P.dv / P.den) * diff * vctb;
+                const float diffb = -(P.dv * DInv) / P.den * vctb;
+                aadd(pbar + L, wL * diffb);
+                aadd(pbar + H, wH * diffb);
+                if (hh) aadd(pbar + HH, wHH * diffb);
+                if (ll) aadd(pbar + LL, wLL * diffb);
+            }
+            aadd(Dbar + a * N + c.i, -0.5f * dinvb / (DP * DP));
+            aadd(Dbar + a * N + q, -0.5f * dinvb / (DQ * DQ));
+        } else {
+            const int bc = face_bc(f), vb = P.vbc[bc];
+            if (vb == WF_BND_FIXED_VALUE) {
+                aadd(bnd_bar(P, G, bc, c.x, c.y, c.z, a), s * bpb);
+            } else if (vb == WF_BND_ZERO_GRAD) {
+                aadd(ubar + a * N + c.i, s * bpb);
+            }
+            if (P.pbc[bc] == WF_BND_FIXED_VALUE) {
+                const float DP = ld(Dv, a * N + c.i);
+                aadd(Dbar + a * N + c.i, dpb * 2.f * (P.dv / P.den) / (P.dx * DP * DP));
+            }
+        }
+    }
+}
+
+// ainv = 1/Dp (fluid): Dpbar += -aibar ainv^2
+__global__ void k_adj_inv(int n, const float* __restrict__ aibar, const float* __restrict__ ai,
+                          float* __restrict__ Dpbar) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float a = ai[i];
+    if (a != 0.f) Dpbar[i] += -aibar[i] * a * a;
+}
+
+// One reversed momentum sweep u^{k+1} = iD (A u^k + b) (fluid cells; non-fluid
+// cells keep their value).  ub0 = adjoint of u^k; accumulates the adjoints of
+// A (own faces), iD and b.
+__global__ void k_adj_vsweep(const __grid_constant__ Params P, const float* __restrict__ ub1,
+                             const float* __restrict__ u_k, const float* __restrict__ u_k1,
+                             const float* __restrict__ A, const float* __restrict__ iD, float* __restrict__ ub0,
+                             float* __restrict__ Abar, float* __restrict__ iDbar, float* __restrict__ bbar) {
+    Cell c;
+    if (!thread_cell(P, c)) return;
+    const size_t N = P.N;
+    const int off[6] = {1, -1, P.nx, -P.nx, P.nx * P.ny, -P.nx * P.ny};
+    bool has[6];
+    has[0] = c.x + 1 < P.nx;
+    has[1] = c.x > 0;
+    has[2] = c.y + 1 < P.ny;
+    has[3] = c.y > 0;
+    has[4] = c.z + 1 < P.nz;
+    has[5] = c.z > 0;
+    const bool fluidP = ld(iD, c.i) != 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        // gather: neighbour P' = Q + d holds the coefficient of Q on its face
+        // pointing back (opposite of d)
+        float acc = fluidP ? 0.f : ld(ub1, k * N + c.i);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            if (!has[f]) continue;
+            const int nb = c.i + off[f];
+            const int back = f ^ 1;
+            const float coef = ld(A, (size_t)back * N + nb);
+            if (coef != 0.f) acc += coef * ld(iD, k * N + nb) * ld(ub1, k * N + nb);
+        }
+        ub0[k * N + c.i] = acc;
+    }
+    if (!fluidP) return;
+    float w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float d = ld(iD, k * N + c.i);
+        const float u1 = ld(ub1, k * N + c.i);
+        w[k] = d * u1;
+        bbar[k * N + c.i] += w[k];
+        iDbar[k * N + c.i] += u1 * ld(u_k1, k * N + c.i) / d;
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (!has[f]) continue;  // faces that are not fluid-fluid are dropped in k_adj_vcoef
+        const int nb = c.i + off[f];
+        float t = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) t += w[k] * ld(u_k, k * N + nb);
+        Abar[(size_t)f * N + c.i] += t;
+    }
+}
+
+// VJP of VCOEF: A_f = nu ds/dx - s_f ds/4 (uT_P[a] + uT_Q[a]) on fluid faces,
+// iD = 1/D.
+__global__ void k_adj_vcoef(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                            const float* __restrict__ Abar, const float* __restrict__ iDbar,
+                            const float* __restrict__ iD, float* __restrict__ uTbar, float* __restrict__ Dbar) {
+    Cell c;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float d = ld(iD, k * N + c.i);
+        aadd(Dbar + k * N + c.i, -ld(iDbar, k * N + c.i) * d * d);
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const float ab = ld(Abar, (size_t)f * N + c.i);
+        if (ab == 0.f) continue;
+        const int a = face_axis(f), s = face_sign(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (!in_region(P, X, Y, Z)) continue;
+        const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
+        const float t = -s * P.ds * 0.25f * ab;
+        aadd(uTbar + a * N + c.i, t);
+        aadd(uTbar + a * N + q, t);
+    }
+}
+
+// VJP of PRE (CSVelPredictPreCompute with LES off, FvmColl.compute:1292-1859).
+__global__ void k_adj_pre(const __grid_constant__ Params P, const Bnd B, const BndBar G,
+                          const uint8_t* __restrict__ fl, const float* __restrict__ Dbar,
+                          const float* __restrict__ bbar, float* __restrict__ uTbar, float* __restrict__ pbar) {
+    Cell c;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
+    const size_t N = P.N;
+    const float db[3] = {ld(Dbar, c.i), ld(Dbar, N + c.i), ld(Dbar, 2 * N + c.i)};
+    const float bb[3] = {ld(bbar, c.i), ld(bbar, N + c.i), ld(bbar, 2 * N + c.i)};
+    const float sD = db[0] + db[1] + db[2];
+    // advection
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f), s = face_sign(f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        if (in_region(P, X, Y, Z)) {
+            const int q = cidx(P, X, Y, Z);
+            if (fluid_at(fl, q)) {
+                const float t = s * P.ds * 0.25f * sD;
+                aadd(uTbar + a * N + c.i, t);
+                aadd(uTbar + a * N + q, t);
+            }
+        } else {
+            const int bc = face_bc(f), bt = P.vbc[bc];
+            if (bt == WF_BND_FIXED_VALUE) {
+                float g[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) g[k] = bnd_comp(P, B, bc, c.x, c.y, c.z, k);
+                float tsum = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    aadd(bnd_bar(P, G, bc, c.x, c.y, c.z, k), -s * P.ds * g[a] * bb[k]);
+                    tsum += g[k] * bb[k];
+                }
+                aadd(bnd_bar(P, G, bc, c.x, c.y, c.z, a), -s * P.ds * tsum);
+                // diffusion of the fixed value: b[k] += 2 nu ds/dx g[k]
+                const float t = 2.f * P.nu * P.ds / P.dx;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) aadd(bnd_bar(P, G, bc, c.x, c.y, c.z, k), t * bb[k]);
+            } else if (bt == WF_BND_ZERO_GRAD) {
+                aadd(uTbar + a * N + c.i, s * P.ds * sD);
+            }
+        }
+    }
+    // pressure: b[a] += -(1/den) ds (pf[2a] - pf[2a+1])
+    float own = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f);
+        const float pfb = (f & 1) ? (P.ds / P.den) * bb[a] : -(P.ds / P.den) * bb[a];
+        int q;
+        bool fx;
+        face_rule(P, fl, c, f, q, fx);
+        if (q >= 0) {
+            own += 0.5f * pfb;
+            aadd(pbar + q, 0.5f * pfb);
+        } else if (!fx) {
+            own += pfb;
+        }
+    }
+    aadd(pbar + c.i, own);
+    // time term
+    const float dvdt = P.dv / P.dt;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) aadd(uTbar + k * N + c.i, dvdt * bb[k]);
+}
+
+__global__ void k_axpy(long long n, float a, const float* __restrict__ x, float* __restrict__ y) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) y[i] += a * x[i];
+}
+// y[i] += x[i] on cells of the mask (solid_ok: every non-solid cell; else fluid)
+__global__ void k_add_masked(int n, const uint8_t* __restrict__ fl, const float* __restrict__ x,
+                             float* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && fl[i] == WF_CELL_FLUID) y[i] += x[i];
+}
+
+// Objective: J += w * sum of |u|^2 over the fluid cells of the patch, and
+// ubar += 2 w u there.
+__global__ void k_objective(const __grid_constant__ Params P, const uint8_t* __restrict__ fl, int x0, int x1, int y,
+                            int z0, int z1, float w, const float* __restrict__ u, float* __restrict__ ubar,
+                            double* __restrict__ Jacc) {
+    const int x = x0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = z0 + blockIdx.y * blockDim.y + threadIdx.y;
+    double s = 0.0;
+    if (x < x1 && z < z1 && fl[cidx(P, x, y, z)] == WF_CELL_FLUID) {
+        const int i = cidx(P, x, y, z);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float v = u[(size_t)k * P.N + i];
+            s += (double)v * v;
+            if (ubar) ubar[(size_t)k * P.N + i] += 2.f * w * v;
+        }
+    }
+    if (Jacc) {
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0 && s != 0.0) atomicAdd(Jacc, s * (double)w);
+    }
+}
+
+dim3 cblk() { return dim3(32, 4, 2); }
+dim3 cgrd(const Params& P) {
+    dim3 b = cblk();
+    return dim3((P.nx + b.x - 1) / b.x, (P.ny + b.y - 1) / b.y, (P.nz + b.z - 1) / b.z);
+}
+int lin_blocks(long long n) { return (int)((n + 255) / 256); }
+
+}  // namespace
+}  // namespace wf
+
+// =====================================================================
+struct wf_adjoint {
+    wf_solver* h = nullptr;
+    cudaStream_t st = nullptr;
+    int nV = 0, nP = 0, nC = 0;
+    size_t N = 0;
+    // tape of one step
+    float *uT = nullptr, *p0 = nullptr, *D = nullptr, *b = nullptr, *A = nullptr, *iD = nullptr;
+    float* uit = nullptr;  // (nV+1) x 3N
+    float *Dp = nullptr, *bp = nullptr, *c3 = nullptr, *ainv = nullptr;
+    float* qit = nullptr;  // (nP+1) x N
+    float* cbuf = nullptr; // (nC+1) x 3N corrections c_1..c_{nC+1}
+    float *aod = nullptr, *pai = nullptr, *prhs = nullptr;  // nC x 3N, nC x N, nC x N
+    float* sit = nullptr;  // nC x (nP+1) x N
+    float *uout = nullptr, *pout = nullptr;
+    // adjoint work
+    float *ub = nullptr, *ub2 = nullptr, *uTb = nullptr, *pb = nullptr, *pb_in = nullptr;
+    float *Db = nullptr, *bb = nullptr, *Ab = nullptr, *iDb = nullptr, *c3b = nullptr;
+    float *cb = nullptr, *cb2 = nullptr, *ab = nullptr, *sb = nullptr, *sb2 = nullptr;
+    float *aib = nullptr, *rb = nullptr, *Dpb = nullptr, *bpb = nullptr;
+    float* gb = nullptr;   // adjoint of the 6 boundary planes (same layout)
+    double* dJ = nullptr;  // device accumulator of the objective
+    std::vector<float*> ck;  // stored states (4N each: u then p)
+    std::string err;
+};
+
+namespace {
+
+using wf::Params;
+
+int adj_fail(wf_adjoint* a, int code, const char* msg) {
+    a->err = msg;
+    return code;
+}
+
+#define WFA_CUDA(call)                                                         \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) {                                               \
+            a->err = std::string(#call) + ": " + cudaGetErrorString(e_);       \
+            return e_ == cudaErrorMemoryAllocation ? WF_ERR_OOM : WF_ERR_CUDA; \
+        }                                                                      \
+    } while (0)
+
+float* U(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * 3 * a->N; }
+float* S1(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * a->N; }
+float* SIT(const wf_adjoint* a, int m, int k) { return a->sit + ((size_t)m * (a->nP + 1) + k) * a->N; }
+
+wf::BndBar bnd_bar(const wf_adjoint* a) {
+    wf::BndBar G;
+    const Params& P = a->h->P;
+    float* p = a->gb;
+    for (int f = 0; f < 6; ++f) {
+        G.p[f] = p;
+        p += 3 * (size_t)P.plane[f];
+    }
+    return G;
+}
+size_t plane_floats(const Params& P) {
+    size_t n = 0;
+    for (int f = 0; f < 6; ++f) n += 3 * (size_t)P.plane[f];
+    return n;
+}
+
+// Forward step from (u_in, p_in) with every intermediate kept.  phases: 1 =
+// stop after the momentum predictor, 2 = after the SIMPLE correction, 3 = the
+// whole step.  Output state in uout / pout.
+int record_step(wf_adjoint* a, const float* u_in, const float* p_in, int phases) {
+    wf_solver* h = a->h;
+    const Params& P = h->P;
+    cudaStream_t st = a->st;
+    const size_t N = a->N;
+    const size_t v = 3 * N * sizeof(float), s = N * sizeof(float);
+    WFA_CUDA(cudaMemcpyAsync(a->uT, u_in, v, cudaMemcpyDeviceToDevice, st));
+    WFA_CUDA(cudaMemcpyAsync(a->p0, p_in, s, cudaMemcpyDeviceToDevice, st));
+    wf::launch_vel_precompute(P, h->B, st, h->fl, a->uT, a->p0, h->eddy, h->face, nullptr, a->D, a->b);
+    wf::launch_vel_coef_ptr(P, st, h->fl, a->uT, h->eddy, h->face, a->D, a->A, a->iD);
+    for (int k = 0; k <= a->nV; ++k)
+        WFA_CUDA(cudaMemcpyAsync(U(a, a->uit, k), a->uT, v, cudaMemcpyDeviceToDevice, st));
+    for (int k = 0; k < a->nV; ++k)
+        wf::launch_vel_sweep1_ptr(P, st, a->A, a->iD, a->b, U(a, a->uit, k), U(a, a->uit, k + 1));
+    const float* ustar = U(a, a->uit, a->nV);
+    WFA_CUDA(cudaMemcpyAsync(a->uout, ustar, v, cudaMemcpyDeviceToDevice, st));
+    WFA_CUDA(cudaMemcpyAsync(a->pout, a->p0, s, cudaMemcpyDeviceToDevice, st));
+    if (phases >= 2) {
+        wf::launch_pres_precompute(P, h->B, st, h->fl, ustar, a->p0, a->D, a->Dp, a->bp);
+        wf::launch_pres_coef_ptr(P, st, h->fl, a->D, a->c3);
+        wf::launch_inv_ptr(P, st, h->fl, a->Dp, a->ainv);
+        WFA_CUDA(cudaMemsetAsync(a->qit, 0, (size_t)(a->nP + 1) * s, st));
+        for (int k = 0; k < a->nP; ++k)
+            wf::launch_pres_sweep1_ptr(P, st, a->c3, a->ainv, a->bp, k == 0 ? nullptr : S1(a, a->qit, k),
+                                       S1(a, a->qit, k + 1));
+        const float* q = S1(a, a->qit, a->nP);
+        WFA_CUDA(cudaMemsetAsync(a->cbuf, 0, (size_t)(a->nC + 1) * v, st));
+        wf::launch_apply_vel(P, st, h->fl, q, a->D, U(a, a->cbuf, 0), a->uout);
+        wf::launch_apply_pres(P, st, h->fl, q, a->pout);
+    }
+    if (phases >= 3) {
+        WFA_CUDA(cudaMemsetAsync(a->aod, 0, (size_t)a->nC * v, st));
+        WFA_CUDA(cudaMemsetAsync(a->sit, 0, (size_t)a->nC * (a->nP + 1) * s, st));
+        for (int m = 0; m < a->nC; ++m) {
+            wf::launch_piso_aodu(P, st, h->fl, U(a, a->cbuf, m), a->uT, h->eddy, h->face, U(a, a->aod, m));
+            wf::launch_piso_pre_ptr(P, st, h->fl, a->D, U(a, a->aod, m), S1(a, a->pai, m), S1(a, a->prhs, m));
+            for (int k = 0; k < a->nP; ++k)
+                wf::launch_pres_sweep1_ptr(P, st, a->c3, S1(a, a->pai, m), S1(a, a->prhs, m),
+                                           k == 0 ? nullptr : SIT(a, m, k), SIT(a, m, k + 1));
+            const float* ss = SIT(a, m, a->nP);
+            wf::launch_apply_pres(P, st, h->fl, ss, a->pout);
+            wf::launch_piso_vel(P, st, h->fl, ss, a->D, U(a, a->aod, m), U(a, a->cbuf, m + 1), a->uout);
+        }
+    }
+    WFA_CUDA(cudaGetLastError());
+    return WF_OK;
+}
+
+// Reverse of record_step: on entry a->ub / a->pb hold the adjoints of
+// (uout, pout); on exit they hold the adjoints of (u_in, p_in), and a->gb
+// has the boundary-plane adjoints added.
+int adjoint_step(wf_adjoint* a, int phases) {
+    wf_solver* h = a->h;
+    const Params& P = h->P;
+    cudaStream_t st = a->st;
+    const size_t N = a->N;
+    const size_t v = 3 * N * sizeof(float), s = N * sizeof(float);
+    const dim3 g = wf::cgrd(P), bk = wf::cblk();
+    const wf::BndBar G = bnd_bar(a);
+    WFA_CUDA(cudaMemsetAsync(a->uTb, 0, v, st));
+    WFA_CUDA(cudaMemsetAsync(a->Db, 0, v, st));
+    WFA_CUDA(cudaMemsetAsync(a->c3b, 0, v, st));
+    WFA_CUDA(cudaMemcpyAsync(a->pb_in, a->pb, s, cudaMemcpyDeviceToDevice, st));
+    const float* ustar = U(a, a->uit, a->nV);
+    if (phases >= 3) {
+        // cb = adjoint of the newest correction
+        WFA_CUDA(cudaMemcpyAsync(a->cb, a->ub, v, cudaMemcpyDeviceToDevice, st));
+        for (int m = a->nC - 1; m >= 0; --m) {
+            WFA_CUDA(cudaMemsetAsync(a->ab, 0, v, st));
+            WFA_CUDA(cudaMemsetAsync(a->sb, 0, s, st));
+            const float* ss = SIT(a, m, a->nP);
+            wf::k_adj_pvel<<<g, bk, 0, st>>>(P, h->fl, a->cb, ss, a->D, U(a, a->aod, m), a->ab, a->sb, a->Db);
+            wf::k_add_masked<<<wf::lin_blocks(N), 256, 0, st>>>((int)N, h->fl, a->pb, a->sb);
+            WFA_CUDA(cudaMemsetAsync(a->aib, 0, s, st));
+            WFA_CUDA(cudaMemsetAsync(a->rb, 0, s, st));
+            float* in = a->sb;
+            float* out = a->sb2;
+            for (int k = a->nP - 1; k >= 0; --k) {
+                wf::k_adj_psweep<<<g, bk, 0, st>>>(P, in, k == 0 ? nullptr : SIT(a, m, k), SIT(a, m, k + 1),
+                                                   S1(a, a->pai, m), a->c3, out, a->c3b, a->aib, a->rb);
+                std::swap(in, out);
+            }
+            wf::k_adj_pisopre<<<g, bk, 0, st>>>(P, h->fl, a->aib, a->rb, S1(a, a->pai, m), a->D, U(a, a->aod, m),
+                                                a->ab, a->Db);
+            // adjoint of c_m: the velocity adjoint (u_m = u_{m-1} + c_m) plus
+            // its use in AOD
+            WFA_CUDA(cudaMemcpyAsync(a->cb2, a->ub, v, cudaMemcpyDeviceToDevice, st));
+            wf::k_adj_aod<<<g, bk, 0, st>>>(P, h->fl, a->ab, U(a, a->cbuf, m), a->uT, a->cb2, a->uTb);
+            std::swap(a->cb, a->cb2);
+        }
+    } else if (phases >= 2) {
+        WFA_CUDA(cudaMemcpyAsync(a->cb, a->ub, v, cudaMemcpyDeviceToDevice, st));
+    }
+    if (phases >= 2) {
+        const float* q = S1(a, a->qit, a->nP);
+        WFA_CUDA(cudaMemsetAsync(a->sb, 0, s, st));
+        wf::k_adj_corr<<<g, bk, 0, st>>>(P, h->fl, a->cb, q, a->D, a->sb, a->Db);
+        wf::k_add_masked<<<wf::lin_blocks(N), 256, 0, st>>>((int)N, h->fl, a->pb, a->sb);
+        WFA_CUDA(cudaMemsetAsync(a->aib, 0, s, st));
+        WFA_CUDA(cudaMemsetAsync(a->bpb, 0, s, st));
+        float* in = a->sb;
+        float* out = a->sb2;
+        for (int k = a->nP - 1; k >= 0; --k) {
+            wf::k_adj_psweep<<<g, bk, 0, st>>>(P, in, k == 0 ? nullptr : S1(a, a->qit, k), S1(a, a->qit, k + 1),
+                                               a->ainv, a->c3, out, a->c3b, a->aib, a->bpb);
+            std::swap(in, out);
+        }
+        WFA_CUDA(cudaMemsetAsync(a->Dpb, 0, s, st));
+        wf::k_adj_inv<<<wf::lin_blocks(N), 256, 0, st>>>((int)N, a->aib, a->ainv, a->Dpb);
+        wf::k_adj_c3<<<g, bk, 0, st>>>(P, a->c3b, a->D, a->Db);
+        wf::k_adj_ppre<<<g, bk, 0, st>>>(P, G, h->fl, a->Dpb, a->bpb, a->p0, a->D, a->ub, a->pb_in, a->Db);
+    }
+    // momentum sweeps in reverse; a->ub is the adjoint of u*
+    WFA_CUDA(cudaMemsetAsync(a->Ab, 0, 2 * v, st));
+    WFA_CUDA(cudaMemsetAsync(a->iDb, 0, v, st));
+    WFA_CUDA(cudaMemsetAsync(a->bb, 0, v, st));
+    float* in = a->ub;
+    float* out = a->ub2;
+    for (int k = a->nV - 1; k >= 0; --k) {
+        wf::k_adj_vsweep<<<g, bk, 0, st>>>(P, in, U(a, a->uit, k), U(a, a->uit, k + 1), a->A, a->iD, out, a->Ab,
+                                           a->iDb, a->bb);
+        std::swap(in, out);
+    }
+    wf::k_axpy<<<wf::lin_blocks(3 * (long long)N), 256, 0, st>>>(3 * (long long)N, 1.f, in, a->uTb);
+    wf::k_adj_vcoef<<<g, bk, 0, st>>>(P, h->fl, a->Ab, a->iDb, a->iD, a->uTb, a->Db);
+    wf::k_adj_pre<<<g, bk, 0, st>>>(P, h->B, G, h->fl, a->Db, a->bb, a->uTb, a->pb_in);
+    (void)ustar;
+    WFA_CUDA(cudaMemcpyAsync(a->ub, a->uTb, v, cudaMemcpyDeviceToDevice, st));
+    WFA_CUDA(cudaMemcpyAsync(a->pb, a->pb_in, s, cudaMemcpyDeviceToDevice, st));
+    WFA_CUDA(cudaGetLastError());
+    return WF_OK;
+}
+
+void free_adj(wf_adjoint* a) {
+    float* ptrs[] = {a->uT, a->p0, a->D, a->b, a->A, a->iD, a->uit, a->Dp, a->bp, a->c3, a->ainv, a->qit, a->cbuf,
+                     a->aod, a->pai, a->prhs, a->sit, a->uout, a->pout, a->ub, a->ub2, a->uTb, a->pb, a->pb_in,
+                     a->Db, a->bb, a->Ab, a->iDb, a->c3b, a->cb, a->cb2, a->ab, a->sb, a->sb2, a->aib, a->rb,
+                     a->Dpb, a->bpb, a->gb};
+    for (float* p : ptrs)
+        if (p) cudaFree(p);
+    if (a->dJ) cudaFree(a->dJ);
+    for (float* p : a->ck)
+        if (p) cudaFree(p);
+    a->ck.clear();
+    if (a->st) cudaStreamDestroy(a->st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int wf_adj_create(wf_solver* h, wf_adjoint** out) {
+    if (!h || !out) return WF_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (h->P.les) return WF_ERR_UNSUPPORTED;
+    if (h->cfg.calc_residual) return WF_ERR_UNSUPPORTED;  // early exits change the iteration counts
+    if (h->cfg.compat_flags & WF_COMPAT_PISO_CONSISTENT) return WF_ERR_UNSUPPORTED;
+    bool fixed_p = false;
+    for (int f = 0; f < 6; ++f) fixed_p |= h->cfg.pres_bc[f] == WF_BND_FIXED_VALUE;
+    if (!fixed_p) return WF_ERR_UNSUPPORTED;  // pressure normalisation not differentiated
+    if (cudaSetDevice(h->device) != cudaSuccess) return WF_ERR_CUDA;
+    auto* a = new (std::nothrow) wf_adjoint;
+    if (!a) return WF_ERR_OOM;
+    a->h = h;
+    a->N = h->P.N;
+    a->nV = h->cfg.vel_iters;
+    a->nP = h->cfg.pres_iters;
+    a->nC = h->cfg.solver_type == WF_SOLVER_PISO ? h->cfg.piso_correctors : 0;
+    const size_t N = a->N, v = 3 * N * sizeof(float), s = N * sizeof(float);
+    bool ok = cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking) == cudaSuccess;
+    auto al = [&](float** p, size_t bytes) {
+        if (!ok) return;
+        ok = cudaMalloc((void**)p, bytes) == cudaSuccess && cudaMemsetAsync(*p, 0, bytes, a->st) == cudaSuccess;
+    };
+    const int nC1 = a->nC > 0 ? a->nC : 1;
+    al(&a->uT, v); al(&a->p0, s); al(&a->D, v); al(&a->b, v); al(&a->A, 2 * v); al(&a->iD, v);
+    al(&a->uit, (size_t)(a->nV + 1) * v);
+    al(&a->Dp, s); al(&a->bp, s); al(&a->c3, v); al(&a->ainv, s);
+    al(&a->qit, (size_t)(a->nP + 1) * s);
+    al(&a->cbuf, (size_t)(a->nC + 1) * v);
+    al(&a->aod, (size_t)nC1 * v); al(&a->pai, (size_t)nC1 * s); al(&a->prhs, (size_t)nC1 * s);
+    al(&a->sit, (size_t)nC1 * (a->nP + 1) * s);
+    al(&a->uout, v); al(&a->pout, s);
+    al(&a->ub, v); al(&a->ub2, v); al(&a->uTb, v); al(&a->pb, s); al(&a->pb_in, s);
+    al(&a->Db, v); al(&a->bb, v); al(&a->Ab, 2 * v); al(&a->iDb, v); al(&a->c3b, v);
+    al(&a->cb, v); al(&a->cb2, v); al(&a->ab, v); al(&a->sb, s); al(&a->sb2, s);
+    al(&a->aib, s); al(&a->rb, s); al(&a->Dpb, s); al(&a->bpb, s);
+    al(&a->gb, plane_floats(h->P) * sizeof(float));
+    if (ok) ok = cudaMalloc((void**)&a->dJ, sizeof(double)) == cudaSuccess;
+    if (ok) ok = cudaStreamSynchronize(a->st) == cudaSuccess;
+    if (!ok) {
+        free_adj(a);
+        delete a;
+        return WF_ERR_OOM;
+    }
+    *out = a;
+    return WF_OK;
+}
+
+int wf_adj_destroy(wf_adjoint* a) {
+    if (!a) return WF_ERR_INVALID_ARG;
+    cudaSetDevice(a->h->device);
+    cudaStreamSynchronize(a->st);
+    free_adj(a);
+    delete a;
+    return WF_OK;
+}
+
+const char* wf_adj_last_error(const wf_adjoint* a) { return a ? a->err.c_str() : "null adjoint"; }
+
+int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const float* pbar_out, float* ubar_in,
+                    float* pbar_in, float* gbar_planes) {
+    if (!a || phases < 1 || phases > 3 || !ubar_out || !pbar_out || !ubar_in || !pbar_in)
+        return WF_ERR_INVALID_ARG;
+    wf_solver* h = a->h;
+    WFA_CUDA(cudaSetDevice(h->device));
+    WFA_CUDA(cudaStreamSynchronize(h->st));
+    const size_t N = a->N, v = 3 * N * sizeof(float), s = N * sizeof(float);
+    // the solver's current state is the step input
+    int st = record_step(a, h->vb[h->iT], h->pr, phases);
+    if (st != WF_OK) return st;
+    WFA_CUDA(cudaMemcpyAsync(a->ub, ubar_out, v, cudaMemcpyHostToDevice, a->st));
+    WFA_CUDA(cudaMemcpyAsync(a->pb, pbar_out, s, cudaMemcpyHostToDevice, a->st));
+    WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(h->P) * sizeof(float), a->st));
+    st = adjoint_step(a, phases);
+    if (st != WF_OK) return st;
+    WFA_CUDA(cudaMemcpyAsync(ubar_in, a->ub, v, cudaMemcpyDeviceToHost, a->st));
+    WFA_CUDA(cudaMemcpyAsync(pbar_in, a->pb, s, cudaMemcpyDeviceToHost, a->st));
+    if (gbar_planes)
+        WFA_CUDA(cudaMemcpyAsync(gbar_planes, a->gb, plane_floats(h->P) * sizeof(float), cudaMemcpyDeviceToHost,
+                                 a->st));
+    WFA_CUDA(cudaStreamSynchronize(a->st));
+    return WF_OK;
+}
+
+int wf_adj_step_forward(wf_adjoint* a, int phases, float* u_out, float* p_out) {
+    if (!a || phases < 1 || phases > 3 || !u_out || !p_out) return WF_ERR_INVALID_ARG;
+    wf_solver* h = a->h;
+    WFA_CUDA(cudaSetDevice(h->device));
+    WFA_CUDA(cudaStreamSynchronize(h->st));
+    const int st = record_step(a, h->vb[h->iT], h->pr, phases);
+    if (st != WF_OK) return st;
+    WFA_CUDA(cudaMemcpyAsync(u_out, a->uout, 3 * a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
+    WFA_CUDA(cudaMemcpyAsync(p_out, a->pout, a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
+    WFA_CUDA(cudaStreamSynchronize(a->st));
+    return WF_OK;
+}
+
+int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
+                    double* J, double* dJ_dustar, double* dJ_dz0, float* ms_forward, float* ms_total) {
+    if (!a || !obj || n_steps < 1 || checkpoint_every < 1) return WF_ERR_INVALID_ARG;
+    wf_solver* h = a->h;
+    const Params& P = h->P;
+    const wf_config& c = h->cfg;
+    if (obj->x0 < 0 || obj->x1 > P.nx || obj->x0 >= obj->x1 || obj->z0 < 0 || obj->z1 > P.nz || obj->z0 >= obj->z1 ||
+        obj->y < 0 || obj->y >= P.ny || obj->window < 1 || obj->window > n_steps)
+        return adj_fail(a, WF_ERR_INVALID_ARG, "objective region or window out of range");
+    if (c.inflow_type != WF_INFLOW_LOG || !(c.inflow_ustar > 0.f))
+        return adj_fail(a, WF_ERR_UNSUPPORTED, "inflow gradients need the log inflow with inflow_ustar > 0");
+    WFA_CUDA(cudaSetDevice(h->device));
+    WFA_CUDA(cudaStreamSynchronize(h->st));
+    const size_t N = a->N, v = 3 * N * sizeof(float), s = N * sizeof(float);
+    const int area = (obj->x1 - obj->x0) * (obj->z1 - obj->z0);
+    const float w = 1.f / (float)(obj->window * area);
+    const dim3 og((obj->x1 - obj->x0 + 31) / 32, (obj->z1 - obj->z0 + 7) / 8), ob(32, 8);
+    // checkpoints: state n for n % C == 0 (n < n_steps); one segment of
+    // states recomputed from its checkpoint at a time
+    const int C = checkpoint_every;
+    const int nck = (n_steps + C - 1) / C;
+    struct Scratch {
+        std::vector<float*> seg;
+        cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+        ~Scratch() {
+            for (float* p : seg)
+                if (p) cudaFree(p);
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } S;
+    for (float* p : a->ck) cudaFree(p);
+    a->ck.assign(nck, nullptr);
+    for (int i = 0; i < nck; ++i)
+        if (cudaMalloc((void**)&a->ck[i], v + s) != cudaSuccess) return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
+    S.seg.assign(C, nullptr);
+    for (int i = 0; i < C; ++i)
+        if (cudaMalloc((void**)&S.seg[i], v + s) != cudaSuccess) return adj_fail(a, WF_ERR_OOM, "segment memory");
+    for (cudaEvent_t& e : S.ev) WFA_CUDA(cudaEventCreate(&e));
+    std::vector<float*>& seg = S.seg;
+    WFA_CUDA(cudaMemsetAsync(a->dJ, 0, sizeof(double), h->st));
+    WFA_CUDA(cudaEventRecord(S.ev[0], h->st));
+    // ---- forward: the solver's own (fast) step, checkpoints, objective
+    for (int n = 0; n < n_steps; ++n) {
+        if (n % C == 0) {
+            WFA_CUDA(cudaMemcpyAsync(a->ck[n / C], h->vb[h->iT], v, cudaMemcpyDeviceToDevice, h->st));
+            WFA_CUDA(cudaMemcpyAsync(a->ck[n / C] + 3 * N, h->pr, s, cudaMemcpyDeviceToDevice, h->st));
+        }
+        const int st = wf_step(h, 1, nullptr);
+        if (st != WF_OK) return adj_fail(a, st, "forward step failed");
+        if (n + 1 > n_steps - obj->window)
+            wf::k_objective<<<og, ob, 0, h->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
+                                                  h->vb[h->iT], nullptr, a->dJ);
+    }
+    WFA_CUDA(cudaEventRecord(S.ev[1], h->st));
+    WFA_CUDA(cudaStreamSynchronize(h->st));
+    // ---- reverse
+    WFA_CUDA(cudaMemsetAsync(a->ub, 0, v, a->st));
+    WFA_CUDA(cudaMemsetAsync(a->pb, 0, s, a->st));
+    WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(P) * sizeof(float), a->st));
+    for (int sgi = nck - 1; sgi >= 0; --sgi) {
+        const int n0 = sgi * C, n1 = std::min(n_steps, n0 + C);
+        WFA_CUDA(cudaMemcpyAsync(seg[0], a->ck[sgi], v + s, cudaMemcpyDeviceToDevice, a->st));
+        for (int n = n0 + 1; n < n1; ++n) {
+            const int st = record_step(a, seg[n - 1 - n0], seg[n - 1 - n0] + 3 * N, 3);
+            if (st != WF_OK) return st;
+            WFA_CUDA(cudaMemcpyAsync(seg[n - n0], a->uout, v, cudaMemcpyDeviceToDevice, a->st));
+            WFA_CUDA(cudaMemcpyAsync(seg[n - n0] + 3 * N, a->pout, s, cudaMemcpyDeviceToDevice, a->st));
+        }
+        for (int n = n1 - 1; n >= n0; --n) {
+            // step n maps state n to state n+1
+            int st = record_step(a, seg[n - n0], seg[n - n0] + 3 * N, 3);
+            if (st != WF_OK) return st;
+            if (n + 1 > n_steps - obj->window)
+                wf::k_objective<<<og, ob, 0, a->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
+                                                      a->uout, a->ub, nullptr);
+            st = adjoint_step(a, 3);
+            if (st != WF_OK) return st;
+        }
+    }
+    WFA_CUDA(cudaEventRecord(S.ev[2], a->st));
+    WFA_CUDA(cudaStreamSynchronize(a->st));
+    // ---- chain to the inflow parameters: X0 plane g_x(y) = u*/k ln((y_c+z0)/z0)
+    const int np = P.plane[WF_FACE_X0];
+    std::vector<float> gx(np);
+    WFA_CUDA(cudaMemcpy(gx.data(), a->gb, np * sizeof(float), cudaMemcpyDeviceToHost));  // x component of X0
+    const double us = c.inflow_ustar, z0 = c.inflow_z0, kap = c.inflow_kappa, dx = c.dx;
+    double gu = 0.0, gz = 0.0;
+    for (int z = 0; z < P.nz; ++z)
+        for (int y = 0; y < P.ny; ++y) {
+            const double yc = (y + 0.5) * dx;
+            const double gb = gx[(size_t)z * P.ny + y];
+            gu += gb * std::log((yc + z0) / z0) / kap;
+            gz += gb * us / kap * (1.0 / (yc + z0) - 1.0 / z0);
+        }
+    if (include_init) {
+        // initial interior profile u_x(y) = u*/k ln((y_p + z0)/z0) on fluid cells
+        std::vector<float> ubar(3 * N);
+        std::vector<uint8_t> flg(N);
+        WFA_CUDA(cudaMemcpy(ubar.data(), a->ub, 3 * N * sizeof(float), cudaMemcpyDeviceToHost));
+        WFA_CUDA(cudaMemcpy(flg.data(), h->fl, N, cudaMemcpyDeviceToHost));
+        const bool centre = (c.compat_flags & WF_COMPAT_INIT_PROFILE_CELL_CENTRE) != 0;
+        for (int z = 0; z < P.nz; ++z)
+            for (int y = 0; y < P.ny; ++y) {
+                const double yp = centre ? (y + 0.5) * dx : y * dx;
+                const double du = std::log((yp + z0) / z0) / kap;
+                const double dz = us / kap * (1.0 / (yp + z0) - 1.0 / z0);
+                for (int x = 0; x < P.nx; ++x) {
+                    const size_t i = ((size_t)z * P.ny + y) * P.nx + x;
+                    if (flg[i] != WF_CELL_FLUID) continue;
+                    gu += ubar[i] * du;
+                    gz += ubar[i] * dz;
+                }
+            }
+    }
+    double Jh = 0.0;
+    WFA_CUDA(cudaMemcpy(&Jh, a->dJ, sizeof(double), cudaMemcpyDeviceToHost));
+    if (J) *J = Jh;
+    if (dJ_dustar) *dJ_dustar = gu;
+    if (dJ_dz0) *dJ_dz0 = gz;
+    float tf = 0.f, tt = 0.f;
+    WFA_CUDA(cudaEventElapsedTime(&tf, S.ev[0], S.ev[1]));
+    WFA_CUDA(cudaEventElapsedTime(&tt, S.ev[0], S.ev[2]));
+    if (ms_forward) *ms_forward = tf;
+    if (ms_total) *ms_total = tt;
+    return WF_OK;
+}
+
+}  // extern "C"

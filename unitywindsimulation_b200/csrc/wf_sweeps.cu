@@ -917,4 +917,34 @@ int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double
     return WF_OK;
 }
 
+// Explicit-pointer launchers (the adjoint's recorded forward step).
+void launch_vel_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, const float* eddy,
+                         const float* face, const float* Dv, float* A, float* iD) {
+    WF_COUNT_LAUNCH();
+    k_vel_coef<<<grd(P), blk(), 0, st>>>(P, fl, uT, eddy, face, Dv, A, iD);
+}
+void launch_vel_sweep1_ptr(const Params& P, cudaStream_t st, const float* A, const float* iD, const float* bv,
+                           const float* ui, float* uo) {
+    WF_COUNT_LAUNCH();
+    k_vel_sweep1<<<grd(P), blk(), 0, st>>>(P, A, iD, bv, ui, uo);
+}
+void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, float* c3) {
+    WF_COUNT_LAUNCH();
+    k_pres_coef<<<grd(P), blk(), 0, st>>>(P, fl, Dv, c3);
+}
+void launch_inv_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dp, float* ainv) {
+    WF_COUNT_LAUNCH();
+    k_inv<<<(P.N + 255) / 256, 256, 0, st>>>(P, fl, Dp, ainv);
+}
+void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* aodu,
+                         float* ainv, float* rhs) {
+    WF_COUNT_LAUNCH();
+    k_piso_pre<<<grd(P), blk(), 0, st>>>(P, fl, Dv, aodu, ainv, rhs);
+}
+void launch_pres_sweep1_ptr(const Params& P, cudaStream_t st, const float* c3, const float* ainv, const float* rhs,
+                            const float* pi, float* po) {
+    WF_COUNT_LAUNCH();
+    k_pres_sweep1<<<grd(P), blk(), 0, st>>>(P, c3, ainv, rhs, pi, po);
+}
+
 }  // namespace wf

@@ -18,6 +18,21 @@ int vel_sweeps_fast(wf_solver* h, int n);
 // or CSPisoPresCorrection (piso = true, :1493-1514) with the same rotation.
 int pres_sweeps_fast(wf_solver* h, int n, bool piso);
 
+// Explicit-pointer launchers of the fast Jacobi building blocks: momentum
+// coefficients A (6 planes) and 1/D (3), one momentum sweep, pressure face
+// coefficients c_E/c_N/c_U, 1/Dp, PISO diagonal and right-hand side, one
+// pressure-type sweep (pi == nullptr: zero iterate).
+void launch_vel_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, const float* eddy,
+                         const float* face, const float* Dv, float* A, float* iD);
+void launch_vel_sweep1_ptr(const Params& P, cudaStream_t st, const float* A, const float* iD, const float* bv,
+                           const float* ui, float* uo);
+void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, float* c3);
+void launch_inv_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dp, float* ainv);
+void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* aodu,
+                         float* ainv, float* rhs);
+void launch_pres_sweep1_ptr(const Params& P, cudaStream_t st, const float* c3, const float* ainv, const float* rhs,
+                            const float* pi, float* po);
+
 // Event-timed launches of one hot kernel (WF_KERNEL_*), see wf_time_kernel.
 int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double* bytes, int* sweeps);
 
