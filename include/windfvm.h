@@ -196,8 +196,16 @@ enum {
     WF_FIELD_BND_YN = 17,              /*   Z planes nx*ny, index y*nx+x */
     WF_FIELD_BND_Z0 = 18,
     WF_FIELD_BND_ZN = 19,
-    WF_FIELD_COUNT = 20
+    WF_FIELD_DRAG = 20,                /* drag coefficient chi (scalar, 1/s); no
+                                        * counterpart in the reference, see below */
+    WF_FIELD_COUNT = 21
 };
+/* WF_FIELD_DRAG: Brinkman drag chi >= 0 per cell, added implicitly to the
+ * momentum diagonal (D += dv * chi), which lets a soft (partly porous)
+ * obstacle mask stand in for the binary flags, e.g. buildings whose heights
+ * are continuous parameters.  Zero (the default, no storage) leaves the
+ * reference's equations unchanged.  Setting it the first time drops the
+ * handle's captured step graphs; rebuild batches that contain the handle. */
 /* Number of cells (or plane points) of a field; vectors carry 3 floats per
  * point in SoA order. */
 int wf_field_size(const wf_solver* h, int field, size_t* points, int* comps);
@@ -333,11 +341,12 @@ const char* wf_adj_last_error(const wf_adjoint* a);
  * wf_adj_step_forward: the state after the cut (u_out 3N, p_out N).
  * wf_adj_step_vjp: given adjoints of that output (ubar_out 3N, pbar_out N),
  * the adjoints of the input state (ubar_in 3N, pbar_in N) and, when
- * gbar_planes is non-NULL, of the six boundary-value planes (3 * plane
- * points each, planes in WF_FACE_* order, as wf_field_size reports them). */
+ * non-NULL, of the six boundary-value planes (gbar_planes: 3 * plane points
+ * each, planes in WF_FACE_* order, as wf_field_size reports them) and of
+ * the drag field (dragbar, N; defined whether or not a drag field is set). */
 int wf_adj_step_forward(wf_adjoint* a, int phases, float* u_out, float* p_out);
 int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const float* pbar_out, float* ubar_in,
-                    float* pbar_in, float* gbar_planes);
+                    float* pbar_in, float* gbar_planes, float* dragbar);
 
 /* Pedestrian-comfort objective: the mean over the last `window` steps of the
  * mean squared speed |u|^2 on the fluid cells of one horizontal patch
@@ -353,11 +362,16 @@ typedef struct wf_objective {
  * (inflow_ustar, inflow_z0; needs inflow_type = WF_INFLOW_LOG with
  * inflow_ustar > 0).  include_init != 0 also differentiates the initial
  * interior profile of wf_init_vel_pres_fields (the current state must be that
- * profile).  States are stored every `checkpoint_every` steps and the others
- * recomputed.  ms_forward / ms_total (nullable): device time of the forward
- * pass and of the whole call. */
+ * profile).  dJ_ddrag (nullable, N floats): derivative with respect to the
+ * drag field (WF_FIELD_DRAG), from which a soft building mask's height
+ * gradients follow by the chain rule.  States are stored every
+ * `checkpoint_every` steps and the others recomputed.  ms_forward / ms_total
+ * (nullable): device time of the forward pass and of the whole call.
+ * Derivatives are summed with float atomics: repeated calls agree to
+ * rounding, not bit for bit. */
 int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
-                    double* J, double* dJ_dustar, double* dJ_dz0, float* ms_forward, float* ms_total);
+                    double* J, double* dJ_dustar, double* dJ_dz0, float* dJ_ddrag, float* ms_forward,
+                    float* ms_total);
 
 /* ---- allocation-free residual --------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate

@@ -54,6 +54,7 @@ template <class R> struct Oracle {
     std::vector<int32_t> flag;
     std::vector<V3<R>> vel, velT, velI, velC, Dv, bv, aodu, face;
     std::vector<R> p, pc, pcL, Dp, bp, eddy;
+    std::vector<R> drag;  // Brinkman drag per cell (library extension; zero = reference equations)
     std::vector<V3<R>> bnd[6];
     int64_t step = 0;
     double res_vel = -1.0, res_pres = -1.0;
@@ -127,7 +128,7 @@ template <class R> struct Oracle {
         vel.assign(N, z3); velT.assign(N, z3); velI.assign(N, z3); velC.assign(N, z3);
         Dv.assign(N, z3); bv.assign(N, z3); aodu.assign(N, z3); face.assign(N, z3);
         p.assign(N, R(0)); pc.assign(N, R(0)); pcL.assign(N, R(0));
-        Dp.assign(N, R(0)); bp.assign(N, R(0)); eddy.assign(N, R(0));
+        Dp.assign(N, R(0)); bp.assign(N, R(0)); eddy.assign(N, R(0)); drag.assign(N, R(0));
         bnd[0].assign(size_t(ny) * nz, z3); bnd[1].assign(size_t(ny) * nz, z3);
         bnd[2].assign(size_t(nx) * nz, z3); bnd[3].assign(size_t(nx) * nz, z3);
         bnd[4].assign(size_t(nx) * ny, z3); bnd[5].assign(size_t(nx) * ny, z3);
@@ -434,6 +435,9 @@ template <class R> struct Oracle {
             for (int c = 0; c < 3; ++c) b[c] += dv * force[c];
             if (les)
                 for (int c = 0; c < 3; ++c) b[c] += bv[P].c[c];
+            // Brinkman drag of a soft obstacle mask (no reference counterpart)
+            if (drag[P] != R(0))
+                for (int c = 0; c < 3; ++c) D[c] += dv * drag[P];
             Dv[P] = V3<R>{{D[0], D[1], D[2]}};
             bv[P] = V3<R>{{b[0], b[1], b[2]}};
         });
@@ -832,6 +836,7 @@ template <class R> struct Oracle {
             case WF_FIELD_DP: return &Dp;
             case WF_FIELD_BP: return &bp;
             case WF_FIELD_EDDY_VIS: return &eddy;
+            case WF_FIELD_DRAG: return &drag;
             default: return nullptr;
         }
     }

@@ -8,8 +8,9 @@ oracle, which restates the forward step independently:
   the oracle's differences against <J^T ubar, dx> from the adjoint, for
   random directions in the velocity, the pressure and the inlet plane;
 * the gradient of the pedestrian-comfort objective over a window of steps
-  with respect to the log-inflow parameters (u*, z0), with checkpoints and
-  recomputation, against FP64 differences with step 1e-4.
+  with respect to the log-inflow parameters (u*, z0) and the heights of
+  soft buildings, with checkpoints and recomputation, against FP64
+  differences with step 1e-4.
 
 Bound: 1e-3 relative, as for the objective gradient.
 """
@@ -18,7 +19,7 @@ import pytest
 
 from unitywindsimulation_b200 import FvmSolverCuda, _lib, cases
 from unitywindsimulation_b200.adjoint import (PHASE_FULL, PHASE_PREDICTOR, PHASE_SIMPLE, AdjointSolver,
-                                              InflowObjective, Objective)
+                                              Objective, WindObjective)
 from oracle import OracleSolver
 
 pytestmark = pytest.mark.gpu
@@ -38,15 +39,18 @@ def developed_solver(case, steps=3):
     return g
 
 
-def oracle_phase(case, g, u, p, phases, bnd_x0=None):
+def oracle_phase(case, g, u, p, phases, bnd_x0=None, drag=None):
     """One step of the FP64 oracle from state (u, p), cut after `phases`
-    parts, with the GPU solver's boundary planes (X0 replaced by bnd_x0)."""
+    parts, with the GPU solver's boundary planes (X0 replaced by bnd_x0) and
+    the case's drag field (replaced by drag)."""
     o = OracleSolver(case.cfg, 64)
-    o.InitFlags(case.flags)
+    cases.apply_case(o, case)
     for f in range(_lib.FIELD_BND_X0, _lib.FIELD_BND_ZN + 1):
         o.set_field(f, np.asarray(g.get_field(f), dtype=np.float64))
     if bnd_x0 is not None:
         o.set_field(_lib.FIELD_BND_X0, bnd_x0)
+    if drag is not None:
+        o.set_field(_lib.FIELD_DRAG, drag)
     for f in (_lib.FIELD_VEL, _lib.FIELD_VEL_LAST_TIME, _lib.FIELD_VEL_LAST_ITER):
         o.set_field(f, u)
     o.set_field(_lib.FIELD_PRES, p)
@@ -70,9 +74,16 @@ def oracle_phase(case, g, u, p, phases, bnd_x0=None):
     return out
 
 
-@pytest.fixture(scope="module")
-def setup(built):
-    case = adj_case()
+def drag_of(case):
+    c = case.cfg
+    if case.soft is None:
+        return np.zeros(c.nx * c.ny * c.nz)
+    return case.soft.drag(c.nx, c.ny, c.nz, np.float64).reshape(-1)
+
+
+@pytest.fixture(scope="module", params=["flags", "soft"])
+def setup(built, request):
+    case = adj_case() if request.param == "flags" else cases.small_soft_case(seed=3)
     g = developed_solver(case)
     adj = AdjointSolver(g)
     u0, p0, _ = g.get_state()
@@ -98,41 +109,48 @@ def test_tape_matches_step(setup):
 
 
 @pytest.mark.parametrize("phases", [PHASE_PREDICTOR, PHASE_SIMPLE, PHASE_FULL])
-@pytest.mark.parametrize("direction", ["vel", "pres", "inlet"])
+@pytest.mark.parametrize("direction", ["vel", "pres", "inlet", "drag"])
 def test_step_vjp_dot_product(setup, phases, direction):
     case, g, adj, u0, p0 = setup
     n = g.n_cells
     rng = np.random.default_rng(100 + 10 * phases + len(direction))
     ubar = rng.standard_normal((3, n))
     pbar = rng.standard_normal(n)
-    ui, pi, planes = adj.step_vjp(ubar, pbar, phases)
+    ui, pi, planes, dragbar = adj.step_vjp(ubar, pbar, phases)
     x0 = np.asarray(g.get_field(_lib.FIELD_BND_X0), dtype=np.float64)
+    chi = drag_of(case)
     du = np.zeros_like(u0)
     dp = np.zeros_like(p0)
     dg = np.zeros_like(x0)
+    dchi = np.zeros_like(chi)
     if direction == "vel":
         du = rng.standard_normal(u0.shape) * 0.5
         ad = float((ui.astype(np.float64) * du).sum())
     elif direction == "pres":
         dp = rng.standard_normal(p0.shape) * max(1e-3, np.abs(p0).max())
         ad = float((pi.astype(np.float64) * dp).sum())
-    else:
+    elif direction == "inlet":
         dg = rng.standard_normal(x0.shape) * 0.5
         ad = float((planes[_lib.FACE_X0].astype(np.float64) * dg.reshape(planes[0].shape)).sum())
+    else:
+        dchi = rng.uniform(0.0, 1.0, chi.shape) / case.cfg.dt
+        ad = float((dragbar.astype(np.float64) * dchi).sum())
 
     def J(s):
-        u, p = oracle_phase(case, g, u0 + s * du, p0 + s * dp, phases, x0 + s * dg)
+        u, p = oracle_phase(case, g, u0 + s * du, p0 + s * dp, phases, x0 + s * dg, chi + s * dchi)
         return float((ubar * u).sum() + (pbar * p).sum())
 
     fd = (J(FD_EPS) - J(-FD_EPS)) / (2 * FD_EPS)
     assert abs(fd - ad) <= ADJ_TOL * abs(fd), f"phase {phases} {direction}: adjoint {ad} vs FD {fd}"
 
 
-def _oracle_objective(case, obj, n_steps, ustar, z0):
+def _oracle_objective(case, obj, n_steps, ustar, z0, heights=None):
     cfg = case.cfg.copy()
     cfg.inflow_ustar, cfg.inflow_z0 = ustar, z0
     o = OracleSolver(cfg, 64)
-    o.InitFlags(case.flags)
+    c = case if heights is None else cases.Case(case.name, cfg, case.flags, case.inlet, case.steps, case.seed,
+                                                case.buildings, case.soft.with_heights(heights))
+    cases.apply_case(o, c)
     flags = o.GetFlagField()
     J = 0.0
     for n in range(n_steps):
@@ -164,6 +182,31 @@ def test_inflow_gradient_vs_fd(built, piso):
     assert abs(r["dJ_dz0"] - fz) <= ADJ_TOL * abs(fz), (r, fz)
 
 
+@pytest.mark.parametrize("piso", [True, False])
+def test_soft_height_gradient_vs_fd(built, piso):
+    case = cases.small_soft_case(piso=piso, seed=4)
+    obj = Objective(x0=4, x1=20, z0=2, z1=14, y=1, window=3)
+    n_steps = 6
+    g = FvmSolverCuda(case.cfg)
+    cases.apply_case(g, case)
+    with AdjointSolver(g) as adj:
+        r = adj.gradient(obj, n_steps, checkpoint_every=2, soft=case.soft)
+    g.close()
+    us, z0 = case.cfg.inflow_ustar, case.cfg.inflow_z0
+    h0 = case.soft.heights
+    for i in range(h0.size):
+        hp, hm = h0.copy(), h0.copy()
+        hp[i] += FD_EPS
+        hm[i] -= FD_EPS
+        fd = (_oracle_objective(case, obj, n_steps, us, z0, hp)
+              - _oracle_objective(case, obj, n_steps, us, z0, hm)) / (2 * FD_EPS)
+        ad = r["dJ_dheights"][i]
+        assert abs(ad - fd) <= ADJ_TOL * abs(fd), (i, ad, fd)
+    fu = (_oracle_objective(case, obj, n_steps, us + FD_EPS, z0, h0)
+          - _oracle_objective(case, obj, n_steps, us - FD_EPS, z0, h0)) / (2 * FD_EPS)
+    assert abs(r["dJ_dustar"] - fu) <= ADJ_TOL * abs(fu), (r["dJ_dustar"], fu)
+
+
 def test_checkpoint_interval_does_not_change_gradient(built):
     case = adj_case(seed=7)
     obj = Objective(x0=6, x1=22, z0=2, z1=14, y=1, window=2)
@@ -184,27 +227,29 @@ def test_checkpoint_interval_does_not_change_gradient(built):
 
 def test_autograd_function(built):
     torch = pytest.importorskip("torch")
-    case = adj_case(seed=8)
-    obj = Objective(x0=6, x1=22, z0=2, z1=14, y=1, window=2)
+    case = cases.small_soft_case(seed=8)
+    obj = Objective(x0=4, x1=20, z0=2, z1=14, y=1, window=2)
 
-    def make(us, z0):
+    def make(us, z0, soft):
         cfg = case.cfg.copy()
         cfg.inflow_ustar, cfg.inflow_z0 = us, z0
+        c = cases.Case(case.name, cfg, case.flags, None, 1, case.seed, [], soft)
         s = FvmSolverCuda(cfg)
-        cases.apply_case(s, case)
+        cases.apply_case(s, c)
         return s
 
-    params = torch.tensor([case.cfg.inflow_ustar, case.cfg.inflow_z0], dtype=torch.float64, requires_grad=True)
-    J = InflowObjective.apply(params, make, obj, 4, 2)
+    p0 = [case.cfg.inflow_ustar, case.cfg.inflow_z0] + list(case.soft.heights)
+    params = torch.tensor(p0, dtype=torch.float64, requires_grad=True)
+    J = WindObjective.apply(params, make, obj, 4, 2, case.soft)
     J.backward()
-    s = make(case.cfg.inflow_ustar, case.cfg.inflow_z0)
+    s = make(case.cfg.inflow_ustar, case.cfg.inflow_z0, case.soft)
     with AdjointSolver(s) as adj:
-        r = adj.gradient(obj, 4, 2)
+        r = adj.gradient(obj, 4, 2, soft=case.soft)
     s.close()
     # the adjoint scatters with float atomics: equal up to summation order
     assert J.item() == pytest.approx(r["J"], rel=1e-9)
-    assert params.grad[0].item() == pytest.approx(r["dJ_dustar"], rel=1e-6)
-    assert params.grad[1].item() == pytest.approx(r["dJ_dz0"], rel=1e-6)
+    ref = [r["dJ_dustar"], r["dJ_dz0"]] + list(r["dJ_dheights"])
+    np.testing.assert_allclose(params.grad.numpy(), ref, rtol=1e-5)
 
 
 def test_unsupported_configurations(built):

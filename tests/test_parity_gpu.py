@@ -196,6 +196,33 @@ def test_steps_from_init_match(built):
         assert ev <= REL_TOL * (k + 1) and ep <= REL_TOL * (k + 1), (k, ev, ep)
 
 
+@pytest.mark.parametrize("piso", [True, False])
+def test_drag_field_steps_match(built, piso):
+    """Soft building mask (Brinkman drag field, every cell fluid): five steps
+    from the initial state against the FP32 oracle with the same drag."""
+    case = cases.small_soft_case(piso=piso, seed=2)
+    g = FvmSolverCuda(case.cfg)
+    o = OracleSolver(case.cfg, 32)
+    for s in (g, o):
+        cases.apply_case(s, case)
+    np.testing.assert_array_equal(g.get_field(_lib.FIELD_DRAG), o.get_field(_lib.FIELD_DRAG).astype(np.float32))
+    for k in range(5):
+        g.Step(1)
+        o.Step(1)
+        ev = rel_l2(g.GetVelField(), o.GetVelField())
+        ep = rel_l2(g.GetPresField(), o.GetPresField())
+        assert ev <= REL_TOL * (k + 1) and ep <= REL_TOL * (k + 1), (k, ev, ep)
+    assert rel_l2(g.get_field(_lib.FIELD_D), o.get_field(_lib.FIELD_D)) <= REL_TOL
+
+
+def test_drag_field_default_is_zero(built):
+    case = cases.small_case(seed=3)
+    g = FvmSolverCuda(case.cfg)
+    assert g.field_size(_lib.FIELD_DRAG) == (g.n_cells, 1)
+    assert not np.any(g.get_field(_lib.FIELD_DRAG))
+    g.close()
+
+
 def test_plain_cube_one_step(built):
     """The 64 x 32 x 48 cube workload: one full step from the initial state."""
     case = cases.plain_cube()

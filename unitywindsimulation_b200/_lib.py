@@ -57,7 +57,8 @@ FIELD_BND_Y0 = 16
 FIELD_BND_YN = 17
 FIELD_BND_Z0 = 18
 FIELD_BND_ZN = 19
-FIELD_COUNT = 20
+FIELD_DRAG = 20
+FIELD_COUNT = 21
 
 FIELD_NAMES = {
     FIELD_VEL: "velField", FIELD_VEL_LAST_TIME: "velFieldLastTime", FIELD_VEL_LAST_ITER: "velFieldLastIter",
@@ -66,7 +67,7 @@ FIELD_NAMES = {
     FIELD_DP: "DFieldPresCorrect", FIELD_BP: "bFieldPresCorrect", FIELD_AODU: "AodUCorrectField",
     FIELD_EDDY_VIS: "eddyVisField", FIELD_FACE_EDDY_VIS: "faceEddyVisField", FIELD_BND_X0: "bndFieldX0",
     FIELD_BND_XN: "bndFieldXn", FIELD_BND_Y0: "bndFieldY0", FIELD_BND_YN: "bndFieldYn", FIELD_BND_Z0: "bndFieldZ0",
-    FIELD_BND_ZN: "bndFieldZn",
+    FIELD_BND_ZN: "bndFieldZn", FIELD_DRAG: "dragField",
 }
 
 
@@ -180,9 +181,9 @@ _SIGNATURES = {
     "wf_adj_destroy": (c_int, [c_void_p]),
     "wf_adj_last_error": (c_char_p, [c_void_p]),
     "wf_adj_step_forward": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
-    "wf_adj_step_vjp": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wf_adj_step_vjp": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "wf_adj_gradient": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_double), POINTER(c_double),
-                                POINTER(c_double), POINTER(c_float), POINTER(c_float)]),
+                                POINTER(c_double), c_void_p, POINTER(c_float), POINTER(c_float)]),
 }
 
 NOALLOC_BLOCKS = 4096

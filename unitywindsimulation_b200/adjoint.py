@@ -3,8 +3,10 @@
 ``AdjointSolver`` wraps one ``FvmSolverCuda`` handle: vector-Jacobian
 products of one step (cut after the momentum predictor, the SIMPLE
 correction or the whole step) and the gradient of the pedestrian-comfort
-objective with respect to the log-inflow parameters over a window of steps.
-``InflowObjective`` exposes that gradient as a ``torch.autograd.Function``.
+objective with respect to the log-inflow parameters and the drag field of a
+soft building mask over a window of steps.
+``WindObjective`` exposes that gradient (inflow parameters and soft building
+heights) as a ``torch.autograd.Function``.
 
 The reference has no derivatives; the operations differentiated are the ones
 of ``FvmSolverGpu.Step`` (Assets/Code/FvmSolver/FvmSolverGpu.cs:1050-1121)
@@ -19,6 +21,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import WfObjective, WindFvmError
+from .soft_mask import SoftBuildings
 from .solver import FvmSolverCuda
 
 PHASE_PREDICTOR, PHASE_SIMPLE, PHASE_FULL = 1, 2, 3
@@ -93,35 +96,44 @@ class AdjointSolver:
         return u, p
 
     def step_vjp(self, ubar: np.ndarray, pbar: np.ndarray, phases: int = PHASE_FULL):
-        """Adjoints of the step input (u, p) and of the six boundary planes for
-        output adjoints (ubar (3, N), pbar (N)).  Returns (ubar_in, pbar_in,
-        planes) with planes[f] of shape (3, points of plane f)."""
+        """Adjoints of the step input (u, p), of the six boundary planes and of
+        the drag field for output adjoints (ubar (3, N), pbar (N)).  Returns
+        (ubar_in, pbar_in, planes, dragbar) with planes[f] of shape
+        (3, points of plane f)."""
         n = self.solver.n_cells
         ub = np.ascontiguousarray(ubar, dtype=np.float32).reshape(3, n)
         pb = np.ascontiguousarray(pbar, dtype=np.float32).reshape(n)
         ui = np.empty((3, n), dtype=np.float32)
         pi = np.empty(n, dtype=np.float32)
         g = np.empty(3 * sum(self.plane_sizes), dtype=np.float32)
+        db = np.empty(n, dtype=np.float32)
         self._check(self._lib.wf_adj_step_vjp(self._a, int(phases), ub.ctypes.data, pb.ctypes.data, ui.ctypes.data,
-                                              pi.ctypes.data, g.ctypes.data))
+                                              pi.ctypes.data, g.ctypes.data, db.ctypes.data))
         planes, o = [], 0
         for s in self.plane_sizes:
             planes.append(g[o:o + 3 * s].reshape(3, s))
             o += 3 * s
-        return ui, pi, planes
+        return ui, pi, planes, db
 
-    def gradient(self, objective: Objective, n_steps: int, checkpoint_every: int = 1, include_init: bool = True):
+    def gradient(self, objective: Objective, n_steps: int, checkpoint_every: int = 1, include_init: bool = True,
+                 soft: SoftBuildings | None = None):
         """Advances the solver ``n_steps`` steps and returns a dict with the
-        objective J, dJ/du*, dJ/dz0 and the device times of the forward pass
-        and of the whole call (ms)."""
+        objective J, dJ/du*, dJ/dz0, dJ/dchi (the drag field, (N,)), the
+        device times of the forward pass and of the whole call (ms) and, when
+        ``soft`` describes the solver's drag field, dJ/dh per building."""
         J, gu, gz = c_double(0), c_double(0), c_double(0)
         tf, tt = c_float(0), c_float(0)
+        dd = np.empty(self.solver.n_cells, dtype=np.float32)
         obj = objective.to_c()
         self._check(self._lib.wf_adj_gradient(self._a, byref(obj), int(n_steps), int(checkpoint_every),
-                                              int(bool(include_init)), byref(J), byref(gu), byref(gz), byref(tf),
-                                              byref(tt)))
-        return {"J": J.value, "dJ_dustar": gu.value, "dJ_dz0": gz.value, "ms_forward": tf.value,
-                "ms_total": tt.value}
+                                              int(bool(include_init)), byref(J), byref(gu), byref(gz), dd.ctypes.data,
+                                              byref(tf), byref(tt)))
+        out = {"J": J.value, "dJ_dustar": gu.value, "dJ_dz0": gz.value, "dJ_ddrag": dd, "ms_forward": tf.value,
+               "ms_total": tt.value}
+        if soft is not None:
+            c = self.solver.cfg
+            out["dJ_dheights"] = soft.height_gradient(dd, c.nx, c.ny, c.nz)
+        return out
 
 
 def _torch():
@@ -129,12 +141,18 @@ def _torch():
     return torch
 
 
-class InflowObjective:
-    """``torch.autograd.Function`` of J(u*, z0): ``InflowObjective.apply(params,
-    make_solver, objective, n_steps, checkpoint_every)`` with ``params`` a
-    float64 tensor [u*, z0] and ``make_solver(ustar, z0)`` returning a freshly
-    initialised FvmSolverCuda (flags set, fields at the inflow profile).
-    The backward pass returns dJ/d(u*, z0) from the discrete adjoint."""
+class WindObjective:
+    """``torch.autograd.Function`` of the pedestrian-comfort objective J(u*,
+    z0[, h_1..h_n]):
+
+        J = WindObjective.apply(params, make_solver, objective, n_steps,
+                                checkpoint_every, soft)
+
+    ``params`` is a float64 tensor [u*, z0] or, with a SoftBuildings ``soft``,
+    [u*, z0, h_1, ..., h_n]; ``make_solver(ustar, z0, soft_or_None)`` returns
+    a freshly initialised FvmSolverCuda (flags set, fields at the inflow
+    profile, drag field from the soft buildings).  The backward pass returns
+    dJ/dparams from the discrete adjoint."""
 
     _fn = None
 
@@ -145,26 +163,30 @@ class InflowObjective:
 
             class _Fn(torch.autograd.Function):
                 @staticmethod
-                def forward(ctx, params, make_solver, objective, n_steps, checkpoint_every):
-                    us, z0 = (float(v) for v in params.detach().cpu().tolist())
-                    solver = make_solver(us, z0)
+                def forward(ctx, params, make_solver, objective, n_steps, checkpoint_every, soft):
+                    v = [float(x) for x in params.detach().cpu().tolist()]
+                    sb = soft.with_heights(v[2:]) if soft is not None else None
+                    solver = make_solver(v[0], v[1], sb)
                     try:
                         with AdjointSolver(solver) as adj:
-                            r = adj.gradient(objective, n_steps, checkpoint_every, include_init=True)
+                            r = adj.gradient(objective, n_steps, checkpoint_every, include_init=True, soft=sb)
                     finally:
                         solver.close()
-                    ctx.save_for_backward(torch.tensor([r["dJ_dustar"], r["dJ_dz0"]], dtype=params.dtype,
-                                                       device=params.device))
+                    g = [r["dJ_dustar"], r["dJ_dz0"]]
+                    if sb is not None:
+                        g += list(r["dJ_dheights"])
+                    ctx.save_for_backward(torch.tensor(g, dtype=params.dtype, device=params.device))
                     return torch.tensor(r["J"], dtype=params.dtype, device=params.device)
 
                 @staticmethod
                 def backward(ctx, gJ):
                     (g,) = ctx.saved_tensors
-                    return gJ * g, None, None, None, None
+                    return gJ * g, None, None, None, None, None
 
             cls._fn = _Fn
         return cls._fn
 
     @classmethod
-    def apply(cls, params, make_solver, objective: Objective, n_steps: int, checkpoint_every: int = 1):
-        return cls._function().apply(params, make_solver, objective, n_steps, checkpoint_every)
+    def apply(cls, params, make_solver, objective: Objective, n_steps: int, checkpoint_every: int = 1,
+              soft: SoftBuildings | None = None):
+        return cls._function().apply(params, make_solver, objective, n_steps, checkpoint_every, soft)

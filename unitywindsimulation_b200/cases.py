@@ -17,7 +17,7 @@ Workloads (synthetic, seeded):
                   u*=0.6 z0=0.3 with 5 % Gaussian inlet perturbation
   batch_directions 16 uneven grids 96..192 x 48..80(up) x 96..160, 8-32
                   buildings each, wind rotated by k * 22.5 degrees
-  adjoint_street  128 x 64(up) x 96, 12 buildings with continuous heights
+  adjoint_street  128 x 64(up) x 96, 12 soft buildings with continuous heights
   adjoint_batch   8 directions x 256 x 96(up) x 256, 64 buildings
 """
 from __future__ import annotations
@@ -29,6 +29,7 @@ import numpy as np
 
 from . import _lib
 from .config import default_config
+from .soft_mask import SoftBuildings
 
 MARGIN = 10  # building-free cells next to the x and z boundaries (BuildingVoxelizer.cs:379)
 KAPPA = 0.41
@@ -43,6 +44,7 @@ class Case:
     steps: int = 1
     seed: int | None = None
     buildings: list = dataclasses.field(default_factory=list)  # (x0, x1, z0, z1, height[, angle])
+    soft: SoftBuildings | None = None  # soft building mask (drag field), all cells fluid
 
     @property
     def n_cells(self) -> int:
@@ -213,16 +215,27 @@ def batch_directions(seed: int = 3, n_cases: int = 16, nv: int = 50, np_: int = 
 
 
 def adjoint_street(seed: int = 4, nv: int = 50, np_: int = 30, steps: int = 200) -> Case:
-    """128 x 64(up) x 96 cells, 12 buildings with continuous heights in
-    [4, 30] cells (the rasterised flags round them)."""
+    """128 x 64(up) x 96 cells of 0.5 m, 12 buildings on a street lattice
+    with footprints 6-16 cells and continuous heights in [4, 30] cells, as a
+    soft mask (sigmoid of width 1 cell, Brinkman drag 50/dt in solid cells;
+    every cell fluid).  PISO with turbulence off (the adjoint differentiates
+    the laminar step).  Objective patch: the 32 x 32 street region x 48..80,
+    z 32..64 at y index 3 (1.5-2.0 m), the last 100 of 200 steps,
+    checkpoints every 20 steps."""
     nx, ny, nz, dx = 128, 64, 96, 0.5
     rng = np.random.default_rng(seed)
     blds = street_lattice_buildings(rng, nx, nz, 12, 6, 16, 4, 30, integer_heights=False)
-    flags = remove_isolated_fluid(rasterise_boxes(nx, ny, nz, blds))
     ustar, z0 = 0.5, 0.1
     umax = float(log_profile((ny - 0.5) * dx, ustar, z0))
     cfg = _les_piso_cfg(nx, ny, nz, dx, cfl_dt(umax, dx), ustar, z0, 0.1, nv, np_)
-    return Case("adjoint_street", cfg, flags, None, steps, seed, blds)
+    cfg.turbulence = _lib.TURB_NONE
+    soft = SoftBuildings([b[:4] for b in blds], [b[4] for b in blds], chi_max=50.0 / cfg.dt, width=1.0)
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    return Case("adjoint_street", cfg, flags, None, steps, seed, blds, soft)
+
+
+ADJOINT_STREET_OBJECTIVE = dict(x0=48, x1=80, z0=32, z1=64, y=3, window=100)
+ADJOINT_STREET_CHECKPOINT = 20
 
 
 def aij_building(nv: int = 100, np_: int = 1000, steps: int = 1) -> Case:
@@ -271,12 +284,32 @@ def small_case(nx=24, ny=12, nz=16, piso=True, les=True, seed=0, nv=8, np_=12, b
     return Case(f"small_{nx}x{ny}x{nz}_s{seed}", cfg, flags, None, 1, seed, blds)
 
 
+def small_soft_case(nx=24, ny=12, nz=16, piso=True, seed=0, nv=6, np_=8, buildings=2) -> Case:
+    """Small seeded case with soft buildings (drag field, every cell fluid)
+    and turbulence off, for the adjoint tests."""
+    base = small_case(nx, ny, nz, piso=piso, les=False, seed=seed, nv=nv, np_=np_, buildings=0)
+    rng = np.random.default_rng(1000 + seed)
+    fps, hs = [], []
+    x = 5
+    for _ in range(buildings):
+        wx, wz = int(rng.integers(2, 4)), int(rng.integers(3, 6))
+        z0_ = int(rng.integers(2, max(3, nz - 2 - wz)))
+        fps.append((x, x + wx, z0_, z0_ + wz))
+        hs.append(float(rng.uniform(2.0, ny / 2)))
+        x += wx + int(rng.integers(3, 6))
+    soft = SoftBuildings(fps, hs, chi_max=50.0 / base.cfg.dt, width=1.0)
+    return Case(f"small_soft_{nx}x{ny}x{nz}_s{seed}", base.cfg, base.flags, None, 1, seed, [], soft)
+
+
 def apply_case(solver, case: Case) -> None:
     """Reference set-up order: flags after the fields (FvmSolverController.cs:
     368-375), then the inlet plane."""
     solver.InitFlags(case.flags)
     if case.inlet is not None:
         solver.set_inflow_plane(case.inlet)
+    if case.soft is not None:
+        c = case.cfg
+        solver.set_field(_lib.FIELD_DRAG, case.soft.drag(c.nx, c.ny, c.nz, np.float64).reshape(-1))
 
 
 WORKLOADS = {

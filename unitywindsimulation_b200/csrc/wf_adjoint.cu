@@ -472,13 +472,16 @@ __global__ void k_adj_vcoef(const __grid_constant__ Params P, const uint8_t* __r
 // VJP of PRE (CSVelPredictPreCompute with LES off, FvmColl.compute:1292-1859).
 __global__ void k_adj_pre(const __grid_constant__ Params P, const Bnd B, const BndBar G,
                           const uint8_t* __restrict__ fl, const float* __restrict__ Dbar,
-                          const float* __restrict__ bbar, float* __restrict__ uTbar, float* __restrict__ pbar) {
+                          const float* __restrict__ bbar, float* __restrict__ uTbar, float* __restrict__ pbar,
+                          float* __restrict__ dragbar) {
     Cell c;
     if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
     const size_t N = P.N;
     const float db[3] = {ld(Dbar, c.i), ld(Dbar, N + c.i), ld(Dbar, 2 * N + c.i)};
     const float bb[3] = {ld(bbar, c.i), ld(bbar, N + c.i), ld(bbar, 2 * N + c.i)};
     const float sD = db[0] + db[1] + db[2];
+    // Brinkman drag: D[k] += dv * drag for every k
+    dragbar[c.i] += P.dv * sD;
     // advection
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -601,6 +604,7 @@ struct wf_adjoint {
     float *cb = nullptr, *cb2 = nullptr, *ab = nullptr, *sb = nullptr, *sb2 = nullptr;
     float *aib = nullptr, *rb = nullptr, *Dpb = nullptr, *bpb = nullptr;
     float* gb = nullptr;   // adjoint of the 6 boundary planes (same layout)
+    float* dragb = nullptr;  // adjoint of the drag field (N)
     double* dJ = nullptr;  // device accumulator of the objective
     std::vector<float*> ck;  // stored states (4N each: u then p)
     std::string err;
@@ -655,7 +659,7 @@ int record_step(wf_adjoint* a, const float* u_in, const float* p_in, int phases)
     const size_t v = 3 * N * sizeof(float), s = N * sizeof(float);
     WFA_CUDA(cudaMemcpyAsync(a->uT, u_in, v, cudaMemcpyDeviceToDevice, st));
     WFA_CUDA(cudaMemcpyAsync(a->p0, p_in, s, cudaMemcpyDeviceToDevice, st));
-    wf::launch_vel_precompute(P, h->B, st, h->fl, a->uT, a->p0, h->eddy, h->face, nullptr, a->D, a->b);
+    wf::launch_vel_precompute(P, h->B, st, h->fl, a->uT, a->p0, h->eddy, h->face, nullptr, h->drag, a->D, a->b);
     wf::launch_vel_coef_ptr(P, st, h->fl, a->uT, h->eddy, h->face, a->D, a->A, a->iD);
     for (int k = 0; k <= a->nV; ++k)
         WFA_CUDA(cudaMemcpyAsync(U(a, a->uit, k), a->uT, v, cudaMemcpyDeviceToDevice, st));
@@ -772,7 +776,7 @@ int adjoint_step(wf_adjoint* a, int phases) {
     }
     wf::k_axpy<<<wf::lin_blocks(3 * (long long)N), 256, 0, st>>>(3 * (long long)N, 1.f, in, a->uTb);
     wf::k_adj_vcoef<<<g, bk, 0, st>>>(P, h->fl, a->Ab, a->iDb, a->iD, a->uTb, a->Db);
-    wf::k_adj_pre<<<g, bk, 0, st>>>(P, h->B, G, h->fl, a->Db, a->bb, a->uTb, a->pb_in);
+    wf::k_adj_pre<<<g, bk, 0, st>>>(P, h->B, G, h->fl, a->Db, a->bb, a->uTb, a->pb_in, a->dragb);
     (void)ustar;
     WFA_CUDA(cudaMemcpyAsync(a->ub, a->uTb, v, cudaMemcpyDeviceToDevice, st));
     WFA_CUDA(cudaMemcpyAsync(a->pb, a->pb_in, s, cudaMemcpyDeviceToDevice, st));
@@ -784,7 +788,7 @@ void free_adj(wf_adjoint* a) {
     float* ptrs[] = {a->uT, a->p0, a->D, a->b, a->A, a->iD, a->uit, a->Dp, a->bp, a->c3, a->ainv, a->qit, a->cbuf,
                      a->aod, a->pai, a->prhs, a->sit, a->uout, a->pout, a->ub, a->ub2, a->uTb, a->pb, a->pb_in,
                      a->Db, a->bb, a->Ab, a->iDb, a->c3b, a->cb, a->cb2, a->ab, a->sb, a->sb2, a->aib, a->rb,
-                     a->Dpb, a->bpb, a->gb};
+                     a->Dpb, a->bpb, a->gb, a->dragb};
     for (float* p : ptrs)
         if (p) cudaFree(p);
     if (a->dJ) cudaFree(a->dJ);
@@ -835,6 +839,7 @@ int wf_adj_create(wf_solver* h, wf_adjoint** out) {
     al(&a->cb, v); al(&a->cb2, v); al(&a->ab, v); al(&a->sb, s); al(&a->sb2, s);
     al(&a->aib, s); al(&a->rb, s); al(&a->Dpb, s); al(&a->bpb, s);
     al(&a->gb, plane_floats(h->P) * sizeof(float));
+    al(&a->dragb, s);
     if (ok) ok = cudaMalloc((void**)&a->dJ, sizeof(double)) == cudaSuccess;
     if (ok) ok = cudaStreamSynchronize(a->st) == cudaSuccess;
     if (!ok) {
@@ -858,7 +863,7 @@ int wf_adj_destroy(wf_adjoint* a) {
 const char* wf_adj_last_error(const wf_adjoint* a) { return a ? a->err.c_str() : "null adjoint"; }
 
 int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const float* pbar_out, float* ubar_in,
-                    float* pbar_in, float* gbar_planes) {
+                    float* pbar_in, float* gbar_planes, float* dragbar) {
     if (!a || phases < 1 || phases > 3 || !ubar_out || !pbar_out || !ubar_in || !pbar_in)
         return WF_ERR_INVALID_ARG;
     wf_solver* h = a->h;
@@ -871,6 +876,7 @@ int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const floa
     WFA_CUDA(cudaMemcpyAsync(a->ub, ubar_out, v, cudaMemcpyHostToDevice, a->st));
     WFA_CUDA(cudaMemcpyAsync(a->pb, pbar_out, s, cudaMemcpyHostToDevice, a->st));
     WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(h->P) * sizeof(float), a->st));
+    WFA_CUDA(cudaMemsetAsync(a->dragb, 0, s, a->st));
     st = adjoint_step(a, phases);
     if (st != WF_OK) return st;
     WFA_CUDA(cudaMemcpyAsync(ubar_in, a->ub, v, cudaMemcpyDeviceToHost, a->st));
@@ -878,6 +884,7 @@ int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const floa
     if (gbar_planes)
         WFA_CUDA(cudaMemcpyAsync(gbar_planes, a->gb, plane_floats(h->P) * sizeof(float), cudaMemcpyDeviceToHost,
                                  a->st));
+    if (dragbar) WFA_CUDA(cudaMemcpyAsync(dragbar, a->dragb, s, cudaMemcpyDeviceToHost, a->st));
     WFA_CUDA(cudaStreamSynchronize(a->st));
     return WF_OK;
 }
@@ -896,7 +903,8 @@ int wf_adj_step_forward(wf_adjoint* a, int phases, float* u_out, float* p_out) {
 }
 
 int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
-                    double* J, double* dJ_dustar, double* dJ_dz0, float* ms_forward, float* ms_total) {
+                    double* J, double* dJ_dustar, double* dJ_dz0, float* dJ_ddrag, float* ms_forward,
+                    float* ms_total) {
     if (!a || !obj || n_steps < 1 || checkpoint_every < 1) return WF_ERR_INVALID_ARG;
     wf_solver* h = a->h;
     const Params& P = h->P;
@@ -955,6 +963,7 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     WFA_CUDA(cudaMemsetAsync(a->ub, 0, v, a->st));
     WFA_CUDA(cudaMemsetAsync(a->pb, 0, s, a->st));
     WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(P) * sizeof(float), a->st));
+    WFA_CUDA(cudaMemsetAsync(a->dragb, 0, s, a->st));
     for (int sgi = nck - 1; sgi >= 0; --sgi) {
         const int n0 = sgi * C, n1 = std::min(n_steps, n0 + C);
         WFA_CUDA(cudaMemcpyAsync(seg[0], a->ck[sgi], v + s, cudaMemcpyDeviceToDevice, a->st));
@@ -1010,6 +1019,7 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
                 }
             }
     }
+    if (dJ_ddrag) WFA_CUDA(cudaMemcpy(dJ_ddrag, a->dragb, s, cudaMemcpyDeviceToHost));
     double Jh = 0.0;
     WFA_CUDA(cudaMemcpy(&Jh, a->dJ, sizeof(double), cudaMemcpyDeviceToHost));
     if (J) *J = Jh;

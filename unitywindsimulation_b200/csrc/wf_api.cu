@@ -114,7 +114,7 @@ void free_all(wf_solver* h) {
     wf::drop_graphs(h);
     void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->vb[3], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
                     h->pcb[0], h->pcb[1], h->pcb[2], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->grad, h->part, h->dsum, h->dref,
-                    h->dbad, h->stage, h->bnd[0]};
+                    h->dbad, h->stage, h->bnd[0], h->drag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->hsum) cudaFreeHost(h->hsum);
@@ -160,7 +160,7 @@ int do_les(wf_solver* h) {
 
 int do_vel_precompute(wf_solver* h) {
     wf::launch_vel_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->pr, h->eddy, h->face,
-                              h->P.les ? h->bv : nullptr, h->Dv, h->bv);
+                              h->P.les ? h->bv : nullptr, h->drag, h->Dv, h->bv);
     WF_CHECK_LAUNCH();
     return WF_OK;
 }
@@ -374,6 +374,7 @@ float* field_ptr(wf_solver* h, int field, size_t* points, int* comps) {
         case WF_FIELD_DP: return h->Dp;
         case WF_FIELD_BP: return h->bp;
         case WF_FIELD_EDDY_VIS: return h->eddy;
+        case WF_FIELD_DRAG: return h->drag;
         default: break;
     }
     if (field >= WF_FIELD_BND_X0 && field <= WF_FIELD_BND_ZN) {
@@ -744,6 +745,11 @@ int wf_set_state(wf_solver* h, const float* vel, const float* pres, int64_t step
 int wf_field_size(const wf_solver* hc, int field, size_t* points, int* comps) {
     wf_solver* h = const_cast<wf_solver*>(hc);
     if (!h || !points || !comps) return WF_ERR_INVALID_ARG;
+    if (field == WF_FIELD_DRAG) {  // stored only once set
+        *points = (size_t)h->P.N;
+        *comps = 1;
+        return WF_OK;
+    }
     if (!field_ptr(h, field, points, comps)) return WF_ERR_INVALID_ARG;
     return WF_OK;
 }
@@ -754,6 +760,10 @@ int wf_get_field(wf_solver* h, int field, float* out) {
     WF_CUDA(cudaSetDevice(h->device));
     if ((field == WF_FIELD_PRES_CORRECT || field == WF_FIELD_PRES_CORRECT_LAST_ITER) && h->pc_zero)
         WF_TRY(materialize_pc(h));
+    if (field == WF_FIELD_DRAG && !h->drag) {
+        for (int i = 0; i < h->P.N; ++i) out[i] = 0.f;
+        return WF_OK;
+    }
     size_t n = 0;
     int comps = 0;
     float* p = field_ptr(h, field, &n, &comps);
@@ -768,6 +778,12 @@ int wf_set_field(wf_solver* h, int field, const float* in) {
     WF_CUDA(cudaSetDevice(h->device));
     if (field == WF_FIELD_VEL_LAST_TIME || field == WF_FIELD_VEL_LAST_ITER) WF_TRY(materialize_iter(h));
     if (field == WF_FIELD_PRES_CORRECT || field == WF_FIELD_PRES_CORRECT_LAST_ITER) WF_TRY(materialize_pc(h));
+    if (field == WF_FIELD_DRAG && !h->drag) {
+        // first use: the captured step graphs hold the old (null) pointer
+        WF_TRY(sync(h));
+        wf::drop_graphs(h);
+        WF_TRY(alloc(h, (void**)&h->drag, sizeof(float) * h->P.N));
+    }
     size_t n = 0;
     int comps = 0;
     float* p = field_ptr(h, field, &n, &comps);

@@ -267,7 +267,8 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
 __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
                                  const float* __restrict__ uT, const float* __restrict__ pr,
                                  const float* __restrict__ eddy, const float* __restrict__ face,
-                                 const float* bles, float* __restrict__ Dv, float* bv) {
+                                 const float* bles, const float* __restrict__ drag, float* __restrict__ Dv,
+                                 float* bv) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     if (!fluid_at(fl, c.i)) return;
@@ -351,6 +352,12 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
     if (P.les && bles) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) b[k] += bles[k * N + c.i];
+    }
+    // Brinkman drag of a soft obstacle mask (no reference counterpart)
+    if (drag) {
+        const float t = P.dv * ld(drag, c.i);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) D[k] += t;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -863,9 +870,9 @@ void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8
     WF_LAUNCH(k_les_term, B, fl, uT, eddy, face, grad, bles);
 }
 void launch_vel_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
-                           const float* pr, const float* eddy, const float* face, const float* bles, float* Dv,
-                           float* bv) {
-    WF_LAUNCH(k_vel_precompute, B, fl, uT, pr, eddy, face, bles, Dv, bv);
+                           const float* pr, const float* eddy, const float* face, const float* bles,
+                           const float* drag, float* Dv, float* bv) {
+    WF_LAUNCH(k_vel_precompute, B, fl, uT, pr, eddy, face, bles, drag, Dv, bv);
 }
 void launch_vel_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uI, const float* uT,
                       const float* eddy, const float* face, const float* Dv, const float* bv, float* uo) {

@@ -18,9 +18,10 @@ void launch_cell_grad(const Params& P, const Bnd& B, cudaStream_t st, const uint
                       float* grad);
 void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
                      const float* eddy, const float* face, const float* grad, float* bles);
+// drag (nullable): Brinkman drag coefficient per cell, added to D as dv*drag.
 void launch_vel_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
-                           const float* pr, const float* eddy, const float* face, const float* bles, float* Dv,
-                           float* bv);
+                           const float* pr, const float* eddy, const float* face, const float* bles,
+                           const float* drag, float* Dv, float* bv);
 void launch_vel_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uI, const float* uT,
                       const float* eddy, const float* face, const float* Dv, const float* bv, float* uo);
 void launch_pres_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* u,

@@ -40,6 +40,7 @@ struct wf_solver {
     int iPC = 0, iPCL = 1;
     bool pc_zero = true;
     float *Dp = nullptr, *bp = nullptr, *eddy = nullptr;
+    float* drag = nullptr;    // Brinkman drag per cell (allocated when first set)
     float* bnd[6] = {};
     // sweep coefficient caches of the fast path (wf_sweeps.cu)
     float* pcoef = nullptr;   // pressure: c_E, c_N, c_U, 1/Dp, PISO rhs (5 planes)

@@ -1,0 +1,63 @@
+"""Soft building mask: buildings whose heights are continuous parameters.
+
+The reference marks obstacles with binary cell flags (InitFlags,
+FvmSolverGpu.cs:972-987), which have no derivative with respect to a
+building's height.  Here a building is a footprint (x0 <= x < x1,
+z0 <= z < z1) with a height h in cells, and every cell of the footprint
+column gets the solid fraction
+
+    alpha(y) = sigmoid((h - (y + 0.5)) / width)
+
+(1 well below the roof, 0 well above it, 1/2 at the roof line).  The
+fraction acts through a Brinkman drag chi = chi_max * alpha added to the
+momentum diagonal (WF_FIELD_DRAG), with every cell left fluid, so the flow
+depends smoothly on h.  ``height_gradient`` chains dJ/dchi (from the
+adjoint) to dJ/dh.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+
+def _sigmoid(t):
+    return 0.5 * (1.0 + np.tanh(0.5 * t))
+
+
+@dataclasses.dataclass
+class SoftBuildings:
+    footprints: list          # (x0, x1, z0, z1) per building, cells
+    heights: np.ndarray       # float64, cells
+    chi_max: float            # drag of a fully solid cell, 1/s
+    width: float = 1.0        # sigmoid width, cells
+
+    def __post_init__(self):
+        self.heights = np.asarray(self.heights, dtype=np.float64)
+        if len(self.footprints) != self.heights.size:
+            raise ValueError("one height per footprint")
+
+    def with_heights(self, heights) -> "SoftBuildings":
+        return dataclasses.replace(self, heights=np.asarray(heights, dtype=np.float64).copy())
+
+    def drag(self, nx: int, ny: int, nz: int, dtype=np.float32) -> np.ndarray:
+        """Drag field chi, shape (nz, ny, nx)."""
+        out = np.zeros((nz, ny, nx), dtype=np.float64)
+        yc = np.arange(ny, dtype=np.float64) + 0.5
+        for (x0, x1, z0, z1), h in zip(self.footprints, self.heights):
+            a = self.chi_max * _sigmoid((h - yc) / self.width)
+            out[z0:z1, :, x0:x1] = np.maximum(out[z0:z1, :, x0:x1], a[None, :, None])
+        return out.astype(dtype)
+
+    def height_gradient(self, dJ_ddrag: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
+        """dJ/dh per building from dJ/dchi (any shape with nz*ny*nx values).
+        Footprints must not overlap (the max in ``drag`` is then a plain
+        assignment)."""
+        g = np.asarray(dJ_ddrag, dtype=np.float64).reshape(nz, ny, nx)
+        yc = np.arange(ny, dtype=np.float64) + 0.5
+        out = np.zeros(self.heights.size)
+        for i, ((x0, x1, z0, z1), h) in enumerate(zip(self.footprints, self.heights)):
+            s = _sigmoid((h - yc) / self.width)
+            dchi_dh = self.chi_max * s * (1.0 - s) / self.width
+            out[i] = float((g[z0:z1, :, x0:x1].sum(axis=(0, 2)) * dchi_dh).sum())
+        return out
