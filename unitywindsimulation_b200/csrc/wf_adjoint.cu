@@ -122,53 +122,67 @@ __global__ void k_adj_pvel(const __grid_constant__ Params P, const uint8_t* __re
     aadd(ssbar + c.i, own);
 }
 
-// One reversed pressure-type sweep s^{k+1} = ai (r - C s^k): sb0 = adjoint of
-// s^k, plus the adjoints of r, ai and the face coefficients (owner cell holds
-// its E/N/U faces).  s_k == nullptr is the zero start.
-__global__ void k_adj_psweep(const __grid_constant__ Params P, const float* __restrict__ sb1,
-                             const float* __restrict__ s_k, const float* __restrict__ s_k1,
-                             const float* __restrict__ ai, const float* __restrict__ c3, float* __restrict__ sb0,
-                             float* __restrict__ c3bar, float* __restrict__ aibar, float* __restrict__ rbar) {
+// Reversed pressure-type Jacobi loop s^{k+1} = ai (r - C s^k), s^0 = 0,
+// k = 0..n-1, in the variable W^k = ai * sbar^k (sbar^k: adjoint of s^k):
+//   W^n = ai * sbar^n,   W^k = ai * (-C W^{k+1})
+// (C is symmetric, so the transposed sweep is the forward sweep with a zero
+// right-hand side, run by the multi-sweep kernel with every level kept),
+// then one pass over the stored iterates gives the adjoints of the loop's
+// inputs:  rbar = sum_k W^k,  coefbar = -sum_k W^k s^k (adjoint of 1/ai),
+// cbar_f(P) = -sum_k (W^k_P s^{k-1}_Q + W^k_Q s^{k-1}_P).
+__global__ void k_adj_pinit(int n, const float* __restrict__ ai, const float* __restrict__ sbar,
+                            float* __restrict__ W) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) W[i] = ai[i] * sbar[i];
+}
+// W: stack with W^k in slot n-k (k = 1..n), s: stack of s^0..s^n.
+__global__ void __launch_bounds__(256) k_adj_pacc(const __grid_constant__ Params P, int n,
+                                                  const float* __restrict__ ai, const float* __restrict__ W,
+                                                  const float* __restrict__ s, float* __restrict__ rbar,
+                                                  float* __restrict__ coefbar, float* __restrict__ c3bar) {
     Cell c;
     if (!thread_cell(P, c)) return;
     const size_t N = P.N;
-    const int sx = P.nx, sz = P.nx * P.ny;
-    const float* cE = c3;
-    const float* cN = c3 + N;
-    const float* cU = c3 + 2 * N;
-    auto w_at = [&](int q) { return ld(ai, q) * ld(sb1, q); };
-    const float wP = w_at(c.i);
-    float acc = 0.f;
-    if (c.x + 1 < P.nx) acc += ld(cE, c.i) * w_at(c.i + 1);
-    if (c.x > 0) acc += ld(cE, c.i - 1) * w_at(c.i - 1);
-    if (c.y + 1 < P.ny) acc += ld(cN, c.i) * w_at(c.i + sx);
-    if (c.y > 0) acc += ld(cN, c.i - sx) * w_at(c.i - sx);
-    if (c.z + 1 < P.nz) acc += ld(cU, c.i) * w_at(c.i + sz);
-    if (c.z > 0) acc += ld(cU, c.i - sz) * w_at(c.i - sz);
-    sb0[c.i] = -acc;
-    const float aiP = ld(ai, c.i);
-    if (aiP == 0.f) return;  // non-fluid cell: no equation
-    rbar[c.i] += wP;
-    aibar[c.i] += ld(sb1, c.i) * ld(s_k1, c.i) / aiP;
-    if (s_k) {
-        const float sP = ld(s_k, c.i);
-        if (c.x + 1 < P.nx) c3bar[c.i] += -(wP * ld(s_k, c.i + 1) + w_at(c.i + 1) * sP);
-        if (c.y + 1 < P.ny) c3bar[N + c.i] += -(wP * ld(s_k, c.i + sx) + w_at(c.i + sx) * sP);
-        if (c.z + 1 < P.nz) c3bar[2 * N + c.i] += -(wP * ld(s_k, c.i + sz) + w_at(c.i + sz) * sP);
+    if (ld(ai, c.i) == 0.f) {
+        rbar[c.i] = 0.f;
+        coefbar[c.i] = 0.f;
+        return;
     }
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const bool hE = c.x + 1 < P.nx, hN = c.y + 1 < P.ny, hU = c.z + 1 < P.nz;
+    float r = 0.f, d = 0.f, cE = 0.f, cN = 0.f, cU = 0.f;
+    for (int k = 1; k <= n; ++k) {
+        const float* Wk = W + (size_t)(n - k) * N;
+        const float* sk = s + (size_t)k * N;
+        const float* sm = s + (size_t)(k - 1) * N;
+        const float w = ld(Wk, c.i);
+        r += w;
+        d -= w * ld(sk, c.i);
+        if (k > 1) {
+            const float sP = ld(sm, c.i);
+            if (hE) cE -= w * ld(sm, c.i + 1) + ld(Wk, c.i + 1) * sP;
+            if (hN) cN -= w * ld(sm, c.i + sx) + ld(Wk, c.i + sx) * sP;
+            if (hU) cU -= w * ld(sm, c.i + sz) + ld(Wk, c.i + sz) * sP;
+        }
+    }
+    rbar[c.i] = r;
+    coefbar[c.i] = d;
+    c3bar[c.i] += cE;
+    c3bar[N + c.i] += cN;
+    c3bar[2 * N + c.i] += cU;
 }
 
 // VJP of PISOPRE: coef = -sum_f (dv/den) AdInv_f / dx, ai = 1/coef,
-// r = -sum_f s_f AdInv_f Aod_f (PisoColl.compute:196-255).
+// r = -sum_f s_f AdInv_f Aod_f (PisoColl.compute:196-255); coefbar is the
+// adjoint of coef.
 __global__ void k_adj_pisopre(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
-                              const float* __restrict__ aibar, const float* __restrict__ rbar,
-                              const float* __restrict__ ai, const float* __restrict__ Dv,
-                              const float* __restrict__ aod, float* __restrict__ abar, float* __restrict__ Dbar) {
+                              const float* __restrict__ coefbar, const float* __restrict__ rbar,
+                              const float* __restrict__ Dv, const float* __restrict__ aod, float* __restrict__ abar,
+                              float* __restrict__ Dbar) {
     Cell c;
     if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
     const size_t N = P.N;
-    const float aiP = ld(ai, c.i);
-    const float coefb = -ld(aibar, c.i) * aiP * aiP;
+    const float coefb = ld(coefbar, c.i);
     const float rb = ld(rbar, c.i);
     const float k = P.dv / P.den / P.dx;
 #pragma unroll
@@ -192,10 +206,10 @@ __global__ void k_adj_pisopre(const __grid_constant__ Params P, const uint8_t* _
 
 // VJP of the face coefficients c_f = (dv/den) 0.5 (1/D_P + 1/D_Q) / dx
 // (owner cell P holds its E/N/U faces).
-__global__ void k_adj_c3(const __grid_constant__ Params P, const float* __restrict__ c3bar,
-                         const float* __restrict__ Dv, float* __restrict__ Dbar) {
+__global__ void k_adj_c3(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                         const float* __restrict__ c3bar, const float* __restrict__ Dv, float* __restrict__ Dbar) {
     Cell c;
-    if (!thread_cell(P, c)) return;
+    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
     const size_t N = P.N;
     const float k = P.dv / P.den / P.dx;
 #pragma unroll
@@ -206,6 +220,7 @@ __global__ void k_adj_c3(const __grid_constant__ Params P, const float* __restri
         const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
         if (!in_region(P, X, Y, Z)) continue;
         const int q = cidx(P, X, Y, Z);
+        if (!fluid_at(fl, q)) continue;
         const float DP = ld(Dv, a * N + c.i), DQ = ld(Dv, a * N + q);
         aadd(Dbar + a * N + c.i, -0.5f * k * cb / (DP * DP));
         aadd(Dbar + a * N + q, -0.5f * k * cb / (DQ * DQ));
@@ -377,95 +392,113 @@ __global__ void k_adj_ppre(const __grid_constant__ Params P, const BndBar G,
     }
 }
 
-// ainv = 1/Dp (fluid): Dpbar += -aibar ainv^2
-__global__ void k_adj_inv(int n, const float* __restrict__ aibar, const float* __restrict__ ai,
-                          float* __restrict__ Dpbar) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float a = ai[i];
-    if (a != 0.f) Dpbar[i] += -aibar[i] * a * a;
-}
-
-// One reversed momentum sweep u^{k+1} = iD (A u^k + b) (fluid cells; non-fluid
-// cells keep their value).  ub0 = adjoint of u^k; accumulates the adjoints of
-// A (own faces), iD and b.
-__global__ void k_adj_vsweep(const __grid_constant__ Params P, const float* __restrict__ ub1,
-                             const float* __restrict__ u_k, const float* __restrict__ u_k1,
-                             const float* __restrict__ A, const float* __restrict__ iD, float* __restrict__ ub0,
-                             float* __restrict__ Abar, float* __restrict__ iDbar, float* __restrict__ bbar) {
+// Reversed momentum Jacobi loop u^{k+1} = iD (A u^k + b), u^0 = uT, in the
+// variable W^k = iD * ubar^k (fluid cells):
+//   W^n = iD * ubar^n,  W^k = iD * (A^T W^{k+1}),  ubar^0 = A^T W^1
+// (non-fluid cells keep their value through the loop, so their ubar^0 is
+// ubar^n).  A^T is stored per receiving cell: AT_f(Q) = A_{f^1}(nb_f(Q)),
+// the coefficient with which neighbour nb_f(Q) reads Q; it is 0 unless both
+// cells are fluid.
+__global__ void k_adj_vtrans(const __grid_constant__ Params P, const float* __restrict__ A, float* __restrict__ AT) {
     Cell c;
     if (!thread_cell(P, c)) return;
     const size_t N = P.N;
-    const int off[6] = {1, -1, P.nx, -P.nx, P.nx * P.ny, -P.nx * P.ny};
-    bool has[6];
-    has[0] = c.x + 1 < P.nx;
-    has[1] = c.x > 0;
-    has[2] = c.y + 1 < P.ny;
-    has[3] = c.y > 0;
-    has[4] = c.z + 1 < P.nz;
-    has[5] = c.z > 0;
-    const bool fluidP = ld(iD, c.i) != 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        AT[f * N + c.i] = in_region(P, X, Y, Z) ? ld(A, (size_t)(f ^ 1) * N + cidx(P, X, Y, Z)) : 0.f;
+    }
+}
+__global__ void k_adj_vinit(long long n3, const float* __restrict__ iD, const float* __restrict__ ubar,
+                            float* __restrict__ W) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n3) W[i] = iD[i] * ubar[i];
+}
+// kLast: out += ubar^0 (ubarN on non-fluid cells); else out = W^k.
+template <bool kLast>
+__global__ void __launch_bounds__(256) k_adj_vsweepT(const __grid_constant__ Params P, const float* __restrict__ AT,
+                                                     const float* __restrict__ iD, const float* __restrict__ Wi,
+                                                     const float* __restrict__ ubarN, float* __restrict__ out) {
+    Cell c;
+    if (!thread_cell(P, c)) return;
+    const size_t N = P.N;
+    if (kLast && ld(iD, c.i) == 0.f) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) out[k * N + c.i] += ld(ubarN, k * N + c.i);
+        return;
+    }
+    // non-fluid cells: AT = 0 and iD = 0, so W^k = 0 there without a test
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const int iE = c.x + 1 < P.nx ? c.i + 1 : c.i, iW = c.x > 0 ? c.i - 1 : c.i;
+    const int iN = c.y + 1 < P.ny ? c.i + sx : c.i, iS = c.y > 0 ? c.i - sx : c.i;
+    const int iU = c.z + 1 < P.nz ? c.i + sz : c.i, iDn = c.z > 0 ? c.i - sz : c.i;
+    const float t0 = ld(AT, c.i), t1 = ld(AT, N + c.i), t2 = ld(AT, 2 * N + c.i);
+    const float t3 = ld(AT, 3 * N + c.i), t4 = ld(AT, 4 * N + c.i), t5 = ld(AT, 5 * N + c.i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        // gather: neighbour P' = Q + d holds the coefficient of Q on its face
-        // pointing back (opposite of d)
-        float acc = fluidP ? 0.f : ld(ub1, k * N + c.i);
+        const float* w = Wi + k * N;
+        float s = t0 * ld(w, iE);
+        s += t1 * ld(w, iW);
+        s += t2 * ld(w, iN);
+        s += t3 * ld(w, iS);
+        s += t4 * ld(w, iU);
+        s += t5 * ld(w, iDn);
+        if (kLast) out[k * N + c.i] += s;
+        else out[k * N + c.i] = ld(iD, k * N + c.i) * s;
+    }
+}
+// One pass over the loop's iterates (u: stack u^0..u^n, W: stack W^1..W^n,
+// slot k at k*3N): bbar = sum_k W^k, Dbar -= sum_k W^k u^k (adjoint of 1/D
+// folded in), Abar_f = sum_k W^k . u^{k-1}_nb, and the adjoint of
+// A_f = nu ds/dx - s_f ds/4 (uT_P[a] + uT_Q[a]) scattered to uTbar.
+__global__ void __launch_bounds__(256) k_adj_vacc(const __grid_constant__ Params P, int n,
+                                                  const uint8_t* __restrict__ fl, const float* __restrict__ W,
+                                                  const float* __restrict__ u, float* __restrict__ bbar,
+                                                  float* __restrict__ Dbar, float* __restrict__ uTbar) {
+    Cell c;
+    if (!thread_cell(P, c)) return;
+    const size_t N = P.N, N3 = 3 * N;
+    if (!fluid_at(fl, c.i)) return;
+    int nb[6];
+    bool has[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        has[f] = in_region(P, X, Y, Z) && fluid_at(fl, cidx(P, X, Y, Z));
+        nb[f] = has[f] ? cidx(P, X, Y, Z) : c.i;
+    }
+    float Ab[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float bb[3] = {0.f, 0.f, 0.f}, db[3] = {0.f, 0.f, 0.f};
+#pragma unroll 2
+    for (int k = 1; k <= n; ++k) {
+        const float* Wk = W + k * N3;
+        const float* uk = u + k * N3;
+        const float* um = u + (k - 1) * N3;
+        float w[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            w[j] = ld(Wk, j * N + c.i);
+            bb[j] += w[j];
+            db[j] -= w[j] * ld(uk, j * N + c.i);
+        }
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
             if (!has[f]) continue;
-            const int nb = c.i + off[f];
-            const int back = f ^ 1;
-            const float coef = ld(A, (size_t)back * N + nb);
-            if (coef != 0.f) acc += coef * ld(iD, k * N + nb) * ld(ub1, k * N + nb);
+            Ab[f] += w[0] * ld(um, nb[f]) + w[1] * ld(um, N + nb[f]) + w[2] * ld(um, 2 * N + nb[f]);
         }
-        ub0[k * N + c.i] = acc;
     }
-    if (!fluidP) return;
-    float w[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float d = ld(iD, k * N + c.i);
-        const float u1 = ld(ub1, k * N + c.i);
-        w[k] = d * u1;
-        bbar[k * N + c.i] += w[k];
-        iDbar[k * N + c.i] += u1 * ld(u_k1, k * N + c.i) / d;
+    for (int j = 0; j < 3; ++j) {
+        bbar[j * N + c.i] = bb[j];
+        aadd(Dbar + j * N + c.i, db[j]);
     }
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        if (!has[f]) continue;  // faces that are not fluid-fluid are dropped in k_adj_vcoef
-        const int nb = c.i + off[f];
-        float t = 0.f;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) t += w[k] * ld(u_k, k * N + nb);
-        Abar[(size_t)f * N + c.i] += t;
-    }
-}
-
-// VJP of VCOEF: A_f = nu ds/dx - s_f ds/4 (uT_P[a] + uT_Q[a]) on fluid faces,
-// iD = 1/D.
-__global__ void k_adj_vcoef(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
-                            const float* __restrict__ Abar, const float* __restrict__ iDbar,
-                            const float* __restrict__ iD, float* __restrict__ uTbar, float* __restrict__ Dbar) {
-    Cell c;
-    if (!thread_cell(P, c) || !fluid_at(fl, c.i)) return;
-    const size_t N = P.N;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float d = ld(iD, k * N + c.i);
-        aadd(Dbar + k * N + c.i, -ld(iDbar, k * N + c.i) * d * d);
-    }
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        const float ab = ld(Abar, (size_t)f * N + c.i);
-        if (ab == 0.f) continue;
+        if (!has[f]) continue;
         const int a = face_axis(f), s = face_sign(f);
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (!in_region(P, X, Y, Z)) continue;
-        const int q = cidx(P, X, Y, Z);
-        if (!fluid_at(fl, q)) continue;
-        const float t = -s * P.ds * 0.25f * ab;
+        const float t = -s * P.ds * 0.25f * Ab[f];
         aadd(uTbar + a * N + c.i, t);
-        aadd(uTbar + a * N + q, t);
+        aadd(uTbar + a * N + nb[f], t);
     }
 }
 
@@ -584,28 +617,37 @@ int lin_blocks(long long n) { return (int)((n + 255) / 256); }
 }  // namespace wf
 
 // =====================================================================
+namespace {
+// Everything one forward step leaves behind for its adjoint.
+struct Tape {
+    float *uT = nullptr, *p0 = nullptr;         // step input
+    float *D = nullptr, *b = nullptr;           // momentum diagonal, rhs (3N each)
+    float *A = nullptr, *iD = nullptr;          // sweep coefficients (6N, 3N)
+    float* uit = nullptr;                       // u^0..u^nV ((nV+1) x 3N)
+    float *Dp = nullptr, *bp = nullptr, *c3 = nullptr, *ainv = nullptr;
+    float* qit = nullptr;                       // q^0..q^nP ((nP+1) x N)
+    float* cbuf = nullptr;                      // corrections c_0..c_nC ((nC+1) x 3N)
+    float *aod = nullptr, *pai = nullptr, *prhs = nullptr;  // per PISO corrector
+    float* sit = nullptr;                       // s^0..s^nP per corrector
+    float *uout = nullptr, *pout = nullptr;     // step output
+};
+}  // namespace
+
 struct wf_adjoint {
     wf_solver* h = nullptr;
     cudaStream_t st = nullptr;
     int nV = 0, nP = 0, nC = 0;
     size_t N = 0;
-    // tape of one step
-    float *uT = nullptr, *p0 = nullptr, *D = nullptr, *b = nullptr, *A = nullptr, *iD = nullptr;
-    float* uit = nullptr;  // (nV+1) x 3N
-    float *Dp = nullptr, *bp = nullptr, *c3 = nullptr, *ainv = nullptr;
-    float* qit = nullptr;  // (nP+1) x N
-    float* cbuf = nullptr; // (nC+1) x 3N corrections c_1..c_{nC+1}
-    float *aod = nullptr, *pai = nullptr, *prhs = nullptr;  // nC x 3N, nC x N, nC x N
-    float* sit = nullptr;  // nC x (nP+1) x N
-    float *uout = nullptr, *pout = nullptr;
+    std::vector<Tape> tapes;                    // tapes[0] always allocated
+    std::vector<void*> blocks;                  // allocations behind the tapes
     // adjoint work
-    float *ub = nullptr, *ub2 = nullptr, *uTb = nullptr, *pb = nullptr, *pb_in = nullptr;
-    float *Db = nullptr, *bb = nullptr, *Ab = nullptr, *iDb = nullptr, *c3b = nullptr;
-    float *cb = nullptr, *cb2 = nullptr, *ab = nullptr, *sb = nullptr, *sb2 = nullptr;
-    float *aib = nullptr, *rb = nullptr, *Dpb = nullptr, *bpb = nullptr;
-    float* gb = nullptr;   // adjoint of the 6 boundary planes (same layout)
+    float *ub = nullptr, *uTb = nullptr, *pb = nullptr, *pb_in = nullptr;
+    float *Db = nullptr, *bb = nullptr, *AT = nullptr, *Wv = nullptr, *Wp = nullptr, *c3b = nullptr;
+    float *cb = nullptr, *cb2 = nullptr, *ab = nullptr, *sb = nullptr;
+    float *rb = nullptr, *dgb = nullptr;
+    float* gb = nullptr;     // adjoint of the 6 boundary planes (same layout)
     float* dragb = nullptr;  // adjoint of the drag field (N)
-    double* dJ = nullptr;  // device accumulator of the objective
+    double* dJ = nullptr;    // device accumulator of the objective
     std::vector<float*> ck;  // stored states (4N each: u then p)
     std::string err;
 };
@@ -628,9 +670,11 @@ int adj_fail(wf_adjoint* a, int code, const char* msg) {
         }                                                                      \
     } while (0)
 
-float* U(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * 3 * a->N; }
-float* S1(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * a->N; }
-float* SIT(const wf_adjoint* a, int m, int k) { return a->sit + ((size_t)m * (a->nP + 1) + k) * a->N; }
+float* V(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * 3 * a->N; }
+float* S(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * a->N; }
+float* SIT(const wf_adjoint* a, const Tape& t, int m, int k) {
+    return t.sit + ((size_t)m * (a->nP + 1) + k) * a->N;
+}
 
 wf::BndBar bnd_bar(const wf_adjoint* a) {
     wf::BndBar G;
@@ -648,61 +692,114 @@ size_t plane_floats(const Params& P) {
     return n;
 }
 
-// Forward step from (u_in, p_in) with every intermediate kept.  phases: 1 =
-// stop after the momentum predictor, 2 = after the SIMPLE correction, 3 = the
-// whole step.  Output state in uout / pout.
-int record_step(wf_adjoint* a, const float* u_in, const float* p_in, int phases) {
+// Floats of one tape, carved from one allocation.
+size_t tape_floats(const wf_adjoint* a) {
+    const size_t N = a->N, nC1 = a->nC > 0 ? a->nC : 1;
+    return N * (3 + 1 + 3 + 3 + 6 + 3 + 3 * (a->nV + 1) + 4 + 3 + (a->nP + 1) + 3 * (a->nC + 1) + nC1 * (3 + 1 + 1) +
+                nC1 * (a->nP + 1) + 3 + 1);
+}
+void carve(const wf_adjoint* a, float* base, Tape& t) {
+    const size_t N = a->N, nC1 = a->nC > 0 ? a->nC : 1;
+    float* p = base;
+    auto take = [&](float** dst, size_t n) {
+        *dst = p;
+        p += n;
+    };
+    take(&t.uT, 3 * N); take(&t.p0, N); take(&t.D, 3 * N); take(&t.b, 3 * N); take(&t.A, 6 * N);
+    take(&t.iD, 3 * N); take(&t.uit, 3 * N * (a->nV + 1)); take(&t.Dp, N); take(&t.bp, N); take(&t.c3, 3 * N);
+    take(&t.ainv, N); take(&t.qit, N * (a->nP + 1)); take(&t.cbuf, 3 * N * (a->nC + 1)); take(&t.aod, 3 * N * nC1);
+    take(&t.pai, N * nC1); take(&t.prhs, N * nC1); take(&t.sit, N * nC1 * (a->nP + 1)); take(&t.uout, 3 * N);
+    take(&t.pout, N);
+}
+int ensure_tapes(wf_adjoint* a, int n) {
+    if ((int)a->tapes.size() >= n) return WF_OK;
+    const size_t bytes = tape_floats(a) * sizeof(float);
+    while ((int)a->tapes.size() < n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return adj_fail(a, WF_ERR_OOM, "no device memory for the step tapes: lower checkpoint_every");
+        }
+        a->blocks.push_back(p);
+        Tape t;
+        carve(a, (float*)p, t);
+        a->tapes.push_back(t);
+    }
+    return WF_OK;
+}
+
+// Forward step from (u_in, p_in) into tape t with every intermediate kept.
+// phases: 1 = stop after the momentum predictor, 2 = after the SIMPLE
+// correction, 3 = the whole step.  Output state in t.uout / t.pout.
+int record_step(wf_adjoint* a, Tape& t, const float* u_in, const float* p_in, int phases) {
     wf_solver* h = a->h;
     const Params& P = h->P;
     cudaStream_t st = a->st;
     const size_t N = a->N;
     const size_t v = 3 * N * sizeof(float), s = N * sizeof(float);
-    WFA_CUDA(cudaMemcpyAsync(a->uT, u_in, v, cudaMemcpyDeviceToDevice, st));
-    WFA_CUDA(cudaMemcpyAsync(a->p0, p_in, s, cudaMemcpyDeviceToDevice, st));
-    wf::launch_vel_precompute(P, h->B, st, h->fl, a->uT, a->p0, h->eddy, h->face, nullptr, h->drag, a->D, a->b);
-    wf::launch_vel_coef_ptr(P, st, h->fl, a->uT, h->eddy, h->face, a->D, a->A, a->iD);
-    for (int k = 0; k <= a->nV; ++k)
-        WFA_CUDA(cudaMemcpyAsync(U(a, a->uit, k), a->uT, v, cudaMemcpyDeviceToDevice, st));
+    WFA_CUDA(cudaMemcpyAsync(t.uT, u_in, v, cudaMemcpyDeviceToDevice, st));
+    WFA_CUDA(cudaMemcpyAsync(t.p0, p_in, s, cudaMemcpyDeviceToDevice, st));
+    wf::launch_vel_precompute(P, h->B, st, h->fl, t.uT, t.p0, h->eddy, h->face, nullptr, h->drag, t.D, t.b);
+    wf::launch_vel_coef_ptr(P, st, h->fl, t.uT, h->eddy, h->face, t.D, t.A, t.iD);
+    WFA_CUDA(cudaMemcpyAsync(V(a, t.uit, 0), t.uT, v, cudaMemcpyDeviceToDevice, st));
     for (int k = 0; k < a->nV; ++k)
-        wf::launch_vel_sweep1_ptr(P, st, a->A, a->iD, a->b, U(a, a->uit, k), U(a, a->uit, k + 1));
-    const float* ustar = U(a, a->uit, a->nV);
-    WFA_CUDA(cudaMemcpyAsync(a->uout, ustar, v, cudaMemcpyDeviceToDevice, st));
-    WFA_CUDA(cudaMemcpyAsync(a->pout, a->p0, s, cudaMemcpyDeviceToDevice, st));
+        wf::launch_vel_sweep1_ptr(P, st, t.A, t.iD, t.b, V(a, t.uit, k), V(a, t.uit, k + 1));
+    const float* ustar = V(a, t.uit, a->nV);
+    WFA_CUDA(cudaMemcpyAsync(t.uout, ustar, v, cudaMemcpyDeviceToDevice, st));
+    WFA_CUDA(cudaMemcpyAsync(t.pout, t.p0, s, cudaMemcpyDeviceToDevice, st));
     if (phases >= 2) {
-        wf::launch_pres_precompute(P, h->B, st, h->fl, ustar, a->p0, a->D, a->Dp, a->bp);
-        wf::launch_pres_coef_ptr(P, st, h->fl, a->D, a->c3);
-        wf::launch_inv_ptr(P, st, h->fl, a->Dp, a->ainv);
-        WFA_CUDA(cudaMemsetAsync(a->qit, 0, (size_t)(a->nP + 1) * s, st));
-        for (int k = 0; k < a->nP; ++k)
-            wf::launch_pres_sweep1_ptr(P, st, a->c3, a->ainv, a->bp, k == 0 ? nullptr : S1(a, a->qit, k),
-                                       S1(a, a->qit, k + 1));
-        const float* q = S1(a, a->qit, a->nP);
-        WFA_CUDA(cudaMemsetAsync(a->cbuf, 0, (size_t)(a->nC + 1) * v, st));
-        wf::launch_apply_vel(P, st, h->fl, q, a->D, U(a, a->cbuf, 0), a->uout);
-        wf::launch_apply_pres(P, st, h->fl, q, a->pout);
+        wf::launch_pres_precompute(P, h->B, st, h->fl, ustar, t.p0, t.D, t.Dp, t.bp);
+        wf::launch_pres_coef_ptr(P, st, h->fl, t.D, t.c3);
+        wf::launch_inv_ptr(P, st, h->fl, t.Dp, t.ainv);
+        WFA_CUDA(cudaMemsetAsync(t.qit, 0, s, st));
+        wf::launch_pres_stack(P, st, h->num_sms, t.c3, t.ainv, t.bp, t.qit, a->nP, true);
+        const float* q = S(a, t.qit, a->nP);
+        WFA_CUDA(cudaMemsetAsync(t.cbuf, 0, v, st));
+        wf::launch_apply_vel(P, st, h->fl, q, t.D, V(a, t.cbuf, 0), t.uout);
+        wf::launch_apply_pres(P, st, h->fl, q, t.pout);
     }
     if (phases >= 3) {
-        WFA_CUDA(cudaMemsetAsync(a->aod, 0, (size_t)a->nC * v, st));
-        WFA_CUDA(cudaMemsetAsync(a->sit, 0, (size_t)a->nC * (a->nP + 1) * s, st));
         for (int m = 0; m < a->nC; ++m) {
-            wf::launch_piso_aodu(P, st, h->fl, U(a, a->cbuf, m), a->uT, h->eddy, h->face, U(a, a->aod, m));
-            wf::launch_piso_pre_ptr(P, st, h->fl, a->D, U(a, a->aod, m), S1(a, a->pai, m), S1(a, a->prhs, m));
-            for (int k = 0; k < a->nP; ++k)
-                wf::launch_pres_sweep1_ptr(P, st, a->c3, S1(a, a->pai, m), S1(a, a->prhs, m),
-                                           k == 0 ? nullptr : SIT(a, m, k), SIT(a, m, k + 1));
-            const float* ss = SIT(a, m, a->nP);
-            wf::launch_apply_pres(P, st, h->fl, ss, a->pout);
-            wf::launch_piso_vel(P, st, h->fl, ss, a->D, U(a, a->aod, m), U(a, a->cbuf, m + 1), a->uout);
+            WFA_CUDA(cudaMemsetAsync(V(a, t.aod, m), 0, v, st));
+            WFA_CUDA(cudaMemsetAsync(V(a, t.cbuf, m + 1), 0, v, st));
+            WFA_CUDA(cudaMemsetAsync(SIT(a, t, m, 0), 0, s, st));
+            wf::launch_piso_aodu(P, st, h->fl, V(a, t.cbuf, m), t.uT, h->eddy, h->face, V(a, t.aod, m));
+            wf::launch_piso_pre_ptr(P, st, h->fl, t.D, V(a, t.aod, m), S(a, t.pai, m), S(a, t.prhs, m));
+            wf::launch_pres_stack(P, st, h->num_sms, t.c3, S(a, t.pai, m), S(a, t.prhs, m), SIT(a, t, m, 0),
+                                  a->nP, true);
+            const float* ss = SIT(a, t, m, a->nP);
+            wf::launch_apply_pres(P, st, h->fl, ss, t.pout);
+            wf::launch_piso_vel(P, st, h->fl, ss, t.D, V(a, t.aod, m), V(a, t.cbuf, m + 1), t.uout);
         }
     }
     WFA_CUDA(cudaGetLastError());
     return WF_OK;
 }
 
+// Reversed pressure-type loop: on entry a->sb holds the adjoint of the final
+// iterate; on exit a->rb holds the adjoint of the right-hand side, a->dgb the
+// adjoint of the diagonal coefficient (1/ai), and a->c3b has the face
+// coefficient adjoints added.  sstack: the loop's iterates s^0..s^n.
+void reverse_pres_loop(wf_adjoint* a, const float* ai, const float* c3, const float* sstack) {
+    const Params& P = a->h->P;
+    cudaStream_t st = a->st;
+    const dim3 g = wf::cgrd(P), bk = wf::cblk();
+    const int n = a->nP;
+    if (n == 0) {
+        cudaMemsetAsync(a->rb, 0, a->N * sizeof(float), st);
+        cudaMemsetAsync(a->dgb, 0, a->N * sizeof(float), st);
+        return;
+    }
+    // slot j of a->Wp holds W^{n-j}
+    wf::k_adj_pinit<<<wf::lin_blocks(a->N), 256, 0, st>>>((int)a->N, ai, a->sb, a->Wp);
+    if (n > 1) wf::launch_pres_stack(P, st, a->h->num_sms, c3, ai, nullptr, a->Wp, n - 1, false);
+    wf::k_adj_pacc<<<g, bk, 0, st>>>(P, n, ai, a->Wp, sstack, a->rb, a->dgb, a->c3b);
+}
+
 // Reverse of record_step: on entry a->ub / a->pb hold the adjoints of
-// (uout, pout); on exit they hold the adjoints of (u_in, p_in), and a->gb
-// has the boundary-plane adjoints added.
-int adjoint_step(wf_adjoint* a, int phases) {
+// (uout, pout); on exit they hold the adjoints of (uT, p0), and a->gb /
+// a->dragb have the boundary-plane and drag adjoints added.
+int adjoint_step(wf_adjoint* a, const Tape& t, int phases) {
     wf_solver* h = a->h;
     const Params& P = h->P;
     cudaStream_t st = a->st;
@@ -714,70 +811,48 @@ int adjoint_step(wf_adjoint* a, int phases) {
     WFA_CUDA(cudaMemsetAsync(a->Db, 0, v, st));
     WFA_CUDA(cudaMemsetAsync(a->c3b, 0, v, st));
     WFA_CUDA(cudaMemcpyAsync(a->pb_in, a->pb, s, cudaMemcpyDeviceToDevice, st));
-    const float* ustar = U(a, a->uit, a->nV);
+    if (phases >= 2) WFA_CUDA(cudaMemcpyAsync(a->cb, a->ub, v, cudaMemcpyDeviceToDevice, st));
     if (phases >= 3) {
-        // cb = adjoint of the newest correction
-        WFA_CUDA(cudaMemcpyAsync(a->cb, a->ub, v, cudaMemcpyDeviceToDevice, st));
+        // a->cb: adjoint of the newest correction
         for (int m = a->nC - 1; m >= 0; --m) {
             WFA_CUDA(cudaMemsetAsync(a->ab, 0, v, st));
             WFA_CUDA(cudaMemsetAsync(a->sb, 0, s, st));
-            const float* ss = SIT(a, m, a->nP);
-            wf::k_adj_pvel<<<g, bk, 0, st>>>(P, h->fl, a->cb, ss, a->D, U(a, a->aod, m), a->ab, a->sb, a->Db);
+            const float* ss = SIT(a, t, m, a->nP);
+            wf::k_adj_pvel<<<g, bk, 0, st>>>(P, h->fl, a->cb, ss, t.D, V(a, t.aod, m), a->ab, a->sb, a->Db);
             wf::k_add_masked<<<wf::lin_blocks(N), 256, 0, st>>>((int)N, h->fl, a->pb, a->sb);
-            WFA_CUDA(cudaMemsetAsync(a->aib, 0, s, st));
-            WFA_CUDA(cudaMemsetAsync(a->rb, 0, s, st));
-            float* in = a->sb;
-            float* out = a->sb2;
-            for (int k = a->nP - 1; k >= 0; --k) {
-                wf::k_adj_psweep<<<g, bk, 0, st>>>(P, in, k == 0 ? nullptr : SIT(a, m, k), SIT(a, m, k + 1),
-                                                   S1(a, a->pai, m), a->c3, out, a->c3b, a->aib, a->rb);
-                std::swap(in, out);
-            }
-            wf::k_adj_pisopre<<<g, bk, 0, st>>>(P, h->fl, a->aib, a->rb, S1(a, a->pai, m), a->D, U(a, a->aod, m),
-                                                a->ab, a->Db);
-            // adjoint of c_m: the velocity adjoint (u_m = u_{m-1} + c_m) plus
-            // its use in AOD
+            reverse_pres_loop(a, S(a, t.pai, m), t.c3, SIT(a, t, m, 0));
+            wf::k_adj_pisopre<<<g, bk, 0, st>>>(P, h->fl, a->dgb, a->rb, t.D, V(a, t.aod, m), a->ab, a->Db);
+            // adjoint of c_m: the velocity adjoint (u gains c_m) plus its use in AOD
             WFA_CUDA(cudaMemcpyAsync(a->cb2, a->ub, v, cudaMemcpyDeviceToDevice, st));
-            wf::k_adj_aod<<<g, bk, 0, st>>>(P, h->fl, a->ab, U(a, a->cbuf, m), a->uT, a->cb2, a->uTb);
+            wf::k_adj_aod<<<g, bk, 0, st>>>(P, h->fl, a->ab, V(a, t.cbuf, m), t.uT, a->cb2, a->uTb);
             std::swap(a->cb, a->cb2);
         }
-    } else if (phases >= 2) {
-        WFA_CUDA(cudaMemcpyAsync(a->cb, a->ub, v, cudaMemcpyDeviceToDevice, st));
     }
     if (phases >= 2) {
-        const float* q = S1(a, a->qit, a->nP);
+        const float* q = S(a, t.qit, a->nP);
         WFA_CUDA(cudaMemsetAsync(a->sb, 0, s, st));
-        wf::k_adj_corr<<<g, bk, 0, st>>>(P, h->fl, a->cb, q, a->D, a->sb, a->Db);
+        wf::k_adj_corr<<<g, bk, 0, st>>>(P, h->fl, a->cb, q, t.D, a->sb, a->Db);
         wf::k_add_masked<<<wf::lin_blocks(N), 256, 0, st>>>((int)N, h->fl, a->pb, a->sb);
-        WFA_CUDA(cudaMemsetAsync(a->aib, 0, s, st));
-        WFA_CUDA(cudaMemsetAsync(a->bpb, 0, s, st));
-        float* in = a->sb;
-        float* out = a->sb2;
-        for (int k = a->nP - 1; k >= 0; --k) {
-            wf::k_adj_psweep<<<g, bk, 0, st>>>(P, in, k == 0 ? nullptr : S1(a, a->qit, k), S1(a, a->qit, k + 1),
-                                               a->ainv, a->c3, out, a->c3b, a->aib, a->bpb);
-            std::swap(in, out);
-        }
-        WFA_CUDA(cudaMemsetAsync(a->Dpb, 0, s, st));
-        wf::k_adj_inv<<<wf::lin_blocks(N), 256, 0, st>>>((int)N, a->aib, a->ainv, a->Dpb);
-        wf::k_adj_c3<<<g, bk, 0, st>>>(P, a->c3b, a->D, a->Db);
-        wf::k_adj_ppre<<<g, bk, 0, st>>>(P, G, h->fl, a->Dpb, a->bpb, a->p0, a->D, a->ub, a->pb_in, a->Db);
+        reverse_pres_loop(a, t.ainv, t.c3, t.qit);
+        // a->rb: adjoint of bp; a->dgb: adjoint of Dp
+        wf::k_adj_c3<<<g, bk, 0, st>>>(P, h->fl, a->c3b, t.D, a->Db);
+        wf::k_adj_ppre<<<g, bk, 0, st>>>(P, G, h->fl, a->dgb, a->rb, t.p0, t.D, a->ub, a->pb_in, a->Db);
     }
-    // momentum sweeps in reverse; a->ub is the adjoint of u*
-    WFA_CUDA(cudaMemsetAsync(a->Ab, 0, 2 * v, st));
-    WFA_CUDA(cudaMemsetAsync(a->iDb, 0, v, st));
-    WFA_CUDA(cudaMemsetAsync(a->bb, 0, v, st));
-    float* in = a->ub;
-    float* out = a->ub2;
-    for (int k = a->nV - 1; k >= 0; --k) {
-        wf::k_adj_vsweep<<<g, bk, 0, st>>>(P, in, U(a, a->uit, k), U(a, a->uit, k + 1), a->A, a->iD, out, a->Ab,
-                                           a->iDb, a->bb);
-        std::swap(in, out);
+    // momentum loop in reverse; a->ub is the adjoint of u*
+    if (a->nV > 0) {
+        const int n = a->nV;
+        wf::k_adj_vtrans<<<g, bk, 0, st>>>(P, t.A, a->AT);
+        wf::k_adj_vinit<<<wf::lin_blocks(3 * (long long)N), 256, 0, st>>>(3 * (long long)N, t.iD, a->ub,
+                                                                           V(a, a->Wv, n));
+        for (int k = n - 1; k >= 1; --k)
+            wf::k_adj_vsweepT<false><<<g, bk, 0, st>>>(P, a->AT, t.iD, V(a, a->Wv, k + 1), nullptr, V(a, a->Wv, k));
+        wf::k_adj_vsweepT<true><<<g, bk, 0, st>>>(P, a->AT, t.iD, V(a, a->Wv, 1), a->ub, a->uTb);
+        wf::k_adj_vacc<<<g, bk, 0, st>>>(P, n, h->fl, a->Wv, t.uit, a->bb, a->Db, a->uTb);
+    } else {
+        wf::k_axpy<<<wf::lin_blocks(3 * (long long)N), 256, 0, st>>>(3 * (long long)N, 1.f, a->ub, a->uTb);
+        WFA_CUDA(cudaMemsetAsync(a->bb, 0, v, st));
     }
-    wf::k_axpy<<<wf::lin_blocks(3 * (long long)N), 256, 0, st>>>(3 * (long long)N, 1.f, in, a->uTb);
-    wf::k_adj_vcoef<<<g, bk, 0, st>>>(P, h->fl, a->Ab, a->iDb, a->iD, a->uTb, a->Db);
     wf::k_adj_pre<<<g, bk, 0, st>>>(P, h->B, G, h->fl, a->Db, a->bb, a->uTb, a->pb_in, a->dragb);
-    (void)ustar;
     WFA_CUDA(cudaMemcpyAsync(a->ub, a->uTb, v, cudaMemcpyDeviceToDevice, st));
     WFA_CUDA(cudaMemcpyAsync(a->pb, a->pb_in, s, cudaMemcpyDeviceToDevice, st));
     WFA_CUDA(cudaGetLastError());
@@ -785,12 +860,13 @@ int adjoint_step(wf_adjoint* a, int phases) {
 }
 
 void free_adj(wf_adjoint* a) {
-    float* ptrs[] = {a->uT, a->p0, a->D, a->b, a->A, a->iD, a->uit, a->Dp, a->bp, a->c3, a->ainv, a->qit, a->cbuf,
-                     a->aod, a->pai, a->prhs, a->sit, a->uout, a->pout, a->ub, a->ub2, a->uTb, a->pb, a->pb_in,
-                     a->Db, a->bb, a->Ab, a->iDb, a->c3b, a->cb, a->cb2, a->ab, a->sb, a->sb2, a->aib, a->rb,
-                     a->Dpb, a->bpb, a->gb, a->dragb};
+    float* ptrs[] = {a->ub, a->uTb, a->pb, a->pb_in, a->Db, a->bb, a->AT, a->Wv, a->Wp, a->c3b, a->cb, a->cb2,
+                     a->ab, a->sb, a->rb, a->dgb, a->gb, a->dragb};
     for (float* p : ptrs)
         if (p) cudaFree(p);
+    for (void* p : a->blocks) cudaFree(p);
+    a->blocks.clear();
+    a->tapes.clear();
     if (a->dJ) cudaFree(a->dJ);
     for (float* p : a->ck)
         if (p) cudaFree(p);
@@ -825,24 +901,16 @@ int wf_adj_create(wf_solver* h, wf_adjoint** out) {
         if (!ok) return;
         ok = cudaMalloc((void**)p, bytes) == cudaSuccess && cudaMemsetAsync(*p, 0, bytes, a->st) == cudaSuccess;
     };
-    const int nC1 = a->nC > 0 ? a->nC : 1;
-    al(&a->uT, v); al(&a->p0, s); al(&a->D, v); al(&a->b, v); al(&a->A, 2 * v); al(&a->iD, v);
-    al(&a->uit, (size_t)(a->nV + 1) * v);
-    al(&a->Dp, s); al(&a->bp, s); al(&a->c3, v); al(&a->ainv, s);
-    al(&a->qit, (size_t)(a->nP + 1) * s);
-    al(&a->cbuf, (size_t)(a->nC + 1) * v);
-    al(&a->aod, (size_t)nC1 * v); al(&a->pai, (size_t)nC1 * s); al(&a->prhs, (size_t)nC1 * s);
-    al(&a->sit, (size_t)nC1 * (a->nP + 1) * s);
-    al(&a->uout, v); al(&a->pout, s);
-    al(&a->ub, v); al(&a->ub2, v); al(&a->uTb, v); al(&a->pb, s); al(&a->pb_in, s);
-    al(&a->Db, v); al(&a->bb, v); al(&a->Ab, 2 * v); al(&a->iDb, v); al(&a->c3b, v);
-    al(&a->cb, v); al(&a->cb2, v); al(&a->ab, v); al(&a->sb, s); al(&a->sb2, s);
-    al(&a->aib, s); al(&a->rb, s); al(&a->Dpb, s); al(&a->bpb, s);
+    al(&a->ub, v); al(&a->uTb, v); al(&a->pb, s); al(&a->pb_in, s); al(&a->Db, v); al(&a->bb, v);
+    al(&a->AT, 2 * v); al(&a->Wv, (size_t)(a->nV + 1) * v); al(&a->Wp, (size_t)(a->nP + 1) * s);
+    al(&a->c3b, v); al(&a->cb, v); al(&a->cb2, v); al(&a->ab, v); al(&a->sb, s); al(&a->rb, s); al(&a->dgb, s);
     al(&a->gb, plane_floats(h->P) * sizeof(float));
     al(&a->dragb, s);
     if (ok) ok = cudaMalloc((void**)&a->dJ, sizeof(double)) == cudaSuccess;
+    if (ok) ok = ensure_tapes(a, 1) == WF_OK;
     if (ok) ok = cudaStreamSynchronize(a->st) == cudaSuccess;
     if (!ok) {
+        cudaGetLastError();
         free_adj(a);
         delete a;
         return WF_ERR_OOM;
@@ -870,14 +938,15 @@ int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const floa
     WFA_CUDA(cudaSetDevice(h->device));
     WFA_CUDA(cudaStreamSynchronize(h->st));
     const size_t N = a->N, v = 3 * N * sizeof(float), s = N * sizeof(float);
+    Tape& t = a->tapes[0];
     // the solver's current state is the step input
-    int st = record_step(a, h->vb[h->iT], h->pr, phases);
+    int st = record_step(a, t, h->vb[h->iT], h->pr, phases);
     if (st != WF_OK) return st;
     WFA_CUDA(cudaMemcpyAsync(a->ub, ubar_out, v, cudaMemcpyHostToDevice, a->st));
     WFA_CUDA(cudaMemcpyAsync(a->pb, pbar_out, s, cudaMemcpyHostToDevice, a->st));
     WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(h->P) * sizeof(float), a->st));
     WFA_CUDA(cudaMemsetAsync(a->dragb, 0, s, a->st));
-    st = adjoint_step(a, phases);
+    st = adjoint_step(a, t, phases);
     if (st != WF_OK) return st;
     WFA_CUDA(cudaMemcpyAsync(ubar_in, a->ub, v, cudaMemcpyDeviceToHost, a->st));
     WFA_CUDA(cudaMemcpyAsync(pbar_in, a->pb, s, cudaMemcpyDeviceToHost, a->st));
@@ -894,10 +963,11 @@ int wf_adj_step_forward(wf_adjoint* a, int phases, float* u_out, float* p_out) {
     wf_solver* h = a->h;
     WFA_CUDA(cudaSetDevice(h->device));
     WFA_CUDA(cudaStreamSynchronize(h->st));
-    const int st = record_step(a, h->vb[h->iT], h->pr, phases);
+    Tape& t = a->tapes[0];
+    const int st = record_step(a, t, h->vb[h->iT], h->pr, phases);
     if (st != WF_OK) return st;
-    WFA_CUDA(cudaMemcpyAsync(u_out, a->uout, 3 * a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
-    WFA_CUDA(cudaMemcpyAsync(p_out, a->pout, a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
+    WFA_CUDA(cudaMemcpyAsync(u_out, t.uout, 3 * a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
+    WFA_CUDA(cudaMemcpyAsync(p_out, t.pout, a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
     WFA_CUDA(cudaStreamSynchronize(a->st));
     return WF_OK;
 }
@@ -920,31 +990,29 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     const int area = (obj->x1 - obj->x0) * (obj->z1 - obj->z0);
     const float w = 1.f / (float)(obj->window * area);
     const dim3 og((obj->x1 - obj->x0 + 31) / 32, (obj->z1 - obj->z0 + 7) / 8), ob(32, 8);
-    // checkpoints: state n for n % C == 0 (n < n_steps); one segment of
-    // states recomputed from its checkpoint at a time
-    const int C = checkpoint_every;
+    // checkpoints: state n for n % C == 0 (n < n_steps); the steps of one
+    // segment are recomputed into C tapes and reversed
+    const int C = std::min(checkpoint_every, n_steps);
     const int nck = (n_steps + C - 1) / C;
-    struct Scratch {
-        std::vector<float*> seg;
+    int rs = ensure_tapes(a, C);
+    if (rs != WF_OK) return rs;
+    struct Events {
         cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-        ~Scratch() {
-            for (float* p : seg)
-                if (p) cudaFree(p);
+        ~Events() {
             for (cudaEvent_t e : ev)
                 if (e) cudaEventDestroy(e);
         }
-    } S;
+    } E;
     for (float* p : a->ck) cudaFree(p);
     a->ck.assign(nck, nullptr);
     for (int i = 0; i < nck; ++i)
-        if (cudaMalloc((void**)&a->ck[i], v + s) != cudaSuccess) return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
-    S.seg.assign(C, nullptr);
-    for (int i = 0; i < C; ++i)
-        if (cudaMalloc((void**)&S.seg[i], v + s) != cudaSuccess) return adj_fail(a, WF_ERR_OOM, "segment memory");
-    for (cudaEvent_t& e : S.ev) WFA_CUDA(cudaEventCreate(&e));
-    std::vector<float*>& seg = S.seg;
+        if (cudaMalloc((void**)&a->ck[i], v + s) != cudaSuccess) {
+            cudaGetLastError();
+            return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
+        }
+    for (cudaEvent_t& e : E.ev) WFA_CUDA(cudaEventCreate(&e));
     WFA_CUDA(cudaMemsetAsync(a->dJ, 0, sizeof(double), h->st));
-    WFA_CUDA(cudaEventRecord(S.ev[0], h->st));
+    WFA_CUDA(cudaEventRecord(E.ev[0], h->st));
     // ---- forward: the solver's own (fast) step, checkpoints, objective
     for (int n = 0; n < n_steps; ++n) {
         if (n % C == 0) {
@@ -957,34 +1025,33 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
             wf::k_objective<<<og, ob, 0, h->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
                                                   h->vb[h->iT], nullptr, a->dJ);
     }
-    WFA_CUDA(cudaEventRecord(S.ev[1], h->st));
+    WFA_CUDA(cudaEventRecord(E.ev[1], h->st));
     WFA_CUDA(cudaStreamSynchronize(h->st));
-    // ---- reverse
+    // ---- reverse, one segment at a time
     WFA_CUDA(cudaMemsetAsync(a->ub, 0, v, a->st));
     WFA_CUDA(cudaMemsetAsync(a->pb, 0, s, a->st));
     WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(P) * sizeof(float), a->st));
     WFA_CUDA(cudaMemsetAsync(a->dragb, 0, s, a->st));
     for (int sgi = nck - 1; sgi >= 0; --sgi) {
         const int n0 = sgi * C, n1 = std::min(n_steps, n0 + C);
-        WFA_CUDA(cudaMemcpyAsync(seg[0], a->ck[sgi], v + s, cudaMemcpyDeviceToDevice, a->st));
-        for (int n = n0 + 1; n < n1; ++n) {
-            const int st = record_step(a, seg[n - 1 - n0], seg[n - 1 - n0] + 3 * N, 3);
-            if (st != WF_OK) return st;
-            WFA_CUDA(cudaMemcpyAsync(seg[n - n0], a->uout, v, cudaMemcpyDeviceToDevice, a->st));
-            WFA_CUDA(cudaMemcpyAsync(seg[n - n0] + 3 * N, a->pout, s, cudaMemcpyDeviceToDevice, a->st));
+        for (int n = n0; n < n1; ++n) {
+            Tape& t = a->tapes[n - n0];
+            const float* ui = n == n0 ? a->ck[sgi] : a->tapes[n - n0 - 1].uout;
+            const float* pi = n == n0 ? a->ck[sgi] + 3 * N : a->tapes[n - n0 - 1].pout;
+            rs = record_step(a, t, ui, pi, 3);
+            if (rs != WF_OK) return rs;
         }
         for (int n = n1 - 1; n >= n0; --n) {
             // step n maps state n to state n+1
-            int st = record_step(a, seg[n - n0], seg[n - n0] + 3 * N, 3);
-            if (st != WF_OK) return st;
+            const Tape& t = a->tapes[n - n0];
             if (n + 1 > n_steps - obj->window)
                 wf::k_objective<<<og, ob, 0, a->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
-                                                      a->uout, a->ub, nullptr);
-            st = adjoint_step(a, 3);
-            if (st != WF_OK) return st;
+                                                      t.uout, a->ub, nullptr);
+            rs = adjoint_step(a, t, 3);
+            if (rs != WF_OK) return rs;
         }
     }
-    WFA_CUDA(cudaEventRecord(S.ev[2], a->st));
+    WFA_CUDA(cudaEventRecord(E.ev[2], a->st));
     WFA_CUDA(cudaStreamSynchronize(a->st));
     // ---- chain to the inflow parameters: X0 plane g_x(y) = u*/k ln((y_c+z0)/z0)
     const int np = P.plane[WF_FACE_X0];
@@ -1026,8 +1093,8 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     if (dJ_dustar) *dJ_dustar = gu;
     if (dJ_dz0) *dJ_dz0 = gz;
     float tf = 0.f, tt = 0.f;
-    WFA_CUDA(cudaEventElapsedTime(&tf, S.ev[0], S.ev[1]));
-    WFA_CUDA(cudaEventElapsedTime(&tt, S.ev[0], S.ev[2]));
+    WFA_CUDA(cudaEventElapsedTime(&tf, E.ev[0], E.ev[1]));
+    WFA_CUDA(cudaEventElapsedTime(&tt, E.ev[0], E.ev[2]));
     if (ms_forward) *ms_forward = tf;
     if (ms_total) *ms_total = tt;
     return WF_OK;

@@ -90,6 +90,8 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
 }
 
 // One momentum sweep: uo_P = iD_P (sum_f A_f ui_f + b_P) on fluid cells.
+// kCopyAll: non-fluid cells copy ui (a complete iterate in a fresh buffer).
+template <bool kCopyAll = false>
 __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Params P, const float* __restrict__ A,
                                                     const float* __restrict__ iD, const float* __restrict__ bv,
                                                     const float* __restrict__ ui, float* __restrict__ uo) {
@@ -100,7 +102,12 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
     const float d0 = ld(iD, i);
-    if (d0 == 0.f) return;  // non-fluid cell
+    if (d0 == 0.f) {  // non-fluid cell
+        if (kCopyAll)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) uo[k * N + i] = ld(ui, k * N + i);
+        return;
+    }
     const float a0 = ld(A, i), a1 = ld(A, N + i), a2 = ld(A, 2 * N + i);
     const float a3 = ld(A, 3 * N + i), a4 = ld(A, 4 * N + i), a5 = ld(A, 5 * N + i);
     const int sx = P.nx, sz = P.nx * P.ny;
@@ -330,6 +337,8 @@ struct PresWave {
     const float* __restrict__ rh;
     float* __restrict__ pout;
     float* __restrict__ pprev;
+    float* __restrict__ stack;   // optional: level s of every cell to stack + s*N
+    size_t N;
     int tx, ty, xe, xw, yn, ys, col, sxy, nz, zs, z0, z1, T;
     bool inxy, out_col;
     float h[K + 1][3];           // level values, ring of the last 3 planes
@@ -344,7 +353,7 @@ struct PresWave {
             pn = __ldg(cN + i);
             pu = __ldg(cU + i);
             a = __ldg(ai + i);
-            r = __ldg(rh + i);
+            r = rh ? __ldg(rh + i) : 0.f;
         } else {
             pv = pe = pn = pu = a = r = 0.f;
         }
@@ -376,7 +385,11 @@ struct PresWave {
                 acc -= qu[rs] * h[s - 1][h0];
                 acc -= qu[rd] * h[s - 1][hm2];
                 const float v = qa[rs] * (acc + qr[rs]);
-                if (s == K) {
+                if (stack) {  // every level, non-fluid cells included (v = 0 there)
+                    const int p = zs + t - s;
+                    if (out_col && p >= z0 && p < z1) stack[(size_t)s * N + p * sxy + col] = v;
+                }
+                if (s == K && pout) {
                     const int p = zs + t - K;
                     if (out_col && p >= z0 && p < z1 && qa[rs] != 0.f) {
                         const int i = p * sxy + col;
@@ -396,7 +409,7 @@ template <int K>
 __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
     k_pres_msweep(const __grid_constant__ Params P, const float* __restrict__ c3, const float* __restrict__ ainv,
                   const float* __restrict__ rhs, const float* __restrict__ pin, float* __restrict__ pout,
-                  float* __restrict__ pprev, int zchunk) {
+                  float* __restrict__ pprev, int zchunk, float* __restrict__ stack) {
     // dynamic shared memory: V[K][2][TY][TX] level planes, CE/CN[6][TY][TX]
     // coefficient rings
     extern __shared__ float msm[];
@@ -424,6 +437,8 @@ __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
     w.pin = pin;
     w.pout = pout;
     w.pprev = pprev;
+    w.stack = stack;
+    w.N = P.N;
     w.xe = min(w.tx + 1, MS_TX - 1);
     w.xw = max(w.tx - 1, 0);
     w.yn = min(w.ty + 1, MS_TY - 1);
@@ -642,7 +657,7 @@ void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
         const dim3 g((P.nx / 4 + b.x - 1) / b.x, (P.ny + b.y - 1) / b.y, (P.nz + b.z - 1) / b.z);
         k_vel_sweep4<<<g, b, 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
     } else {
-        k_vel_sweep1<<<grd(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
+        k_vel_sweep1<false><<<grd(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
     }
 }
 
@@ -679,11 +694,14 @@ namespace {
 // z chunking of the wavefront kernels (one resident block per SM): as many
 // chunks as fit one wave of blocks on the device's SMs, so no SM runs a
 // second, partly empty wave; each chunk re-reads 2K halo planes.
-void wave_chunks(const wf_solver* h, int blocks_xy, int K, int& zchunk, int& nchunk) {
-    const int sms = h->num_sms > 0 ? h->num_sms : 148;
+void wave_chunks_n(int sms, int nz, int blocks_xy, int K, int& zchunk, int& nchunk) {
+    sms = sms > 0 ? sms : 148;
     nchunk = std::max(1, sms / std::max(blocks_xy, 1));
-    zchunk = std::max(2 * K + 2, (h->P.nz + nchunk - 1) / nchunk);
-    nchunk = (h->P.nz + zchunk - 1) / zchunk;
+    zchunk = std::max(2 * K + 2, (nz + nchunk - 1) / nchunk);
+    nchunk = (nz + zchunk - 1) / zchunk;
+}
+void wave_chunks(const wf_solver* h, int blocks_xy, int K, int& zchunk, int& nchunk) {
+    wave_chunks_n(h->num_sms, h->P.nz, blocks_xy, K, zchunk, nchunk);
 }
 
 template <int K>
@@ -791,7 +809,7 @@ void launch_msweep_k(wf_solver* h, const float* rhs, const float* in, float* out
     const size_t smem = pres_msweep_smem(K);
     WF_COUNT_LAUNCH();
     k_pres_msweep<K><<<dim3(gx, gy, nchunk), dim3(MS_TX, MS_TY), smem, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
-                                                                              in, out, prev, zchunk);
+                                                                              in, out, prev, zchunk, nullptr);
 }
 
 void launch_msweep(wf_solver* h, int k, const float* rhs, const float* in, float* out, float* prev) {
@@ -917,6 +935,35 @@ int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double
     return WF_OK;
 }
 
+// Multi-sweep passes with every iterate kept (see launch_pres_stack).
+template <int K>
+void launch_stack_pass(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
+                       const float* rhs, const float* in, float* slots) {
+    constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
+    const int gx = (P.nx + OX - 1) / OX, gy = (P.ny + OY - 1) / OY;
+    int zchunk = 0, nchunk = 0;
+    wave_chunks_n(sms, P.nz, gx * gy, K, zchunk, nchunk);
+    WF_COUNT_LAUNCH();
+    k_pres_msweep<K><<<dim3(gx, gy, nchunk), dim3(MS_TX, MS_TY), pres_msweep_smem(K), st>>>(
+        P, c3, ainv, rhs, in, nullptr, nullptr, zchunk, slots);
+}
+void launch_pres_stack(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
+                       const float* rhs, float* stack, int n, bool from_zero) {
+    const size_t N = P.N;
+    for (int base = 0; base < n;) {
+        const int k = std::min(4, n - base);
+        const float* in = (base == 0 && from_zero) ? nullptr : stack + base * N;
+        float* slots = stack + base * N;
+        switch (k) {
+            case 1: launch_stack_pass<1>(P, st, sms, c3, ainv, rhs, in, slots); break;
+            case 2: launch_stack_pass<2>(P, st, sms, c3, ainv, rhs, in, slots); break;
+            case 3: launch_stack_pass<3>(P, st, sms, c3, ainv, rhs, in, slots); break;
+            default: launch_stack_pass<4>(P, st, sms, c3, ainv, rhs, in, slots); break;
+        }
+        base += k;
+    }
+}
+
 // Explicit-pointer launchers (the adjoint's recorded forward step).
 void launch_vel_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, const float* eddy,
                          const float* face, const float* Dv, float* A, float* iD) {
@@ -926,7 +973,7 @@ void launch_vel_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, co
 void launch_vel_sweep1_ptr(const Params& P, cudaStream_t st, const float* A, const float* iD, const float* bv,
                            const float* ui, float* uo) {
     WF_COUNT_LAUNCH();
-    k_vel_sweep1<<<grd(P), blk(), 0, st>>>(P, A, iD, bv, ui, uo);
+    k_vel_sweep1<true><<<grd(P), blk(), 0, st>>>(P, A, iD, bv, ui, uo);
 }
 void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, float* c3) {
     WF_COUNT_LAUNCH();
@@ -940,11 +987,6 @@ void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, co
                          float* ainv, float* rhs) {
     WF_COUNT_LAUNCH();
     k_piso_pre<<<grd(P), blk(), 0, st>>>(P, fl, Dv, aodu, ainv, rhs);
-}
-void launch_pres_sweep1_ptr(const Params& P, cudaStream_t st, const float* c3, const float* ainv, const float* rhs,
-                            const float* pi, float* po) {
-    WF_COUNT_LAUNCH();
-    k_pres_sweep1<<<grd(P), blk(), 0, st>>>(P, c3, ainv, rhs, pi, po);
 }
 
 }  // namespace wf

@@ -20,8 +20,9 @@ int pres_sweeps_fast(wf_solver* h, int n, bool piso);
 
 // Explicit-pointer launchers of the fast Jacobi building blocks: momentum
 // coefficients A (6 planes) and 1/D (3), one momentum sweep, pressure face
-// coefficients c_E/c_N/c_U, 1/Dp, PISO diagonal and right-hand side, one
-// pressure-type sweep (pi == nullptr: zero iterate).
+// coefficients c_E/c_N/c_U, 1/Dp, PISO diagonal and right-hand side.  The
+// momentum sweep writes every cell (non-fluid cells copy the input iterate),
+// so each output buffer holds a complete iterate.
 void launch_vel_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, const float* eddy,
                          const float* face, const float* Dv, float* A, float* iD);
 void launch_vel_sweep1_ptr(const Params& P, cudaStream_t st, const float* A, const float* iD, const float* bv,
@@ -30,8 +31,13 @@ void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, c
 void launch_inv_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dp, float* ainv);
 void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* aodu,
                          float* ainv, float* rhs);
-void launch_pres_sweep1_ptr(const Params& P, cudaStream_t st, const float* c3, const float* ainv, const float* rhs,
-                            const float* pi, float* po);
+
+// n pressure-type sweeps po = ainv (rhs - C pi) (rhs == nullptr: 0) by the
+// multi-sweep kernel, every iterate kept: slot k of `stack` (stride N floats)
+// receives iterate k for k = 1..n on every cell (0 on non-fluid cells).  The
+// first pass reads slot 0, or the all-zero iterate when from_zero is set.
+void launch_pres_stack(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
+                       const float* rhs, float* stack, int n, bool from_zero);
 
 // Event-timed launches of one hot kernel (WF_KERNEL_*), see wf_time_kernel.
 int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double* bytes, int* sweeps);
