@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     return ap.parse_args()
 
@@ -179,14 +180,14 @@ def batched_section(steps: int, local: int):
         tuned.append(autotune.tune(s, cache, reps=3))
     cells = sum(c.n_cells for c in cs)
     for s in solvers:
-        s.Step(2)  # graph capture + warm-up
+        s.Step(2)
+        s.prepare_graphs()  # every step graph captured before timing
     plain_ms = 0.0
     for s in solvers:
         s.Step(steps)
         plain_ms += s.last_step_ms()
     b = BatchSolver(solvers)
     width = autotune.tune_batch(b, steps=2)
-    b.step(1)
     l0 = b.kernel_launches()
     b.step(steps)
     batched_ms = b.last_step_ms()
@@ -201,6 +202,39 @@ def batched_section(steps: int, local: int):
             "plain_mcell_steps_s": plain, "batched_mcell_steps_s": batched, "batched_over_plain": batched / plain,
             "steps": steps, "gpu_launches": launches,
             "depths": sorted({(t["pres_k"], t["vel_k"]) for t in tuned}), "width": width}
+
+
+def adjoint_section(local: int):
+    """Differentiated form on the adjoint workload (128 x 64(up) x 96 cells,
+    12 soft buildings, PISO, turbulence off): the objective's gradient with
+    respect to (u*, z0, 12 building heights) over a 200-step window,
+    checkpoints every 20 steps, objective over the last 100 steps.  Cost
+    against the plain forward of the same 200 steps (device time, CUDA
+    events)."""
+    from unitywindsimulation_b200 import FvmSolverCuda, cases
+    from unitywindsimulation_b200.adjoint import AdjointSolver, Objective
+
+    case = cases.adjoint_street()
+    steps = case.steps
+    obj = Objective(**cases.ADJOINT_STREET_OBJECTIVE)
+    g = FvmSolverCuda(case.cfg, device=local)
+    cases.apply_case(g, case)
+    g.Step(3)
+    g.prepare_graphs()
+    g.Step(steps)
+    fwd_ms = g.last_step_ms()
+    g.close()
+    g = FvmSolverCuda(case.cfg, device=local)
+    cases.apply_case(g, case)
+    with AdjointSolver(g) as adj:
+        r = adj.gradient(obj, steps, cases.ADJOINT_STREET_CHECKPOINT, soft=case.soft)
+    g.close()
+    return {"workload": f"adjoint_street: {case.n_cells} cells, 12 soft buildings, PISO laminar, nV=50 nP=30 nC=2, "
+                        f"{steps}-step window, checkpoints every {cases.ADJOINT_STREET_CHECKPOINT}, objective over "
+                        f"the last {obj.window} steps",
+            "forward_ms": fwd_ms, "gradient_ms": r["ms_total"], "gradient_forward_pass_ms": r["ms_forward"],
+            "adjoint_over_forward": r["ms_total"] / fwd_ms, "J": r["J"], "dJ_dustar": r["dJ_dustar"],
+            "dJ_dz0": r["dJ_dz0"], "dJ_dheights": [float(x) for x in r["dJ_dheights"]]}
 
 
 def run_reference(args):
@@ -282,6 +316,7 @@ def run_windfvm(args):
 
     # ---- device-resident throughput ----
     solver.Step(args.warmup)
+    solver.prepare_graphs()  # captures only; no step runs
     barrier()
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     smi_index = int(vis.split(",")[local]) if vis and vis.split(",")[local].isdigit() else local
@@ -340,6 +375,10 @@ def run_windfvm(args):
     if world == 1 and not args.no_batched:
         batched = batched_section(max(3, min(args.steps, 5)), local)
 
+    adjoint = None
+    if world == 1 and not args.no_adjoint:
+        adjoint = adjoint_section(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case, args.cpu_sample_steps)
@@ -356,6 +395,7 @@ def run_windfvm(args):
             "vel_sweep_kernel": {"ms_per_launch": v_ms, "alg_bytes_per_launch": v_bytes,
                                  "achieved_gbs": v_bytes / (v_ms / 1e3) / 1e9, "sweeps_per_launch": v_sweeps},
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if dist:

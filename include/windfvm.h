@@ -156,6 +156,14 @@ int wf_set_inflow_plane(wf_solver* h, const float* x0_plane_xyz);
 /* Step() repeated n_steps times, each a complete time step with fixed
  * iteration counts (no 30 ms time slicing).  *ready (may be NULL) = 1. */
 int wf_step(wf_solver* h, int n_steps, int* ready);
+/* No counterpart in the reference.  The step rotates its buffers, so its
+ * CUDA graph depends on which buffer holds which field; the few such states
+ * repeat with a short period, and wf_step captures the graph of each state
+ * the first time it meets it.  This call captures them all at once, without
+ * running any step or changing any field, so that later wf_step calls only
+ * replay.  Needs the replay state (use_graph on, calc_residual off, at least
+ * one wf_step since the last field write); otherwise it does nothing. */
+int wf_prepare_graphs(wf_solver* h);
 
 /* ---- field access -------------------------------------------------------- */
 enum { WF_LAYOUT_SOA = 0,   /* 3 planes of N floats: [c][z][y][x]           */
@@ -308,6 +316,11 @@ const char* wf_batch_last_error(const wf_batch* b);
  * (default) = every case its own chain; 1 = all cases in sequence (keeps
  * each case's working set in L2 while it runs).  Speed only. */
 int wf_batch_set_width(wf_batch* b, int width);
+/* Captures the batch graphs of every buffer-role state the cases cycle
+ * through (see wf_prepare_graphs), without stepping.  Needs every case in
+ * the replay state (one wf_batch_step after creating the batch or changing
+ * its width); otherwise it does nothing. */
+int wf_batch_prepare_graphs(wf_batch* b);
 
 /* Temporal-blocking depths of the Jacobi loops: pressure sweeps per pass
  * (1..4) and momentum sweeps per pass (1..2).  Results do not depend on

@@ -52,6 +52,24 @@ def test_batch_width_does_not_change_results(built, width):
         np.testing.assert_array_equal(a.GetVelField(), s.GetVelField())
 
 
+def test_batch_prepare_graphs_keeps_results(built):
+    cs = _small_batch()
+    alone = [FvmSolverCuda(c.cfg) for c in cs]
+    batch = [FvmSolverCuda(c.cfg) for c in cs]
+    for s, c in zip(alone + batch, cs + cs):
+        s.InitFlags(c.flags)
+    for s in alone:
+        s.Step(6)
+    b = BatchSolver(batch)
+    b.step(1)
+    b.prepare_graphs()  # captures only
+    assert all(s.get_state()[2] == 1 for s in batch)
+    b.step(5)
+    for a, s in zip(alone, batch):
+        np.testing.assert_array_equal(a.GetVelField(), s.GetVelField())
+        np.testing.assert_array_equal(a.GetPresField(), s.GetPresField())
+
+
 def test_batched_cases_match_oracle(built):
     cs = _small_batch()[:2]
     gs = [FvmSolverCuda(c.cfg) for c in cs]

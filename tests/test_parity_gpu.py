@@ -272,6 +272,29 @@ def test_graph_replay_equals_eager(built):
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
 
 
+def test_prepare_graphs_keeps_results(built):
+    """Capturing every step graph ahead (wf_prepare_graphs) runs no step and
+    changes no result: bit-identical fields to a solver that captures on
+    the way, and the prepared solver launches no capture while stepping."""
+    case = cases.small_case(seed=11)
+    outs = []
+    for prepare in (False, True):
+        g = FvmSolverCuda(case.cfg)
+        g.InitFlags(case.flags)
+        g.Step(1)
+        if prepare:
+            before = g.get_state()
+            g.prepare_graphs()
+            after = g.get_state()
+            np.testing.assert_array_equal(before[0], after[0])
+            assert before[2] == after[2]
+        g.Step(7)
+        outs.append((g.GetVelField(), g.GetPresField()))
+        g.close()
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+
+
 def test_state_roundtrip(built):
     case = cases.small_case(seed=10)
     g = FvmSolverCuda(case.cfg)

@@ -175,6 +175,8 @@ _SIGNATURES = {
     "wf_batch_kernel_launches": (c_int, [c_void_p, POINTER(c_int64)]),
     "wf_batch_last_error": (c_char_p, [c_void_p]),
     "wf_batch_set_width": (c_int, [c_void_p, c_int]),
+    "wf_batch_prepare_graphs": (c_int, [c_void_p]),
+    "wf_prepare_graphs": (c_int, [c_void_p]),
     "wf_set_blocking": (c_int, [c_void_p, c_int, c_int]),
     "wf_get_blocking": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
     "wf_adj_create": (c_int, [c_void_p, POINTER(c_void_p)]),

@@ -57,13 +57,16 @@ def tune_batch(batch, widths=(1, 2, 4, 0), steps: int = 2) -> dict:
     times = {}
     for w in widths:
         batch.set_width(w)
-        batch.step(1)  # capture
+        batch.step(1)
+        batch.prepare_graphs()  # no capture inside the timed steps
         batch.step(steps)
         ms = batch.last_step_ms() / steps
         times[w] = ms
         if best is None or ms < times[best]:
             best = w
     batch.set_width(best)
+    batch.step(1)
+    batch.prepare_graphs()
     return {"width": best, "ms_per_step": times}
 
 

@@ -666,6 +666,25 @@ int wf_set_inflow_plane(wf_solver* h, const float* pl) {
     return sync(h);
 }
 
+int wf_prepare_graphs(wf_solver* h) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    WF_CUDA(cudaSetDevice(h->device));
+    if (!wf::step_graphable(h)) return WF_OK;  // not in the replay state yet
+    const auto start = role_key(h);
+    for (int i = 0; i < 64; ++i) {
+        const wf_solver::GraphEntry* e = nullptr;
+        const int st = wf::ensure_step_graph(h, &e);
+        if (st != WF_OK) {
+            set_roles(h, start);
+            return st;
+        }
+        set_roles(h, e->after);
+        if (role_key(h) == start) break;
+    }
+    set_roles(h, start);
+    return WF_OK;
+}
+
 int wf_step(wf_solver* h, int n_steps, int* ready) {
     if (!h) return WF_ERR_INVALID_ARG;
     if (n_steps < 0) return set_err(h, WF_ERR_INVALID_ARG, "n_steps must be >= 0");

@@ -190,6 +190,39 @@ int wf_batch_set_width(wf_batch* b, int width) {
     return WF_OK;
 }
 
+int wf_batch_prepare_graphs(wf_batch* b) {
+    if (!b) return WF_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return fail(b, WF_ERR_CUDA, "cudaSetDevice failed");
+    for (wf_solver* h : b->s)
+        if (!wf::step_graphable(h)) return WF_OK;  // not in the replay state yet
+    auto current = [&]() {
+        std::vector<wf_solver::RoleKey> k;
+        for (wf_solver* h : b->s) k.push_back({h->iT, h->iF, h->iI, h->iPC, h->iPCL});
+        return k;
+    };
+    auto apply = [&](const std::vector<wf_solver::RoleKey>& k) {
+        for (size_t i = 0; i < b->s.size(); ++i) {
+            wf_solver* h = b->s[i];
+            h->iT = std::get<0>(k[i]);
+            h->iF = std::get<1>(k[i]);
+            h->iI = std::get<2>(k[i]);
+            h->iPC = std::get<3>(k[i]);
+            h->iPCL = std::get<4>(k[i]);
+        }
+    };
+    const std::vector<wf_solver::RoleKey> start = current();
+    int st = WF_OK;
+    for (int i = 0; i < 64 && st == WF_OK; ++i) {
+        const wf_batch::Entry* ent = nullptr;
+        st = ensure_batch_graph(b, &ent);
+        if (st != WF_OK) break;
+        apply(ent->after);
+        if (current() == start) break;
+    }
+    apply(start);
+    return st;
+}
+
 int wf_batch_kernel_launches(const wf_batch* b, int64_t* total) {
     if (!b || !total) return WF_ERR_INVALID_ARG;
     *total = b->launches;

@@ -67,6 +67,11 @@ class FvmSolverCuda:
         self._check(self._lib.wf_step(self._h, int(n_steps), byref(ready)))
         return bool(ready.value)
 
+    def prepare_graphs(self) -> None:
+        """Captures the step graphs of every buffer-role state ahead of time
+        (wf_prepare_graphs); runs no step."""
+        self._check(self._lib.wf_prepare_graphs(self._h))
+
     def InitFlags(self, flags) -> None:
         f = np.ascontiguousarray(np.asarray(flags, dtype=np.int32).reshape(-1))
         if f.size != self.n_cells:
@@ -251,6 +256,11 @@ class BatchSolver:
 
     def set_width(self, width: int) -> None:
         self._check(self._lib.wf_batch_set_width(self._b, int(width)))
+
+    def prepare_graphs(self) -> None:
+        """Captures the batch graphs of every buffer-role state ahead of time
+        (wf_batch_prepare_graphs); runs no step."""
+        self._check(self._lib.wf_batch_prepare_graphs(self._b))
 
     def kernel_launches(self) -> int:
         n = c_int64(0)
