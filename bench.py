@@ -160,16 +160,18 @@ def cpu_baseline(case, steps: int):
                       f"FP32 oracle, OpenMP {cores} threads"}
 
 
-def batched_section(steps: int, local: int):
-    """Batched form on the 16-case direction sweep (uneven grids 96..192 x
-    48..80(up) x 96..160, wind rotated by 22.5 degree steps): the same
-    cases stepped one after another (plain form) and together in one graph
-    launch per step (batched form), both after autotuning the blocking
-    depths per grid size.  Device time from CUDA events."""
+def batched_section(steps: int, local: int, small: bool = False):
+    """Batched form on 16 cases: the direction sweep (uneven grids 96..192 x
+    48..80(up) x 96..160, wind rotated by 22.5 degree steps), or with
+    small=True 16 small grids (about 0.1 M cells each).  The same cases are
+    stepped one after another (plain form) and together in one graph launch
+    per step (batched form), both after autotuning the blocking depths per
+    grid size and with every step graph captured before timing.  Device
+    time from CUDA events."""
     from unitywindsimulation_b200 import FvmSolverCuda, autotune, cases
     from unitywindsimulation_b200.solver import BatchSolver
 
-    cs = cases.batch_directions()
+    cs = cases.batch_small() if small else cases.batch_directions()
     solvers = [FvmSolverCuda(c.cfg, device=local) for c in cs]
     for s, c in zip(solvers, cs):
         cases.apply_case(s, c)
@@ -197,7 +199,8 @@ def batched_section(steps: int, local: int):
         s.close()
     plain = cells * steps / (plain_ms / 1e3) / 1e6
     batched = cells * steps / (batched_ms / 1e3) / 1e6
-    return {"workload": f"batch_directions: {len(cs)} cases, {cells} cells total, grids "
+    name = "batch_small" if small else "batch_directions"
+    return {"workload": f"{name}: {len(cs)} cases, {cells} cells total, grids "
                         f"{min(c.n_cells for c in cs)}..{max(c.n_cells for c in cs)} cells, nV=50 nP=30 nC=2",
             "plain_mcell_steps_s": plain, "batched_mcell_steps_s": batched, "batched_over_plain": batched / plain,
             "steps": steps, "gpu_launches": launches,
@@ -371,9 +374,10 @@ def run_windfvm(args):
     step_gbs = value / world * b_alg(cfg.vel_iters, cfg.pres_iters, cfg.piso_correctors) / 1e3
 
     solver.close()
-    batched = None
+    batched = batched_small = None
     if world == 1 and not args.no_batched:
         batched = batched_section(max(3, min(args.steps, 5)), local)
+        batched_small = batched_section(max(3, min(args.steps, 5)), local, small=True)
 
     adjoint = None
     if world == 1 and not args.no_adjoint:
@@ -395,6 +399,7 @@ def run_windfvm(args):
             "vel_sweep_kernel": {"ms_per_launch": v_ms, "alg_bytes_per_launch": v_bytes,
                                  "achieved_gbs": v_bytes / (v_ms / 1e3) / 1e9, "sweeps_per_launch": v_sweeps},
             "batched": batched,
+            "batched_small_cases": batched_small,
             "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)

@@ -214,6 +214,31 @@ def batch_directions(seed: int = 3, n_cases: int = 16, nv: int = 50, np_: int = 
     return cases
 
 
+def batch_small(seed: int = 5, n_cases: int = 16, nv: int = 50, np_: int = 30, steps: int = 300):
+    """16 small cases (nx, nz 48..72, ny 24..40 up, multiples of 8; about
+    0.1 M cells each) with 1-4 buildings on a 6-cell margin, footprints
+    rotated by k * 22.5 degrees: the regime where one case alone leaves most
+    of the GPU idle."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_cases):
+        nx = int(rng.integers(6, 10)) * 8
+        ny = int(rng.integers(3, 6)) * 8
+        nz = int(rng.integers(6, 10)) * 8
+        dx = 0.5
+        lots = ((nx - 2 * 6 - 2) // 18) * ((nz - 2 * 6 - 2) // 18)
+        blds = street_lattice_buildings(rng, nx, nz, min(int(rng.integers(1, 5)), lots), 6, 14, 4, ny // 2,
+                                        margin=6)
+        angle = 22.5 * (k % 16)
+        flags = remove_isolated_fluid(rasterise_boxes(nx, ny, nz, blds, angle_deg=angle, margin=6))
+        ustar, z0 = 0.5, 0.1
+        umax = float(log_profile((ny - 0.5) * dx, ustar, z0))
+        cfg = _les_piso_cfg(nx, ny, nz, dx, cfl_dt(umax, dx), ustar, z0, 0.1, nv, np_)
+        out.append(Case(f"small_{k:02d}_{angle:g}deg", cfg, flags, None, steps, seed,
+                        [b + (angle,) for b in blds]))
+    return out
+
+
 def adjoint_street(seed: int = 4, nv: int = 50, np_: int = 30, steps: int = 200) -> Case:
     """128 x 64(up) x 96 cells of 0.5 m, 12 buildings on a street lattice
     with footprints 6-16 cells and continuous heights in [4, 30] cells, as a
