@@ -53,7 +53,8 @@ enum {
     WF_ERR_TIMEOUT = 5,      /* a bounded device wait gave up                */
     WF_ERR_UNSUPPORTED = 6,  /* option not implemented for this build        */
     WF_NOT_FINISHED = 7,     /* step stopped early (time budget)             */
-    WF_ERR_STATE = 8         /* call not valid in the handle's current state */
+    WF_ERR_STATE = 8,        /* call not valid in the handle's current state */
+    WF_ERR_IO = 9            /* a file could not be created or written       */
 };
 
 /* ---- enums mirroring Constants.hlsl:4-14 and FluidSimConfig.cs:16-96 ---- */
@@ -150,6 +151,18 @@ int wf_init_vel_pres_fields(wf_solver* h);
 int wf_set_fixed_value_vel_bnd_cond(wf_solver* h, float wind_speed);
 /* ChangePhysFieldPos(): re-initialise the fields (FvmSolverGpu.cs:1026-1032). */
 int wf_change_phys_field_pos(wf_solver* h);
+/* InitVelPresFieldsFromBackGroundFlow (FvmSolverGpu.cs:898-929, kernel
+ * CSInitVelPresFieldsFromBGFlowRotate, InitShaderColl.compute:185-226): sets
+ * every cell's velocity (all iterate buffers) and pressure to the
+ * background handle's current fields sampled trilinearly (clamped) at the
+ * cell's position; corrections are zeroed.  pos / pos_bg: physical positions
+ * of the two domains' centres (FluidSimConfig.physFieldPos), rot_deg: this
+ * domain's rotation about the vertical axis (RuntimeConfig.
+ * flowFieldOrientation).  As in the reference, a cell sits at (index -
+ * res/2) * dx and the sampled vector is not rotated.  bg must be another
+ * handle on the same device; it is not modified. */
+int wf_init_from_background(wf_solver* h, const wf_solver* bg, const float pos[3], const float pos_bg[3],
+                            float rot_deg);
 /* Replaces the X0 inlet plane with caller data: ny*nz*3 floats, index
  * (z*ny + y)*3 + c (perturbed inflow). */
 int wf_set_inflow_plane(wf_solver* h, const float* x0_plane_xyz);
@@ -329,6 +342,31 @@ int wf_batch_prepare_graphs(wf_batch* b);
  * contain the handle afterwards. */
 int wf_set_blocking(wf_solver* h, int pres_k, int vel_k);
 int wf_get_blocking(const wf_solver* h, int* pres_k, int* vel_k);
+
+/* ---- field export ---------------------------------------------------------
+ * NcFlowFieldExporter (NcFlowFieldExporter.cs:197-393): velocity and
+ * pressure frames appended to a netCDF file while the solver runs.  Same
+ * layout as the reference's file: dimensions time (unlimited), velX, velY,
+ * velZ, velVec (4), presX, presY, presZ; coordinate variables at cell
+ * centres ((i + 0.5) * dx); global attributes gridLayoutType = "Collocated"
+ * and dt; variables time[time], velField[time][velZ][velY][velX][velVec]
+ * (channels u, v, w, 0) and presField[time][presZ][presY][presX], all
+ * float.  Written without libnetcdf as netCDF classic with 64-bit offsets
+ * (CDF-2), which every netCDF reader opens.
+ *
+ * wf_export_frame queues the solver's current fields (the state after the
+ * last wf_step): a device kernel packs the record, one asynchronous copy
+ * moves it to a pinned host slot, a writer thread writes it.  `ring` pinned
+ * slots (1..16) bound the frames in flight; the call blocks only while all
+ * of them are being written.  wf_export_close drains the queue, writes the
+ * record count and closes the file.  The solver must outlive the exporter.
+ * File errors surface as WF_ERR_IO on the next call (wf_export_last_error). */
+typedef struct wf_exporter wf_exporter;
+int wf_export_open(wf_solver* h, const char* path, int save_vel, int save_pres, int ring, wf_exporter** out);
+int wf_export_frame(wf_exporter* e, float phys_time);
+int wf_export_frames_written(wf_exporter* e, int64_t* n);
+const char* wf_export_last_error(const wf_exporter* e);
+int wf_export_close(wf_exporter* e);
 
 /* ---- discrete adjoint ------------------------------------------------------
  * No counterpart in the reference, which computes no derivatives.  The

@@ -38,6 +38,7 @@ def load():
         "wfo_init_vel_pres_fields": (c_int, [c_void_p]),
         "wfo_set_fixed_value_vel_bnd_cond": (c_int, [c_void_p, c_float]),
         "wfo_set_inflow_plane": (c_int, [c_void_p, POINTER(c_float)]),
+        "wfo_init_from_background": (c_int, [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float), c_float]),
         "wfo_step": (c_int, [c_void_p, c_int]),
         "wfo_field_size": (c_int, [c_void_p, c_int, POINTER(c_size_t), POINTER(c_int)]),
         "wfo_get_field": (c_int, [c_void_p, c_int, POINTER(c_double)]),
@@ -112,6 +113,12 @@ class OracleSolver:
         if wind_speed is not None:
             self.wind_speed = float(wind_speed)
         self._ok(self._lib.wfo_set_fixed_value_vel_bnd_cond(self._h, c_float(self.wind_speed)))
+
+    def InitVelPresFieldsFromBackGroundFlow(self, background, pos=(0.0, 0.0, 0.0), pos_background=(0.0, 0.0, 0.0),
+                                            rot_deg=0.0):
+        p = (c_float * 3)(*[float(v) for v in pos])
+        q = (c_float * 3)(*[float(v) for v in pos_background])
+        self._ok(self._lib.wfo_init_from_background(self._h, background._h, p, q, float(rot_deg)))
 
     def set_inflow_plane(self, plane_xyz):
         a = np.ascontiguousarray(plane_xyz, dtype=np.float32).reshape(-1)

@@ -167,6 +167,49 @@ template <class R> struct Oracle {
             p[P] = R(0); pc[P] = R(0); pcL[P] = R(0);
         });
     }
+    // CSInitVelPresFieldsFromBGFlowRotate, InitShaderColl.compute:185-226
+    // (host side FvmSolverGpu.cs:898-929): cell (index - res/2) * dx rotated
+    // by theta about the vertical axis, placed at pos, mapped into the
+    // background's frame and sampled trilinearly with clamped addressing;
+    // the vector is copied unrotated.  Every cell is written.
+    void init_from_background(const Oracle<R>& bg, const float pos[3], const float posb[3], float rot_deg) {
+        const R th = R(rot_deg) * R(3.1415926 / 180);
+        const R s1 = std::sin(th), c1 = std::cos(th), s2 = std::sin(-th), c2 = std::cos(-th);
+        const int bnx = bg.nx, bny = bg.ny, bnz = bg.nz;
+        auto sample = [&](auto get, R u, R v, R w) {
+            const R tx = u * R(bnx) - R(0.5), ty = v * R(bny) - R(0.5), tz = w * R(bnz) - R(0.5);
+            const R fx = std::floor(tx), fy = std::floor(ty), fz = std::floor(tz);
+            const R ax = tx - fx, ay = ty - fy, az = tz - fz;
+            auto cl = [](int i, int n) { return i < 0 ? 0 : (i > n - 1 ? n - 1 : i); };
+            const int x0 = cl(int(fx), bnx), x1 = cl(int(fx) + 1, bnx);
+            const int y0 = cl(int(fy), bny), y1 = cl(int(fy) + 1, bny);
+            const int z0 = cl(int(fz), bnz), z1 = cl(int(fz) + 1, bnz);
+            const R c00 = get(x0, y0, z0) * (R(1) - ax) + get(x1, y0, z0) * ax;
+            const R c10 = get(x0, y1, z0) * (R(1) - ax) + get(x1, y1, z0) * ax;
+            const R c01 = get(x0, y0, z1) * (R(1) - ax) + get(x1, y0, z1) * ax;
+            const R c11 = get(x0, y1, z1) * (R(1) - ax) + get(x1, y1, z1) * ax;
+            const R c0 = c00 * (R(1) - ay) + c10 * ay;
+            const R c1 = c01 * (R(1) - ay) + c11 * ay;
+            return c0 * (R(1) - az) + c1 * az;
+        };
+        for_cells([&](int x, int y, int z) {
+            const R lx = R(x - nx / 2) * dx, ly = R(y - ny / 2) * dx, lz = R(z - nz / 2) * dx;
+            const R gx = R(pos[0]) + (lx * c1 + lz * s1), gy = R(pos[1]) + ly, gz = R(pos[2]) + (lz * c1 - lx * s1);
+            const R rx = gx - R(posb[0]), ry = gy - R(posb[1]), rz = gz - R(posb[2]);
+            const R bx = rx * c2 + rz * s2, by = ry, bz = rz * c2 - rx * s2;
+            const R u = bx / (R(bnx) * bg.dx) + R(0.5);
+            const R v = by / (R(bny) * bg.dx) + R(0.5);
+            const R w = bz / (R(bnz) * bg.dx) + R(0.5);
+            V3<R> uu;
+            for (int k = 0; k < 3; ++k)
+                uu.c[k] = sample([&](int X, int Y, int Z) { return bg.velT[bg.idx(X, Y, Z)].c[k]; }, u, v, w);
+            const size_t P = idx(x, y, z);
+            vel[P] = uu; velT[P] = uu; velI[P] = uu;
+            velC[P] = V3<R>{{R(0), R(0), R(0)}};
+            p[P] = sample([&](int X, int Y, int Z) { return bg.p[bg.idx(X, Y, Z)]; }, u, v, w);
+            pc[P] = R(0); pcL[P] = R(0);
+        });
+    }
     // CSSetZeroVelBndCond, InitShaderColl.compute:229-248
     void set_zero_vel_bnd_cond() {
         for (auto& b : bnd) std::fill(b.begin(), b.end(), V3<R>{{R(0), R(0), R(0)}});
@@ -904,6 +947,20 @@ int wfo_create(const wf_config* cfg, int precision, int threads, wfo_solver** ou
         return WF_ERR_OOM;
     }
     *out = h;
+    return WF_OK;
+}
+
+int wfo_init_from_background(wfo_solver* h, const wfo_solver* bg, const float pos[3], const float pos_bg[3],
+                             float rot_deg) {
+    if (!h || !bg || h == bg || !pos || !pos_bg || !h->impl || !bg->impl) return WF_ERR_INVALID_ARG;
+    if (h->impl->precision() != bg->impl->precision()) return WF_ERR_INVALID_ARG;
+    if (h->impl->precision() == 32) {
+        static_cast<OracleT<float>*>(h->impl.get())->o.init_from_background(
+            static_cast<const OracleT<float>*>(bg->impl.get())->o, pos, pos_bg, rot_deg);
+    } else {
+        static_cast<OracleT<double>*>(h->impl.get())->o.init_from_background(
+            static_cast<const OracleT<double>*>(bg->impl.get())->o, pos, pos_bg, rot_deg);
+    }
     return WF_OK;
 }
 

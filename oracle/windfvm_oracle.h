@@ -35,6 +35,8 @@ int wfo_init_flags(wfo_solver* h, const int32_t* flags, size_t n);
 int wfo_init_vel_pres_fields(wfo_solver* h);
 int wfo_set_fixed_value_vel_bnd_cond(wfo_solver* h, float wind_speed);
 int wfo_set_inflow_plane(wfo_solver* h, const float* x0_plane_xyz);
+int wfo_init_from_background(wfo_solver* h, const wfo_solver* bg, const float pos[3], const float pos_bg[3],
+                             float rot_deg);
 int wfo_step(wfo_solver* h, int n_steps);
 
 /* Field transfer in FP64 (so the FP64 instance loses nothing); vectors SoA. */

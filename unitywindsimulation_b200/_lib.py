@@ -24,6 +24,7 @@ WF_ERR_TIMEOUT = 5
 WF_ERR_UNSUPPORTED = 6
 WF_NOT_FINISHED = 7
 WF_ERR_STATE = 8
+WF_ERR_IO = 9
 
 # ---- enums ----
 CELL_FLUID, CELL_SOLID = 0, 1
@@ -132,6 +133,7 @@ _SIGNATURES = {
     "wf_init_vel_pres_fields": (c_int, [c_void_p]),
     "wf_set_fixed_value_vel_bnd_cond": (c_int, [c_void_p, c_float]),
     "wf_change_phys_field_pos": (c_int, [c_void_p]),
+    "wf_init_from_background": (c_int, [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float), c_float]),
     "wf_set_inflow_plane": (c_int, [c_void_p, POINTER(c_float)]),
     "wf_step": (c_int, [c_void_p, c_int, POINTER(c_int)]),
     "wf_get_vel": (c_int, [c_void_p, POINTER(c_float), c_int]),
@@ -179,6 +181,11 @@ _SIGNATURES = {
     "wf_prepare_graphs": (c_int, [c_void_p]),
     "wf_set_blocking": (c_int, [c_void_p, c_int, c_int]),
     "wf_get_blocking": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
+    "wf_export_open": (c_int, [c_void_p, c_char_p, c_int, c_int, c_int, POINTER(c_void_p)]),
+    "wf_export_frame": (c_int, [c_void_p, c_float]),
+    "wf_export_frames_written": (c_int, [c_void_p, POINTER(c_int64)]),
+    "wf_export_last_error": (c_char_p, [c_void_p]),
+    "wf_export_close": (c_int, [c_void_p]),
     "wf_adj_create": (c_int, [c_void_p, POINTER(c_void_p)]),
     "wf_adj_destroy": (c_int, [c_void_p]),
     "wf_adj_last_error": (c_char_p, [c_void_p]),

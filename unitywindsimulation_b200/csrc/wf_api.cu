@@ -971,6 +971,7 @@ const char* wf_strerror(int s) {
         case WF_ERR_UNSUPPORTED: return "unsupported option";
         case WF_NOT_FINISHED: return "step not finished";
         case WF_ERR_STATE: return "invalid handle state";
+        case WF_ERR_IO: return "file error";
         default: return "unknown status";
     }
 }

@@ -89,6 +89,16 @@ class FvmSolverCuda:
     def ChangePhysFieldPos(self) -> None:
         self._check(self._lib.wf_change_phys_field_pos(self._h))
 
+    def InitVelPresFieldsFromBackGroundFlow(self, background: "FvmSolverCuda", pos=(0.0, 0.0, 0.0),
+                                            pos_background=(0.0, 0.0, 0.0), rot_deg: float = 0.0) -> None:
+        """Velocity and pressure from a background solver's current fields,
+        sampled at this domain's cells (wf_init_from_background).  pos /
+        pos_background: domain centres (physFieldPos), rot_deg: this domain's
+        rotation about the vertical axis (flowFieldOrientation)."""
+        p = (c_float * 3)(*[float(v) for v in pos])
+        q = (c_float * 3)(*[float(v) for v in pos_background])
+        self._check(self._lib.wf_init_from_background(self._h, background._h, p, q, float(rot_deg)))
+
     def ChangePhysDomainSize(self, cfg: WfConfig | None = None, device: int = 0) -> None:
         """Re-creates the handle for a new grid (the reference re-reads gridRes
         and re-initialises the fields, FvmSolverGpu.cs:1034-1046)."""
@@ -226,6 +236,56 @@ class FvmSolverCuda:
         fn = getattr(self._lib, f"wf_op_{which}_residual")
         self._check(fn(self._h, byref(out)))
         return out.value
+
+
+class FieldExporter:
+    """Velocity/pressure frames appended to a netCDF file while the solver
+    runs (wf_export_*; the file layout of the reference's
+    NcFlowFieldExporter).  ``frame(t)`` queues the solver's current fields;
+    ``close()`` drains the queue and finalises the file."""
+
+    def __init__(self, solver: FvmSolverCuda, path: str, save_vel: bool = True, save_pres: bool = True,
+                 ring: int = 3):
+        self._lib = _lib.load()
+        self.solver = solver
+        e = c_void_p()
+        st = self._lib.wf_export_open(solver._h, str(path).encode(), int(save_vel), int(save_pres), int(ring),
+                                      byref(e))
+        if st != _lib.WF_OK:
+            raise WindFvmError(st, f"wf_export_open: {self._lib.wf_last_error(solver._h).decode()}")
+        self._e = e
+
+    def _check(self, st):
+        if st != _lib.WF_OK:
+            raise WindFvmError(st, self._lib.wf_export_last_error(self._e).decode() or
+                               self._lib.wf_strerror(st).decode())
+
+    def frame(self, phys_time: float) -> None:
+        self._check(self._lib.wf_export_frame(self._e, float(phys_time)))
+
+    def frames_written(self) -> int:
+        n = c_int64(0)
+        self._check(self._lib.wf_export_frames_written(self._e, byref(n)))
+        return n.value
+
+    def close(self) -> None:
+        if getattr(self, "_e", None):
+            e, self._e = self._e, None
+            st = self._lib.wf_export_close(e)
+            if st != _lib.WF_OK:
+                raise WindFvmError(st, "wf_export_close failed")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class BatchSolver:
