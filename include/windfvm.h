@@ -420,6 +420,13 @@ typedef struct wf_objective {
  * (nullable): device time of the forward pass and of the whole call.
  * Derivatives are summed with float atomics: repeated calls agree to
  * rounding, not bit for bit. */
+/* Device memory of the gradient: one step tape takes about
+ * (3 nV + (nP + 1)(nC + 1) + 45) floats per cell.  A checkpoint segment is
+ * reversed from checkpoint_every tapes when they fit; otherwise (or beyond
+ * max_tapes, 0 = no cap) the segment's states are stored and it is reversed
+ * in sub-blocks of the tapes that fit, at the cost of one more recomputed
+ * step per step.  Results do not depend on the split. */
+int wf_adj_set_max_tapes(wf_adjoint* a, int max_tapes);
 int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
                     double* J, double* dJ_dustar, double* dJ_dz0, float* dJ_ddrag, float* ms_forward,
                     float* ms_total);

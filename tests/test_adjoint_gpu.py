@@ -225,6 +225,26 @@ def test_checkpoint_interval_does_not_change_gradient(built):
         assert abs(r["dJ_dz0"] - out[0]["dJ_dz0"]) <= 1e-5 * abs(out[0]["dJ_dz0"])
 
 
+def test_tape_cap_does_not_change_gradient(built):
+    """Segments longer than the tape cap are reversed in sub-blocks from
+    stored segment states; the gradient is the same."""
+    case = cases.small_soft_case(seed=9)
+    obj = Objective(x0=4, x1=20, z0=2, z1=14, y=1, window=3)
+    out = []
+    for cap in (0, 2, 1):
+        g = FvmSolverCuda(case.cfg)
+        cases.apply_case(g, case)
+        with AdjointSolver(g) as adj:
+            adj.set_max_tapes(cap)
+            out.append(adj.gradient(obj, 7, checkpoint_every=5, soft=case.soft))
+        g.close()
+    for r in out[1:]:
+        assert r["J"] == pytest.approx(out[0]["J"], rel=1e-12)
+        assert r["dJ_dustar"] == pytest.approx(out[0]["dJ_dustar"], rel=1e-5)
+        np.testing.assert_allclose(r["dJ_dheights"], out[0]["dJ_dheights"], rtol=1e-4,
+                                   atol=1e-6 * np.abs(out[0]["dJ_dheights"]).max())
+
+
 def test_autograd_function(built):
     torch = pytest.importorskip("torch")
     case = cases.small_soft_case(seed=8)

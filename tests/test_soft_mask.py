@@ -31,6 +31,22 @@ def test_height_gradient_chain_rule():
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd))
 
 
+def test_rotated_footprints_chain_rule():
+    rng = np.random.default_rng(1)
+    nx, ny, nz = 24, 10, 20
+    sb = SoftBuildings([(4, 9, 3, 8), (13, 18, 10, 16)], [4.2, 6.7], chi_max=300.0, angle_deg=30.0)
+    assert sb.footprint_mask(0, nx, nz).sum() > 10
+    w = rng.standard_normal((nz, ny, nx))
+    g = sb.height_gradient(w, nx, ny, nz)
+    for i in range(2):
+        hp, hm = sb.heights.copy(), sb.heights.copy()
+        hp[i] += 1e-5
+        hm[i] -= 1e-5
+        fd = ((w * sb.with_heights(hp).drag(nx, ny, nz, np.float64)).sum()
+              - (w * sb.with_heights(hm).drag(nx, ny, nz, np.float64)).sum()) / 2e-5
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd))
+
+
 def test_adjoint_street_case():
     c = cases.adjoint_street()
     assert c.soft is not None and len(c.soft.footprints) == 12

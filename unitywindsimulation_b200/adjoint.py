@@ -86,6 +86,11 @@ class AdjointSolver:
     def __exit__(self, *exc):
         self.close()
 
+    def set_max_tapes(self, max_tapes: int) -> None:
+        """Caps the step tapes a gradient keeps on the device (0: as many as
+        fit); longer checkpoint segments are reversed in sub-blocks."""
+        self._check(self._lib.wf_adj_set_max_tapes(self._a, int(max_tapes)))
+
     def step_forward(self, phases: int = PHASE_FULL):
         """State after one step from the solver's current state, cut after
         ``phases`` parts; the solver does not advance.  Returns (u (3, N), p (N))."""

@@ -18,7 +18,7 @@ Workloads (synthetic, seeded):
   batch_directions 16 uneven grids 96..192 x 48..80(up) x 96..160, 8-32
                   buildings each, wind rotated by k * 22.5 degrees
   adjoint_street  128 x 64(up) x 96, 12 soft buildings with continuous heights
-  adjoint_batch   8 directions x 256 x 96(up) x 256, 64 buildings
+  adjoint_batch   8 directions x 256 x 96(up) x 256, 64 soft buildings
 """
 from __future__ import annotations
 
@@ -263,6 +263,34 @@ def adjoint_street(seed: int = 4, nv: int = 50, np_: int = 30, steps: int = 200)
 
 ADJOINT_STREET_OBJECTIVE = dict(x0=48, x1=80, z0=32, z1=64, y=3, window=100)
 ADJOINT_STREET_CHECKPOINT = 20
+
+
+def adjoint_batch(seed: int = 6, n_dirs: int = 8, nv: int = 50, np_: int = 40, steps: int = 400):
+    """Adjoint at scale: n_dirs wind directions (k * 360/n_dirs degrees; the
+    footprints rotate, the domain stays aligned with the flow) over one
+    256 x 96(up) x 256 block array of 0.5 m cells with 64 soft buildings
+    (footprints 6-16 cells, heights uniform in [6, 40] cells), PISO laminar,
+    nP = 40, dt at CFL 0.25, a 400-step window with checkpoints every 25."""
+    nx, ny, nz, dx = 256, 96, 256, 0.5
+    rng = np.random.default_rng(seed)
+    blds = street_lattice_buildings(rng, nx, nz, 64, 6, 16, 6, 40, integer_heights=False)
+    ustar, z0 = 0.5, 0.1
+    umax = float(log_profile((ny - 0.5) * dx, ustar, z0))
+    out = []
+    for k in range(n_dirs):
+        angle = k * 360.0 / n_dirs
+        cfg = _les_piso_cfg(nx, ny, nz, dx, cfl_dt(umax, dx, 0.25), ustar, z0, 0.1, nv, np_)
+        cfg.turbulence = _lib.TURB_NONE
+        soft = SoftBuildings([b[:4] for b in blds], [b[4] for b in blds], chi_max=50.0 / cfg.dt, width=1.0,
+                             angle_deg=angle)
+        flags = np.zeros((nz, ny, nx), dtype=np.int32)
+        out.append(Case(f"adjoint_batch_{angle:g}deg", cfg, flags, None, steps, seed,
+                        [b + (angle,) for b in blds], soft))
+    return out
+
+
+ADJOINT_BATCH_OBJECTIVE = dict(x0=112, x1=144, z0=112, z1=144, y=3, window=200)
+ADJOINT_BATCH_CHECKPOINT = 25
 
 
 def aij_building(nv: int = 100, np_: int = 1000, steps: int = 1) -> Case:

@@ -639,6 +639,7 @@ struct wf_adjoint {
     int nV = 0, nP = 0, nC = 0;
     size_t N = 0;
     std::vector<Tape> tapes;                    // tapes[0] always allocated
+    int max_tapes = 0;                          // cap on the tapes a gradient uses (0: as many as fit)
     std::vector<void*> blocks;                  // allocations behind the tapes
     // adjoint work
     float *ub = nullptr, *uTb = nullptr, *pb = nullptr, *pb_in = nullptr;
@@ -930,6 +931,12 @@ int wf_adj_destroy(wf_adjoint* a) {
 
 const char* wf_adj_last_error(const wf_adjoint* a) { return a ? a->err.c_str() : "null adjoint"; }
 
+int wf_adj_set_max_tapes(wf_adjoint* a, int max_tapes) {
+    if (!a || max_tapes < 0) return WF_ERR_INVALID_ARG;
+    a->max_tapes = max_tapes;
+    return WF_OK;
+}
+
 int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const float* pbar_out, float* ubar_in,
                     float* pbar_in, float* gbar_planes, float* dragbar) {
     if (!a || phases < 1 || phases > 3 || !ubar_out || !pbar_out || !ubar_in || !pbar_in)
@@ -990,17 +997,20 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     const int area = (obj->x1 - obj->x0) * (obj->z1 - obj->z0);
     const float w = 1.f / (float)(obj->window * area);
     const dim3 og((obj->x1 - obj->x0 + 31) / 32, (obj->z1 - obj->z0 + 7) / 8), ob(32, 8);
-    // checkpoints: state n for n % C == 0 (n < n_steps); the steps of one
-    // segment are recomputed into C tapes and reversed
+    // checkpoints: state n for n % C == 0 (n < n_steps).  The steps of one
+    // segment are recomputed into tapes and reversed: all C at once when C
+    // tapes fit in device memory, else the segment's states are stored and
+    // it is reversed in sub-blocks of as many tapes as fit (one more
+    // recomputation per step).
     const int C = std::min(checkpoint_every, n_steps);
     const int nck = (n_steps + C - 1) / C;
-    int rs = ensure_tapes(a, C);
-    if (rs != WF_OK) return rs;
-    struct Events {
+    struct Scratch {
         cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-        ~Events() {
+        float* states = nullptr;  // C states of 4N floats (sub-block mode)
+        ~Scratch() {
             for (cudaEvent_t e : ev)
                 if (e) cudaEventDestroy(e);
+            if (states) cudaFree(states);
         }
     } E;
     for (float* p : a->ck) cudaFree(p);
@@ -1010,6 +1020,26 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
             cudaGetLastError();
             return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
         }
+    const int cap = a->max_tapes > 0 ? std::min(C, a->max_tapes) : C;
+    int T = std::min((int)a->tapes.size(), cap);
+    if (T < cap) {
+        // as many tapes as fit, keeping room for the segment states
+        const size_t tape_bytes = tape_floats(a) * sizeof(float);
+        const size_t reserve = (size_t)C * (v + s) + (size_t(1) << 30);
+        while (T < cap) {
+            size_t fr = 0, tot = 0;
+            if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || fr < tape_bytes + reserve) break;
+            if (ensure_tapes(a, T + 1) != WF_OK) break;
+            T = (int)a->tapes.size();
+        }
+        cudaGetLastError();
+        if (T < 1) return adj_fail(a, WF_ERR_OOM, "no device memory for one step tape");
+    }
+    T = std::min(T, cap);
+    if (T < C && cudaMalloc((void**)&E.states, (size_t)C * (v + s)) != cudaSuccess) {
+        cudaGetLastError();
+        return adj_fail(a, WF_ERR_OOM, "no device memory for the segment states: lower checkpoint_every");
+    }
     for (cudaEvent_t& e : E.ev) WFA_CUDA(cudaEventCreate(&e));
     WFA_CUDA(cudaMemsetAsync(a->dJ, 0, sizeof(double), h->st));
     WFA_CUDA(cudaEventRecord(E.ev[0], h->st));
@@ -1032,23 +1062,39 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     WFA_CUDA(cudaMemsetAsync(a->pb, 0, s, a->st));
     WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(P) * sizeof(float), a->st));
     WFA_CUDA(cudaMemsetAsync(a->dragb, 0, s, a->st));
+    int rs = WF_OK;
     for (int sgi = nck - 1; sgi >= 0; --sgi) {
-        const int n0 = sgi * C, n1 = std::min(n_steps, n0 + C);
-        for (int n = n0; n < n1; ++n) {
-            Tape& t = a->tapes[n - n0];
-            const float* ui = n == n0 ? a->ck[sgi] : a->tapes[n - n0 - 1].uout;
-            const float* pi = n == n0 ? a->ck[sgi] + 3 * N : a->tapes[n - n0 - 1].pout;
-            rs = record_step(a, t, ui, pi, 3);
-            if (rs != WF_OK) return rs;
+        const int n0 = sgi * C, n1 = std::min(n_steps, n0 + C), L = n1 - n0;
+        // state j of the segment (state n0 + j): from the checkpoint, or
+        // from the stored segment states in sub-block mode
+        auto state = [&](int j) -> float* { return j == 0 ? a->ck[sgi] : E.states + (size_t)j * 4 * N; };
+        if (L > T) {
+            for (int j = 1; j < L; ++j) {
+                rs = record_step(a, a->tapes[0], state(j - 1), state(j - 1) + 3 * N, 3);
+                if (rs != WF_OK) return rs;
+                WFA_CUDA(cudaMemcpyAsync(state(j), a->tapes[0].uout, v, cudaMemcpyDeviceToDevice, a->st));
+                WFA_CUDA(cudaMemcpyAsync(state(j) + 3 * N, a->tapes[0].pout, s, cudaMemcpyDeviceToDevice, a->st));
+            }
         }
-        for (int n = n1 - 1; n >= n0; --n) {
-            // step n maps state n to state n+1
-            const Tape& t = a->tapes[n - n0];
-            if (n + 1 > n_steps - obj->window)
-                wf::k_objective<<<og, ob, 0, a->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
-                                                      t.uout, a->ub, nullptr);
-            rs = adjoint_step(a, t, 3);
-            if (rs != WF_OK) return rs;
+        for (int hi = L; hi > 0;) {
+            const int lo = std::max(0, hi - T);
+            for (int j = lo; j < hi; ++j) {
+                Tape& t = a->tapes[j - lo];
+                const float* ui = j == lo ? state(lo) : a->tapes[j - lo - 1].uout;
+                const float* pi = j == lo ? state(lo) + 3 * N : a->tapes[j - lo - 1].pout;
+                rs = record_step(a, t, ui, pi, 3);
+                if (rs != WF_OK) return rs;
+            }
+            for (int j = hi - 1; j >= lo; --j) {
+                // step n0 + j maps state n0 + j to state n0 + j + 1
+                const Tape& t = a->tapes[j - lo];
+                if (n0 + j + 1 > n_steps - obj->window)
+                    wf::k_objective<<<og, ob, 0, a->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
+                                                          t.uout, a->ub, nullptr);
+                rs = adjoint_step(a, t, 3);
+                if (rs != WF_OK) return rs;
+            }
+            hi = lo;
         }
     }
     WFA_CUDA(cudaEventRecord(E.ev[2], a->st));

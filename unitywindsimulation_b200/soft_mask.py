@@ -31,6 +31,7 @@ class SoftBuildings:
     heights: np.ndarray       # float64, cells
     chi_max: float            # drag of a fully solid cell, 1/s
     width: float = 1.0        # sigmoid width, cells
+    angle_deg: float = 0.0    # footprints rotated about the domain centre (x-z plane)
 
     def __post_init__(self):
         self.heights = np.asarray(self.heights, dtype=np.float64)
@@ -40,13 +41,31 @@ class SoftBuildings:
     def with_heights(self, heights) -> "SoftBuildings":
         return dataclasses.replace(self, heights=np.asarray(heights, dtype=np.float64).copy())
 
+    def footprint_mask(self, i: int, nx: int, nz: int) -> np.ndarray:
+        """Cells (nz, nx) of footprint i: cell centres inside the rectangle
+        after rotating it by angle_deg about the domain centre."""
+        x0, x1, z0, z1 = self.footprints[i]
+        if self.angle_deg == 0.0:
+            m = np.zeros((nz, nx), dtype=bool)
+            m[z0:z1, x0:x1] = True
+            return m
+        X, Z = np.meshgrid(np.arange(nx) + 0.5, np.arange(nz) + 0.5)
+        cx, cz = nx / 2.0, nz / 2.0
+        th = np.radians(self.angle_deg)
+        c, s = np.cos(th), np.sin(th)
+        xr = cx + (X - cx) * c + (Z - cz) * s
+        zr = cz - (X - cx) * s + (Z - cz) * c
+        return (xr >= x0) & (xr < x1) & (zr >= z0) & (zr < z1)
+
     def drag(self, nx: int, ny: int, nz: int, dtype=np.float32) -> np.ndarray:
         """Drag field chi, shape (nz, ny, nx)."""
         out = np.zeros((nz, ny, nx), dtype=np.float64)
         yc = np.arange(ny, dtype=np.float64) + 0.5
-        for (x0, x1, z0, z1), h in zip(self.footprints, self.heights):
+        for i, h in enumerate(self.heights):
             a = self.chi_max * _sigmoid((h - yc) / self.width)
-            out[z0:z1, :, x0:x1] = np.maximum(out[z0:z1, :, x0:x1], a[None, :, None])
+            m = self.footprint_mask(i, nx, nz)
+            col = np.where(m[:, None, :], a[None, :, None], 0.0)
+            np.maximum(out, col, out=out)
         return out.astype(dtype)
 
     def height_gradient(self, dJ_ddrag: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
@@ -56,8 +75,9 @@ class SoftBuildings:
         g = np.asarray(dJ_ddrag, dtype=np.float64).reshape(nz, ny, nx)
         yc = np.arange(ny, dtype=np.float64) + 0.5
         out = np.zeros(self.heights.size)
-        for i, ((x0, x1, z0, z1), h) in enumerate(zip(self.footprints, self.heights)):
+        for i, h in enumerate(self.heights):
             s = _sigmoid((h - yc) / self.width)
             dchi_dh = self.chi_max * s * (1.0 - s) / self.width
-            out[i] = float((g[z0:z1, :, x0:x1].sum(axis=(0, 2)) * dchi_dh).sum())
+            m = self.footprint_mask(i, nx, nz)
+            out[i] = float((g.transpose(1, 0, 2)[:, m].sum(axis=1) * dchi_dh).sum())
         return out
