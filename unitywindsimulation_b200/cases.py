@@ -288,7 +288,7 @@ def adjoint_batch(seed: int = 6, n_dirs: int = 8, nv: int = 50, np_: int = 40, s
         # sweeps diverges inside the 400-step window on this grid
         cfg.mu = 0.3
         soft = SoftBuildings([b[:4] for b in blds], [b[4] for b in blds], chi_max=50.0 / cfg.dt, width=1.0,
-                             angle_deg=angle)
+                             angle_deg=angle, margin=MARGIN)
         flags = np.zeros((nz, ny, nx), dtype=np.int32)
         out.append(Case(f"adjoint_batch_{angle:g}deg", cfg, flags, None, steps, seed,
                         [b + (angle,) for b in blds], soft))

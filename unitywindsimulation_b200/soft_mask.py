@@ -32,6 +32,7 @@ class SoftBuildings:
     chi_max: float            # drag of a fully solid cell, 1/s
     width: float = 1.0        # sigmoid width, cells
     angle_deg: float = 0.0    # footprints rotated about the domain centre (x-z plane)
+    margin: int = 0           # cells this close to the x/z boundaries stay free
 
     def __post_init__(self):
         self.heights = np.asarray(self.heights, dtype=np.float64)
@@ -43,19 +44,22 @@ class SoftBuildings:
 
     def footprint_mask(self, i: int, nx: int, nz: int) -> np.ndarray:
         """Cells (nz, nx) of footprint i: cell centres inside the rectangle
-        after rotating it by angle_deg about the domain centre."""
+        after rotating it by angle_deg about the domain centre, outside the
+        boundary margin (the rule of the binary rasteriser in cases.py)."""
         x0, x1, z0, z1 = self.footprints[i]
-        if self.angle_deg == 0.0:
-            m = np.zeros((nz, nx), dtype=bool)
-            m[z0:z1, x0:x1] = True
-            return m
         X, Z = np.meshgrid(np.arange(nx) + 0.5, np.arange(nz) + 0.5)
-        cx, cz = nx / 2.0, nz / 2.0
-        th = np.radians(self.angle_deg)
-        c, s = np.cos(th), np.sin(th)
-        xr = cx + (X - cx) * c + (Z - cz) * s
-        zr = cz - (X - cx) * s + (Z - cz) * c
-        return (xr >= x0) & (xr < x1) & (zr >= z0) & (zr < z1)
+        if self.angle_deg == 0.0:
+            m = (X >= x0) & (X < x1) & (Z >= z0) & (Z < z1)
+        else:
+            cx, cz = nx / 2.0, nz / 2.0
+            th = np.radians(self.angle_deg)
+            c, s = np.cos(th), np.sin(th)
+            xr = cx + (X - cx) * c + (Z - cz) * s
+            zr = cz - (X - cx) * s + (Z - cz) * c
+            m = (xr >= x0) & (xr < x1) & (zr >= z0) & (zr < z1)
+        if self.margin > 0:
+            m &= (X > self.margin) & (X < nx - self.margin) & (Z > self.margin) & (Z < nz - self.margin)
+        return m
 
     def drag(self, nx: int, ny: int, nz: int, dtype=np.float32) -> np.ndarray:
         """Drag field chi, shape (nz, ny, nx)."""
