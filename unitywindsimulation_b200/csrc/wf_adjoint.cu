@@ -749,14 +749,14 @@ int record_step(wf_adjoint* a, Tape& t, const float* u_in, const float* p_in, in
     WFA_CUDA(cudaMemcpyAsync(t.uout, ustar, v, cudaMemcpyDeviceToDevice, st));
     WFA_CUDA(cudaMemcpyAsync(t.pout, t.p0, s, cudaMemcpyDeviceToDevice, st));
     if (phases >= 2) {
-        wf::launch_pres_precompute(P, h->B, st, h->fl, ustar, t.p0, t.D, t.Dp, t.bp);
-        wf::launch_pres_coef_ptr(P, st, h->fl, t.D, t.c3);
+        wf::launch_pres_precompute(P, h->B, st, h->fl, ustar, t.p0, t.D, t.iD, t.Dp, t.bp);
+        wf::launch_pres_coef_ptr(P, st, h->fl, t.D, t.iD, t.c3);
         wf::launch_inv_ptr(P, st, h->fl, t.Dp, t.ainv);
         WFA_CUDA(cudaMemsetAsync(t.qit, 0, s, st));
         wf::launch_pres_stack(P, st, h->num_sms, t.c3, t.ainv, t.bp, t.qit, a->nP, true);
         const float* q = S(a, t.qit, a->nP);
         WFA_CUDA(cudaMemsetAsync(t.cbuf, 0, v, st));
-        wf::launch_apply_vel(P, st, h->fl, q, t.D, V(a, t.cbuf, 0), t.uout);
+        wf::launch_apply_vel(P, st, h->fl, q, t.D, t.iD, V(a, t.cbuf, 0), t.uout);
         wf::launch_apply_pres(P, st, h->fl, q, t.pout);
     }
     if (phases >= 3) {
@@ -765,12 +765,12 @@ int record_step(wf_adjoint* a, Tape& t, const float* u_in, const float* p_in, in
             WFA_CUDA(cudaMemsetAsync(V(a, t.cbuf, m + 1), 0, v, st));
             WFA_CUDA(cudaMemsetAsync(SIT(a, t, m, 0), 0, s, st));
             wf::launch_piso_aodu(P, st, h->fl, V(a, t.cbuf, m), t.uT, h->eddy, h->face, V(a, t.aod, m));
-            wf::launch_piso_pre_ptr(P, st, h->fl, t.D, V(a, t.aod, m), S(a, t.pai, m), S(a, t.prhs, m));
+            wf::launch_piso_pre_ptr(P, st, h->fl, t.D, t.iD, V(a, t.aod, m), S(a, t.pai, m), S(a, t.prhs, m));
             wf::launch_pres_stack(P, st, h->num_sms, t.c3, S(a, t.pai, m), S(a, t.prhs, m), SIT(a, t, m, 0),
                                   a->nP, true);
             const float* ss = SIT(a, t, m, a->nP);
             wf::launch_apply_pres(P, st, h->fl, ss, t.pout);
-            wf::launch_piso_vel(P, st, h->fl, ss, t.D, V(a, t.aod, m), V(a, t.cbuf, m + 1), t.uout);
+            wf::launch_piso_vel(P, st, h->fl, ss, t.D, t.iD, V(a, t.aod, m), V(a, t.cbuf, m + 1), t.uout);
         }
     }
     WFA_CUDA(cudaGetLastError());

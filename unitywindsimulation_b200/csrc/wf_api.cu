@@ -114,7 +114,7 @@ void free_all(wf_solver* h) {
     wf::drop_graphs(h);
     void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->vb[3], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
                     h->pcb[0], h->pcb[1], h->pcb[2], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->grad, h->part, h->dsum, h->dref,
-                    h->dbad, h->stage, h->bnd[0], h->drag};
+                    h->dbad, h->stage, h->bnd[0], h->drag, h->nbm};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->hsum) cudaFreeHost(h->hsum);
@@ -158,7 +158,11 @@ int do_les(wf_solver* h) {
     return WF_OK;
 }
 
+// 1/D cached by the fast momentum path for the current D, or null.
+const float* cur_inv_d(const wf_solver* h) { return h->id_gen == h->d_gen ? h->vcoef + 6 * (size_t)h->P.N : nullptr; }
+
 int do_vel_precompute(wf_solver* h) {
+    ++h->d_gen;
     wf::launch_vel_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->pr, h->eddy, h->face,
                               h->P.les ? h->bv : nullptr, h->drag, h->Dv, h->bv);
     WF_CHECK_LAUNCH();
@@ -204,7 +208,7 @@ int do_vel_sweeps(wf_solver* h, int n, bool allow_fast) {
 }
 
 int do_pres_precompute(wf_solver* h) {
-    wf::launch_pres_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iF], h->pr, h->Dv, h->Dp, h->bp);
+    wf::launch_pres_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iF], h->pr, h->Dv, cur_inv_d(h), h->Dp, h->bp);
     WF_CHECK_LAUNCH();
     return WF_OK;
 }
@@ -248,7 +252,7 @@ int do_normalize(wf_solver* h) {
     return WF_OK;
 }
 int do_apply_vel(wf_solver* h) {
-    wf::launch_apply_vel(h->P, h->st, h->fl, pc_cur(h), h->Dv, h->uc, h->vb[h->iF]);
+    wf::launch_apply_vel(h->P, h->st, h->fl, pc_cur(h), h->Dv, cur_inv_d(h), h->uc, h->vb[h->iF]);
     WF_CHECK_LAUNCH();
     return WF_OK;
 }
@@ -274,11 +278,11 @@ int do_piso(wf_solver* h, int n, bool allow_fast) {
     wf::launch_apply_pres(P, h->st, h->fl, pc_cur(h), h->pr);
     const float* pc = pc_cur(h);
     if (pc) {
-        wf::launch_piso_vel(P, h->st, h->fl, pc, h->Dv, h->aodu, h->uc, h->vb[h->iF]);
+        wf::launch_piso_vel(P, h->st, h->fl, pc, h->Dv, cur_inv_d(h), h->aodu, h->uc, h->vb[h->iF]);
     } else {
         // p'' == 0: PisoVelCorrection with a zero field still applies -D^-1 AodU
         WF_TRY(materialize_pc(h));
-        wf::launch_piso_vel(P, h->st, h->fl, h->pcb[h->iPC], h->Dv, h->aodu, h->uc, h->vb[h->iF]);
+        wf::launch_piso_vel(P, h->st, h->fl, h->pcb[h->iPC], h->Dv, cur_inv_d(h), h->aodu, h->uc, h->vb[h->iF]);
     }
     WF_CHECK_LAUNCH();
     h->pc_zero = true;  // SetPresCorrectFieldtoZero (:1532)
@@ -584,6 +588,9 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
         (s = alloc(h, (void**)&h->dsum, 4 * sizeof(double))) || (s = alloc(h, (void**)&h->dref, sizeof(float) * 4)) ||
         (s = alloc(h, (void**)&h->dbad, sizeof(int) * 4)) || (s = alloc(h, (void**)&h->bnd[0], sizeof(float) * planes)))
         return fail(s);
+    if ((s = alloc(h, (void**)&h->nbm, N))) return fail(s);
+    P.nbm = h->nbm;
+    wf::launch_nbmask(P, h->st, h->fl, h->nbm);  // all fluid until wf_init_flags
     for (int f = 1; f < 6; ++f) h->bnd[f] = h->bnd[f - 1] + 3 * (size_t)P.plane[f - 1];
     for (int f = 0; f < 6; ++f) h->B.p[f] = h->bnd[f];
     if (cudaMallocHost((void**)&h->hsum, 4 * sizeof(double)) != cudaSuccess) return fail(WF_ERR_OOM);
@@ -615,6 +622,7 @@ int wf_init_flags(wf_solver* h, const int32_t* flags, size_t n) {
     WF_CUDA(cudaMemcpyAsync(h->stage, flags, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->st));
     wf::launch_init_flags(h->P, h->st, (const int32_t*)h->stage, h->fl, h->vb[0], h->vb[1], h->vb[2]);
     wf::launch_init_flags(h->P, h->st, (const int32_t*)h->stage, h->fl, h->vb[3], nullptr, nullptr);
+    wf::launch_nbmask(h->P, h->st, h->fl, h->nbm);
     WF_CHECK_LAUNCH();
     return sync(h);
 }
@@ -797,6 +805,7 @@ int wf_set_field(wf_solver* h, int field, const float* in) {
     WF_CUDA(cudaSetDevice(h->device));
     if (field == WF_FIELD_VEL_LAST_TIME || field == WF_FIELD_VEL_LAST_ITER) WF_TRY(materialize_iter(h));
     if (field == WF_FIELD_PRES_CORRECT || field == WF_FIELD_PRES_CORRECT_LAST_ITER) WF_TRY(materialize_pc(h));
+    if (field == WF_FIELD_D) ++h->d_gen;
     if (field == WF_FIELD_DRAG && !h->drag) {
         // first use: the captured step graphs hold the old (null) pointer
         WF_TRY(sync(h));

@@ -30,6 +30,9 @@ struct Params {
     int vbc[6], pbc[6];
     int les;
     unsigned compat;
+    // per-cell neighbour mask (see nb_fluid): bit f (0..5) = the neighbour
+    // across face f is inside the domain and fluid, bit 6 = the cell is fluid
+    const uint8_t* nbm;
 };
 
 // Boundary planes: base pointer of each plane (3 SoA components of
@@ -57,6 +60,15 @@ __device__ __forceinline__ bool in_region(const Params& P, int x, int y, int z) 
 __device__ __forceinline__ int cidx(const Params& P, int x, int y, int z) {
     return (z * P.ny + y) * P.nx + x;
 }
+// Index offset of the neighbour across face f.
+__device__ __forceinline__ int face_off(const Params& P, int f) {
+    return f == 0 ? 1 : f == 1 ? -1 : f == 2 ? P.nx : f == 3 ? -P.nx : f == 4 ? P.nx * P.ny : -(P.nx * P.ny);
+}
+// The neighbour across face f of cell (x, y, z) is inside the domain.
+__device__ __forceinline__ bool face_in(const Params& P, int x, int y, int z, int f) {
+    return f == 0 ? x + 1 < P.nx : f == 1 ? x > 0 : f == 2 ? y + 1 < P.ny : f == 3 ? y > 0 : f == 4 ? z + 1 < P.nz : z > 0;
+}
+__device__ __forceinline__ bool nb_fluid(unsigned mask, int f) { return (mask >> f) & 1u; }
 __device__ __forceinline__ int plane_idx(const Params& P, int bc, int x, int y, int z) {
     return bc <= WF_FACE_XN ? z * P.ny + y : (bc <= WF_FACE_YN ? z * P.nx + x : y * P.nx + x);
 }

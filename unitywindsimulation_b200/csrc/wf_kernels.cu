@@ -59,6 +59,30 @@ __device__ __forceinline__ float vis_face(const Params& P, const uint8_t* fl, co
     return v;
 }
 
+// vis_face from the neighbour mask (same values).
+__device__ __forceinline__ float vis_face_m(const Params& P, unsigned m, const float* eddy, const float* face,
+                                            const Cell& c, int f) {
+    if (!P.les) return P.nu;
+    const float eP = ld(eddy, c.i);
+    float v = P.nu + eP;
+    if (face_in(P, c.x, c.y, c.z, f)) {
+        const int q = c.i + face_off(P, f);
+        if (nb_fluid(m, f)) {
+            v = P.nu + 0.5f * (eP + ld(eddy, q));
+        } else {
+            v = P.nu + face_read(P, face, face_sign(f) > 0 ? q : c.i, face_axis(f));
+        }
+    } else if (f == 3 && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE) {
+        v = P.nu + face_read(P, face, c.i, 1);
+    }
+    return v;
+}
+// 1/D of component a at cell i: from the cached reciprocals when given
+// (computed with the same division), else divided here.
+__device__ __forceinline__ float inv_d(const float* iD, const float* Dv, size_t N, int a, int i) {
+    return iD ? ld(iD, a * N + i) : 1.f / ld(Dv, a * N + i);
+}
+
 // LogLawWallFunc, WallFunc.compute:77-123
 __device__ float log_law(float uP, float dx, float nu, float den) {
     const float E = 9.8f, k = 0.41f;
@@ -271,7 +295,9 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
                                  float* bv) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    if (!fluid_at(fl, c.i)) return;
+    const unsigned m = __ldg(P.nbm + c.i);
+    if (!(m & 64u)) return;
+    (void)fl;
     const size_t N = P.N;
     float uP[3];
 #pragma unroll
@@ -283,11 +309,9 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f);
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            if (fluid_at(fl, q)) {
-                const float t = P.ds * 0.25f * (uP[a] + ld(uT, a * N + q));
+        if (face_in(P, c.x, c.y, c.z, f)) {
+            if (nb_fluid(m, f)) {
+                const float t = P.ds * 0.25f * (uP[a] + ld(uT, a * N + c.i + face_off(P, f)));
 #pragma unroll
                 for (int k = 0; k < 3; ++k) D[k] = face_sign(f) > 0 ? D[k] + t : D[k] - t;
             }
@@ -312,10 +336,8 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
     float pf[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            pf[f] = fluid_at(fl, q) ? 0.5f * (pP + ld(pr, q)) : pP;
+        if (face_in(P, c.x, c.y, c.z, f)) {
+            pf[f] = nb_fluid(m, f) ? 0.5f * (pP + ld(pr, c.i + face_off(P, f))) : pP;
         } else {
             pf[f] = P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE ? 0.f : pP;
         }
@@ -325,10 +347,9 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
     // diffusion, :1593-1836
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        const float vis = vis_face(P, fl, eddy, face, c, f);
-        if (in_region(P, X, Y, Z)) {
-            const float t = fluid_at(fl, cidx(P, X, Y, Z)) ? vis * P.ds / P.dx : 2.f * vis * P.ds / P.dx;
+        const float vis = vis_face_m(P, m, eddy, face, c, f);
+        if (face_in(P, c.x, c.y, c.z, f)) {
+            const float t = nb_fluid(m, f) ? vis * P.ds / P.dx : 2.f * vis * P.ds / P.dx;
 #pragma unroll
             for (int k = 0; k < 3; ++k) D[k] += t;
         } else {
@@ -406,40 +427,45 @@ __global__ void k_vel_sweep(const __grid_constant__ Params P, const uint8_t* __r
 }
 
 // ----------------------------------------------------- pressure correction
-// CSPresCorrectRhieChowPreCompute, FvmColl.compute:2481-2787
+// CSPresCorrectRhieChowPreCompute, FvmColl.compute:2481-2787.  iD
+// (nullable): cached 1/D of the same D.
 __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
                                   const float* __restrict__ u, const float* __restrict__ pr,
-                                  const float* __restrict__ Dv, float* __restrict__ Dp, float* __restrict__ bp) {
+                                  const float* __restrict__ Dv, const float* __restrict__ iD,
+                                  float* __restrict__ Dp, float* __restrict__ bp) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    if (!fluid_at(fl, c.i)) return;
+    const unsigned m = __ldg(P.nbm + c.i);
+    if (!(m & 64u)) return;
+    (void)fl;
     const size_t N = P.N;
     const float dx2 = 2.f * P.dx;
     float DP = 0.f, bP = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f), s = face_sign(f);
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            if (!fluid_at(fl, q)) continue;
-            const float DInv = 0.5f * (1.f / ld(Dv, a * N + c.i) + 1.f / ld(Dv, a * N + q));
+        if (face_in(P, c.x, c.y, c.z, f)) {
+            if (!nb_fluid(m, f)) continue;
+            const int q = c.i + face_off(P, f);
+            const float DInv = 0.5f * (inv_d(iD, Dv, N, a, c.i) + inv_d(iD, Dv, N, a, q));
             DP -= (P.dv / P.den) * DInv / P.dx;
             const float fl_ = 0.5f * (ld(u, a * N + c.i) + ld(u, a * N + q));
             bP = s > 0 ? bP + fl_ : bP - fl_;
-            // Rhie-Chow over the face between low cell L and high cell H
+            // Rhie-Chow over the face between low cell L and high cell H: the
+            // cell beyond Q (q + off(f)) and the cell behind P (i - off(f))
+            const unsigned mq = __ldg(P.nbm + q);
+            const bool beyondQ = nb_fluid(mq, f), behindP = nb_fluid(m, f ^ 1);
             const int L = s > 0 ? c.i : q, H = s > 0 ? q : c.i;
-            const int lx = s > 0 ? c.x : X, ly = s > 0 ? c.y : Y, lz = s > 0 ? c.z : Z;
-            const int hx = s > 0 ? X : c.x, hy = s > 0 ? Y : c.y, hz = s > 0 ? Z : c.z;
-            const int ex = (a == 0), ey = (a == 1), ez = (a == 2);
-            const bool hh = in_region(P, hx + ex, hy + ey, hz + ez) && fluid_at(fl, cidx(P, hx + ex, hy + ey, hz + ez));
-            const bool ll = in_region(P, lx - ex, ly - ey, lz - ez) && fluid_at(fl, cidx(P, lx - ex, ly - ey, lz - ez));
+            const bool hh = s > 0 ? beyondQ : behindP;
+            const bool ll = s > 0 ? behindP : beyondQ;
+            const int HH = s > 0 ? q + face_off(P, f) : c.i + face_off(P, f ^ 1);
+            const int LL = s > 0 ? c.i + face_off(P, f ^ 1) : q + face_off(P, f);
             const float pL = ld(pr, L), pH = ld(pr, H);
             const float presGrad = (pH - pL) / P.dx;
             float ave = presGrad;
             if (hh || ll) {
-                const float gH = hh ? (ld(pr, cidx(P, hx + ex, hy + ey, hz + ez)) - pL) / dx2 : (pH - pL) / dx2;
-                const float gL = ll ? (pH - ld(pr, cidx(P, lx - ex, ly - ey, lz - ez))) / dx2 : (pH - pL) / dx2;
+                const float gH = hh ? (ld(pr, HH) - pL) / dx2 : (pH - pL) / dx2;
+                const float gL = ll ? (pH - ld(pr, LL)) / dx2 : (pH - pL) / dx2;
                 ave = 0.5f * (gH + gL);
             }
             const float vct = -(P.dv * DInv) / P.den * (presGrad - ave);
@@ -454,7 +480,7 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
                 bP = s > 0 ? bP + t : bP - t;
             }
             if (P.pbc[bc] == WF_BND_FIXED_VALUE) {
-                const float DInv = 1.f / ld(Dv, a * N + c.i);
+                const float DInv = inv_d(iD, Dv, N, a, c.i);
                 DP -= 2.f * (P.dv / P.den) * DInv / P.dx;
             }
         }
@@ -513,69 +539,64 @@ __global__ void k_norm_apply(const __grid_constant__ Params P, const uint8_t* __
 }
 
 // CSApplyVelCorrectionDivergenceTheorem, FvmColl.compute:2951-3121.
-// pc == nullptr reads as zero.
+// pc == nullptr reads as zero; iD (nullable): cached 1/D of the same D.
 __global__ void k_apply_vel(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                             const float* __restrict__ pc, const float* __restrict__ Dv,
-                            float* __restrict__ uc, float* __restrict__ u) {
+                            const float* __restrict__ iD, float* __restrict__ uc, float* __restrict__ u) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    if (!fluid_at(fl, c.i)) return;
+    const unsigned m = __ldg(P.nbm + c.i);
+    if (!(m & 64u)) return;
+    (void)fl;
     const size_t N = P.N;
     const float pP = pc ? ld(pc, c.i) : 0.f;
     float pf[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            pf[f] = fluid_at(fl, q) ? 0.5f * (pP + (pc ? ld(pc, q) : 0.f)) : pP;
+        if (face_in(P, c.x, c.y, c.z, f)) {
+            pf[f] = nb_fluid(m, f) ? 0.5f * (pP + (pc ? ld(pc, c.i + face_off(P, f)) : 0.f)) : pP;
         } else {
             pf[f] = P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE ? 0.f : pP;
         }
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float corr = -(P.dv / P.den) * (1.f / ld(Dv, a * N + c.i)) * (pf[2 * a] - pf[2 * a + 1]) / P.dx;
+        const float corr = -(P.dv / P.den) * inv_d(iD, Dv, N, a, c.i) * (pf[2 * a] - pf[2 * a + 1]) / P.dx;
         uc[a * N + c.i] = corr;
         u[a * N + c.i] += corr;
     }
 }
 
 // ------------------------------------------------------------------ PISO
-// CSPisoCalAodUCorrect, PisoColl.compute:71-178
+// CSPisoCalAodUCorrect, PisoColl.compute:71-178.  The advection and
+// diffusion sums run over the faces in the reference's order, in one loop
+// (each with its own accumulator, so the values are those of two loops).
 __global__ void k_piso_aodu(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                             const float* __restrict__ uc, const float* __restrict__ uT,
                             const float* __restrict__ eddy, const float* __restrict__ face,
                             float* __restrict__ aodu) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    if (!fluid_at(fl, c.i)) return;
+    const unsigned m = __ldg(P.nbm + c.i);
+    if (!(m & 64u)) return;
+    (void)fl;
     const size_t N = P.N;
     const bool consistent = (P.compat & WF_COMPAT_PISO_CONSISTENT) != 0;
     float adv[3] = {0.f, 0.f, 0.f}, dif[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
+        if (!nb_fluid(m, f)) continue;
         const int a = face_axis(f);
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (!in_region(P, X, Y, Z)) continue;
-        const int q = cidx(P, X, Y, Z);
-        if (!fluid_at(fl, q)) continue;
+        const int q = c.i + face_off(P, f);
         const float sum = ld(uT, a * N + c.i) + ld(uT, a * N + q);
+        const float vis = consistent ? vis_face_m(P, m, eddy, face, c, f) : P.nu;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float t = P.ds * 0.25f * ld(uc, k * N + q) * sum;
+            const float uq = ld(uc, k * N + q);
+            const float t = P.ds * 0.25f * uq * sum;
             adv[k] = face_sign(f) > 0 ? adv[k] + t : adv[k] - t;
+            dif[k] -= vis * P.ds / P.dx * uq;
         }
-    }
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (!in_region(P, X, Y, Z)) continue;
-        const int q = cidx(P, X, Y, Z);
-        if (!fluid_at(fl, q)) continue;
-        const float vis = consistent ? vis_face(P, fl, eddy, face, c, f) : P.nu;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) dif[k] -= vis * P.ds / P.dx * ld(uc, k * N + q);
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) aodu[k * N + c.i] = adv[k] + dif[k];
@@ -619,29 +640,26 @@ __global__ void k_piso_pres_sweep(const __grid_constant__ Params P, const uint8_
     pout[c.i] = (1.f / coeff) * (pt + vt);
 }
 
-// CSPisoVelCorrection, PisoColl.compute:270-337
+// CSPisoVelCorrection, PisoColl.compute:270-337.  iD (nullable): cached
+// 1/D of the same D.
 __global__ void k_piso_vel(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                            const float* __restrict__ pc, const float* __restrict__ Dv,
-                           const float* __restrict__ aodu, float* __restrict__ uc, float* __restrict__ u) {
+                           const float* __restrict__ iD, const float* __restrict__ aodu, float* __restrict__ uc,
+                           float* __restrict__ u) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    if (!fluid_at(fl, c.i)) return;
+    const unsigned m = __ldg(P.nbm + c.i);
+    if (!(m & 64u)) return;
+    (void)fl;
     const size_t N = P.N;
     const float pP = ld(pc, c.i);
     float pf[6];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        pf[f] = pP;
-        if (in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            if (fluid_at(fl, q)) pf[f] = 0.5f * (pP + ld(pc, q));
-        }
-    }
+    for (int f = 0; f < 6; ++f) pf[f] = nb_fluid(m, f) ? 0.5f * (pP + ld(pc, c.i + face_off(P, f))) : pP;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float grad = (pf[2 * a] - pf[2 * a + 1]) / P.dx;
-        const float DInv = 1.f / ld(Dv, a * N + c.i);
+        const float DInv = inv_d(iD, Dv, N, a, c.i);
         const float corr = -DInv * (ld(aodu, a * N + c.i) + P.dv / P.den * grad);
         uc[a * N + c.i] = corr;
         u[a * N + c.i] += corr;
@@ -835,6 +853,17 @@ __global__ void k_flags_to_i32(const uint8_t* __restrict__ f, int n, int32_t* __
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) o[i] = f[i];
 }
+// Neighbour mask (Params::nbm) of every cell from the flags.
+__global__ void k_nbmask(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
+                         uint8_t* __restrict__ nbm) {
+    Cell c;
+    if (!cell_of_thread(P, c)) return;
+    unsigned m = fluid_at(fl, c.i) ? 64u : 0u;
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        if (face_in(P, c.x, c.y, c.z, f) && fluid_at(fl, c.i + face_off(P, f))) m |= 1u << f;
+    nbm[c.i] = (uint8_t)m;
+}
 
 }  // namespace
 
@@ -879,8 +908,8 @@ void launch_vel_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const
     WF_LAUNCH(k_vel_sweep, fl, uI, uT, eddy, face, Dv, bv, uo);
 }
 void launch_pres_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* u,
-                            const float* pr, const float* Dv, float* Dp, float* bp) {
-    WF_LAUNCH(k_pres_precompute, B, fl, u, pr, Dv, Dp, bp);
+                            const float* pr, const float* Dv, const float* iD, float* Dp, float* bp) {
+    WF_LAUNCH(k_pres_precompute, B, fl, u, pr, Dv, iD, Dp, bp);
 }
 void launch_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pin, const float* Dv,
                        const float* Dp, const float* bp, float* pout) {
@@ -895,8 +924,8 @@ void launch_normalize(const Params& P, cudaStream_t st, const uint8_t* fl, float
     WF_LAUNCH(k_norm_apply, fl, ref, pr);
 }
 void launch_apply_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
-                      float* uc, float* u) {
-    WF_LAUNCH(k_apply_vel, fl, pc, Dv, uc, u);
+                      const float* iD, float* uc, float* u) {
+    WF_LAUNCH(k_apply_vel, fl, pc, Dv, iD, uc, u);
 }
 void launch_piso_aodu(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uc, const float* uT,
                       const float* eddy, const float* face, float* aodu) {
@@ -907,8 +936,11 @@ void launch_piso_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl,
     WF_LAUNCH(k_piso_pres_sweep, fl, pin, Dv, aodu, pout);
 }
 void launch_piso_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
-                     const float* aodu, float* uc, float* u) {
-    WF_LAUNCH(k_piso_vel, fl, pc, Dv, aodu, uc, u);
+                     const float* iD, const float* aodu, float* uc, float* u) {
+    WF_LAUNCH(k_piso_vel, fl, pc, Dv, iD, aodu, uc, u);
+}
+void launch_nbmask(const Params& P, cudaStream_t st, const uint8_t* fl, uint8_t* nbm) {
+    WF_LAUNCH(k_nbmask, fl, nbm);
 }
 void launch_vel_residual(const Params& P, cudaStream_t st, const float* Dv, const float* u, const float* uI,
                          double* part, double* out) {

@@ -18,6 +18,7 @@ struct wf_solver {
 
     // ---- device fields (see wf_common.cuh for the layout) ----
     uint8_t* fl = nullptr;
+    uint8_t* nbm = nullptr;   // neighbour masks (Params::nbm)
     // Three velocity buffers rotated by role like the reference's
     // velField / velFieldLastTime / velFieldLastIter textures.  When
     // iter_alias is set, velFieldLastIter is logically equal to
@@ -46,6 +47,11 @@ struct wf_solver {
     float* pcoef = nullptr;   // pressure: c_E, c_N, c_U, 1/Dp, PISO rhs (5 planes)
     float* vcoef = nullptr;   // momentum: A_E..A_D, 1/D (9 planes)
     float* grad = nullptr;    // cell-centre velocity gradient tensors (9 planes)
+    // generation of DField (bumped by every write) and the generation the
+    // cached pressure face coefficients c_E, c_N, c_U were built from: the
+    // three pressure solves of a step share D, so they share the coefficients
+    long long d_gen = 1, c3_gen = 0;
+    long long id_gen = 0;     // generation of D the cached 1/D (vcoef + 6N) belongs to
     // scratch
     double* part = nullptr;
     double* dsum = nullptr;   // 4 doubles

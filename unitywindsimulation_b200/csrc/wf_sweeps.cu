@@ -51,6 +51,25 @@ __device__ __forceinline__ float vis_face(const Params& P, const uint8_t* fl, co
     return v;
 }
 
+// vis_face from the neighbour mask (same values).
+__device__ __forceinline__ float vis_face_m(const Params& P, unsigned m, const float* eddy, const float* face, int x,
+                                            int y, int z, int i, int f) {
+    if (!P.les) return P.nu;
+    const float eP = ld(eddy, i);
+    float v = P.nu + eP;
+    if (face_in(P, x, y, z, f)) {
+        const int q = i + face_off(P, f);
+        if (nb_fluid(m, f)) v = P.nu + 0.5f * (eP + ld(eddy, q));
+        else v = P.nu + face_read(P, face, face_sign(f) > 0 ? q : i, face_axis(f));
+    } else if (f == 3 && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE) {
+        v = P.nu + face_read(P, face, i, 1);
+    }
+    return v;
+}
+__device__ __forceinline__ float inv_d(const float* iD, const float* Dv, size_t N, int a, int i) {
+    return iD ? ld(iD, a * N + i) : 1.f / ld(Dv, a * N + i);
+}
+
 // Momentum coefficients.  A: 6 planes (faces E,W,N,S,U,D), iD: 3 planes.
 __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                            const float* __restrict__ uT, const float* __restrict__ eddy,
@@ -60,9 +79,11 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     if (x >= P.nx || y >= P.ny || z >= P.nz) return;
+    (void)fl;
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
-    if (!fluid_at(fl, i)) {
+    const unsigned m = __ldg(P.nbm + i);
+    if (!(m & 64u)) {
 #pragma unroll
         for (int f = 0; f < 6; ++f) A[f * N + i] = 0.f;
 #pragma unroll
@@ -72,16 +93,13 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f);
-        const int X = x + face_ox(f), Y = y + face_oy(f), Z = z + face_oz(f);
         float c = 0.f;
-        if (in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            if (fluid_at(fl, q)) {
-                const float conv = P.ds * 0.25f * (ld(uT, a * N + i) + ld(uT, a * N + q));
-                const float vis = vis_face(P, fl, eddy, face, x, y, z, i, f);
-                const float dif = vis * P.ds / P.dx;
-                c = face_sign(f) > 0 ? dif - conv : dif + conv;
-            }
+        if (nb_fluid(m, f)) {
+            const int q = i + face_off(P, f);
+            const float conv = P.ds * 0.25f * (ld(uT, a * N + i) + ld(uT, a * N + q));
+            const float vis = vis_face_m(P, m, eddy, face, x, y, z, i, f);
+            const float dif = vis * P.ds / P.dx;
+            c = face_sign(f) > 0 ? dif - conv : dif + conv;
         }
         A[f * N + i] = c;
     }
@@ -194,25 +212,24 @@ __global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Para
 // Pressure face coefficients c_E, c_N, c_U (FvmColl.compute:2813-2814 form
 // ((dv/den) * DInv) / dx) for fluid-fluid faces, else 0.
 __global__ void k_pres_coef(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
-                            const float* __restrict__ Dv, float* __restrict__ c3) {
+                            const float* __restrict__ Dv, const float* __restrict__ iDc, float* __restrict__ c3) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     if (x >= P.nx || y >= P.ny || z >= P.nz) return;
+    (void)fl;
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
-    const bool me = fluid_at(fl, i);
+    const unsigned m = __ldg(P.nbm + i);
+    const bool me = (m & 64u) != 0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const int f = 2 * a;  // E, N, U
-        const int X = x + face_ox(f), Y = y + face_oy(f), Z = z + face_oz(f);
         float c = 0.f;
-        if (me && in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            if (fluid_at(fl, q)) {
-                const float DInv = 0.5f * (1.f / ld(Dv, a * N + i) + 1.f / ld(Dv, a * N + q));
-                c = (P.dv / P.den) * DInv / P.dx;
-            }
+        if (me && nb_fluid(m, f)) {
+            const int q = i + face_off(P, f);
+            const float DInv = 0.5f * (inv_d(iDc, Dv, N, a, i) + inv_d(iDc, Dv, N, a, q));
+            c = (P.dv / P.den) * DInv / P.dx;
         }
         c3[a * N + i] = c;
     }
@@ -229,15 +246,17 @@ __global__ void k_inv(const __grid_constant__ Params P, const uint8_t* __restric
 // PISO diagonal and right-hand side (PisoColl.compute:196-255, the parts of
 // the sweep that do not involve p''): ainv = 1/presCoeff, rhs = velTerm.
 __global__ void k_piso_pre(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
-                           const float* __restrict__ Dv, const float* __restrict__ aodu,
-                           float* __restrict__ ainv, float* __restrict__ rhs) {
+                           const float* __restrict__ Dv, const float* __restrict__ iDc,
+                           const float* __restrict__ aodu, float* __restrict__ ainv, float* __restrict__ rhs) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     if (x >= P.nx || y >= P.ny || z >= P.nz) return;
+    (void)fl;
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
-    if (!fluid_at(fl, i)) {
+    const unsigned m = __ldg(P.nbm + i);
+    if (!(m & 64u)) {
         ainv[i] = 0.f;
         rhs[i] = 0.f;
         return;
@@ -247,17 +266,16 @@ __global__ void k_piso_pre(const __grid_constant__ Params P, const uint8_t* __re
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f);
-        const int X = x + face_ox(f), Y = y + face_oy(f), Z = z + face_oz(f);
-        if (!in_region(P, X, Y, Z)) {
+        if (!face_in(P, x, y, z, f)) {
             if (consistent && P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE) {
-                const float DInv = 1.f / ld(Dv, a * N + i);
+                const float DInv = inv_d(iDc, Dv, N, a, i);
                 coeff -= 2.f * (P.dv / P.den) * DInv / P.dx;
             }
             continue;
         }
-        const int q = cidx(P, X, Y, Z);
-        if (!fluid_at(fl, q)) continue;
-        const float AdInv = 0.5f * (1.f / ld(Dv, a * N + i) + 1.f / ld(Dv, a * N + q));
+        if (!nb_fluid(m, f)) continue;
+        const int q = i + face_off(P, f);
+        const float AdInv = 0.5f * (inv_d(iDc, Dv, N, a, i) + inv_d(iDc, Dv, N, a, q));
         const float Aod = 0.5f * (ld(aodu, a * N + i) + ld(aodu, a * N + q));
         if (a == 0) coeff -= (P.dv / P.den) * (AdInv / P.dx);
         else coeff -= (P.dv / P.den) * AdInv / P.dx;
@@ -646,6 +664,7 @@ void vel_coef(wf_solver* h) {
     WF_COUNT_LAUNCH();
     k_vel_coef<<<grd(P), blk(), 0, h->st>>>(P, h->fl, h->vb[h->iT], h->eddy, h->face, h->Dv, h->vcoef,
                                             h->vcoef + 6 * N);
+    h->id_gen = h->d_gen;  // vcoef + 6N now holds 1/D of the current D
 }
 
 void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
@@ -669,11 +688,15 @@ const float* pres_coef(wf_solver* h, bool piso) {
     float* c3 = h->pcoef;
     float* ainv = h->pcoef + 3 * N;
     float* rhs = piso ? h->pcoef + 4 * N : h->bp;
-    WF_COUNT_LAUNCH();
-    k_pres_coef<<<grd(P), blk(), 0, h->st>>>(P, h->fl, h->Dv, c3);
+    const float* iDc = h->id_gen == h->d_gen ? h->vcoef + 6 * N : nullptr;
+    if (h->c3_gen != h->d_gen) {  // c_E, c_N, c_U depend on D only
+        WF_COUNT_LAUNCH();
+        k_pres_coef<<<grd(P), blk(), 0, h->st>>>(P, h->fl, h->Dv, iDc, c3);
+        h->c3_gen = h->d_gen;
+    }
     WF_COUNT_LAUNCH();
     if (piso) {
-        k_piso_pre<<<grd(P), blk(), 0, h->st>>>(P, h->fl, h->Dv, h->aodu, ainv, rhs);
+        k_piso_pre<<<grd(P), blk(), 0, h->st>>>(P, h->fl, h->Dv, iDc, h->aodu, ainv, rhs);
     } else {
         k_inv<<<(P.N + 255) / 256, 256, 0, h->st>>>(P, h->fl, h->Dp, ainv);
     }
@@ -975,18 +998,19 @@ void launch_vel_sweep1_ptr(const Params& P, cudaStream_t st, const float* A, con
     WF_COUNT_LAUNCH();
     k_vel_sweep1<true><<<grd(P), blk(), 0, st>>>(P, A, iD, bv, ui, uo);
 }
-void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, float* c3) {
+void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* iD,
+                          float* c3) {
     WF_COUNT_LAUNCH();
-    k_pres_coef<<<grd(P), blk(), 0, st>>>(P, fl, Dv, c3);
+    k_pres_coef<<<grd(P), blk(), 0, st>>>(P, fl, Dv, iD, c3);
 }
 void launch_inv_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dp, float* ainv) {
     WF_COUNT_LAUNCH();
     k_inv<<<(P.N + 255) / 256, 256, 0, st>>>(P, fl, Dp, ainv);
 }
-void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* aodu,
-                         float* ainv, float* rhs) {
+void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* iD,
+                         const float* aodu, float* ainv, float* rhs) {
     WF_COUNT_LAUNCH();
-    k_piso_pre<<<grd(P), blk(), 0, st>>>(P, fl, Dv, aodu, ainv, rhs);
+    k_piso_pre<<<grd(P), blk(), 0, st>>>(P, fl, Dv, iD, aodu, ainv, rhs);
 }
 
 }  // namespace wf

@@ -27,10 +27,11 @@ void launch_vel_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, co
                          const float* face, const float* Dv, float* A, float* iD);
 void launch_vel_sweep1_ptr(const Params& P, cudaStream_t st, const float* A, const float* iD, const float* bv,
                            const float* ui, float* uo);
-void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, float* c3);
+void launch_pres_coef_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* iD,
+                          float* c3);
 void launch_inv_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dp, float* ainv);
-void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* aodu,
-                         float* ainv, float* rhs);
+void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, const float* Dv, const float* iD,
+                         const float* aodu, float* ainv, float* rhs);
 
 // n pressure-type sweeps po = ainv (rhs - C pi) (rhs == nullptr: 0) by the
 // multi-sweep kernel, every iterate kept: slot k of `stack` (stride N floats)
