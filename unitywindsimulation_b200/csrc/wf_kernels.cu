@@ -147,6 +147,39 @@ __device__ __forceinline__ void cell_grad(const Params& P, const Bnd& B, const u
         for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) / P.dx;
 }
 
+// face_vel / cell_grad from the neighbour mask (same values).
+__device__ __forceinline__ void face_vel_m(const Params& P, const Bnd& B, unsigned m, const float* uT, const Cell& c,
+                                           int f, float r[3]) {
+    r[0] = r[1] = r[2] = 0.f;
+    if (face_in(P, c.x, c.y, c.z, f)) {
+        if (nb_fluid(m, f)) {
+            const int q = c.i + face_off(P, f);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[k] = 0.5f * (ld(uT, (size_t)k * P.N + c.i) + ld(uT, (size_t)k * P.N + q));
+        }
+    } else {
+        const int bc = face_bc(f), bt = P.vbc[bc];
+        if (bt == WF_BND_FIXED_VALUE) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[k] = bnd_comp(P, B, bc, c.x, c.y, c.z, k);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[k] = ld(uT, (size_t)k * P.N + c.i);
+            if (bt == WF_BND_SYMMETRY) r[face_axis(f)] = 0.f;
+        }
+    }
+}
+__device__ __forceinline__ void cell_grad_m(const Params& P, const Bnd& B, unsigned m, const float* uT, const Cell& c,
+                                            float g[3][3]) {
+    float fv[6][3];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) face_vel_m(P, B, m, uT, c, f, fv[f]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) / P.dx;
+}
+
 // ------------------------------------------------------------ wall function
 // CSCalLogLawWallFunc, WallFunc.compute:128-190.  Writes the W/S/D face
 // slots of every cell.
@@ -184,9 +217,11 @@ __global__ void k_eddy_vis(const __grid_constant__ Params P, const Bnd B, const 
                            const float* __restrict__ uT, float* __restrict__ eddy, float* __restrict__ grad) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    if (!fluid_at(fl, c.i)) return;
+    const unsigned m = __ldg(P.nbm + c.i);
+    if (!(m & 64u)) return;
+    (void)fl;
     float g[3][3];
-    cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
+    cell_grad_m(P, B, m, uT, c, g);
     if (grad) {
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -228,7 +263,8 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
                            float* __restrict__ bles) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    if (!fluid_at(fl, c.i)) return;
+    const unsigned m = __ldg(P.nbm + c.i);
+    if (!(m & 64u)) return;
     const size_t N = P.N;
     float g[3][3];
     if (grad) {
@@ -245,9 +281,9 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
         fg[f][0] = fg[f][1] = fg[f][2] = 0.f;
         const int a = face_axis(f);
         const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
-        if (in_region(P, X, Y, Z)) {
-            const int q = cidx(P, X, Y, Z);
-            if (fluid_at(fl, q)) {
+        if (face_in(P, c.x, c.y, c.z, f)) {
+            const int q = c.i + face_off(P, f);
+            if (nb_fluid(m, f)) {
                 if (grad) {
 #pragma unroll
                     for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + ld(grad, (size_t)(3 * a + j) * N + q));
@@ -276,7 +312,7 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
     }
     float vis[6];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) vis[f] = vis_face(P, fl, eddy, face, c, f);
+    for (int f = 0; f < 6; ++f) vis[f] = vis_face_m(P, m, eddy, face, c, f);
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         const float t = vis[0] * fg[0][j] - vis[1] * fg[1][j] + vis[2] * fg[2][j] - vis[3] * fg[3][j] +
