@@ -346,20 +346,29 @@ def run_windfvm(args):
         stream = torch.cuda.ExternalStream(solver.stream_ptr)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        # one untimed iteration: first use of the readback path allocates
+        # its snapshot buffer and copy stream
+        solver.set_inflow_plane(h_in.numpy())
+        solver.Step(1)
+        solver.readback_begin(h_vel.numpy(), h_pres.numpy())
+        solver.readback_wait()
         barrier()
         e0.record(stream)
         for _ in range(args.steps):
             solver.set_inflow_plane(h_in.numpy())
             solver.Step(1)
-            solver.GetVelField(out=h_vel.numpy())
-            solver.GetPresField(out=h_pres.numpy())
+            # the previous step's fields reached the host while this step ran
+            solver.readback_wait()
+            solver.readback_begin(h_vel.numpy(), h_pres.numpy())
+        solver.readback_wait()
         e1.record(stream)
         e1.synchronize()
         barrier()
         e_ms = max_over_ranks(e0.elapsed_time(e1))
         e2e = {"value": world * N * args.steps / (e_ms / 1e3) / 1e6, "unit": METRIC,
                "h2d_bytes_per_step": int(inlet.size * 4), "d2h_bytes_per_step": int(4 * N * 4),
-               "api": "set_inflow_plane + Step + GetVelField + GetPresField, pinned host buffers"}
+               "api": "set_inflow_plane + Step + readback_begin/readback_wait of velocity and pressure "
+                      "(every step's fields copied to pinned host buffers, overlapping the next step)"}
 
     # ---- roofline of the dominant kernel (pressure Jacobi sweep) ----
     peak, peak_kind = measured_peaks()

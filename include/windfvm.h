@@ -192,6 +192,19 @@ int wf_get_flags(wf_solver* h, int32_t* out);
 /* Velocity, pressure and step counter for an exact resume. vel: 3N floats
  * (SoA), pres: N floats. */
 int wf_get_state(wf_solver* h, float* vel, float* pres, int64_t* step);
+
+/* Asynchronous readback of the current velocity and pressure, for hosts that
+ * read the fields every step (no counterpart on IFvmSolver; the reference's
+ * exporter reads back the same way with AsyncGPUReadback,
+ * NcFlowFieldExporter.cs:300-340).  wf_readback_begin snapshots the fields
+ * on the solver's stream and copies them to the host buffers (vel in the
+ * given layout, 3N or 4N floats; pres N floats) on a separate stream, so the
+ * copy overlaps the following wf_step calls.  The buffers are complete after
+ * wf_readback_wait; a second begin waits for the first.  Use page-locked host
+ * memory (cudaHostAlloc, or torch pin_memory) for the copies to run
+ * asynchronously. */
+int wf_readback_begin(wf_solver* h, float* vel, float* pres, int layout);
+int wf_readback_wait(wf_solver* h);
 int wf_set_state(wf_solver* h, const float* vel, const float* pres, int64_t step);
 
 /* Named fields of the reference's field set (MallocTextures,

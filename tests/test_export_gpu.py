@@ -69,3 +69,26 @@ def test_export_bad_path(built, tmp_path):
         FieldExporter(g, tmp_path / "missing_dir" / "x.nc")
     assert e.value.status == _lib.WF_ERR_IO
     g.close()
+
+
+@pytest.mark.parametrize("layout", [_lib.LAYOUT_SOA, _lib.LAYOUT_XYZW])
+def test_async_readback_overlaps_next_step(built, layout):
+    """readback_begin snapshots the state it is called on: a step launched
+    before readback_wait does not change what arrives on the host."""
+    case, g = _solver(5)
+    n = g.n_cells
+    per = 4 if layout == _lib.LAYOUT_XYZW else 3
+    vel = np.empty(per * n, np.float32)
+    pres = np.empty(n, np.float32)
+    g.Step(2)
+    want_v = g.GetVelField(layout=layout).reshape(-1).copy()
+    want_p = g.GetPresField().reshape(-1).copy()
+    g.readback_begin(vel, pres, layout)
+    g.Step(1)
+    g.readback_wait()
+    np.testing.assert_array_equal(vel, want_v)
+    np.testing.assert_array_equal(pres, want_p)
+    g.readback_begin(vel, pres, layout)
+    g.readback_wait()
+    np.testing.assert_array_equal(vel, g.GetVelField(layout=layout).reshape(-1))
+    g.close()

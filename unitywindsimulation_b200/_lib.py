@@ -140,6 +140,8 @@ _SIGNATURES = {
     "wf_get_pres": (c_int, [c_void_p, POINTER(c_float)]),
     "wf_get_flags": (c_int, [c_void_p, POINTER(c_int32)]),
     "wf_get_state": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), POINTER(c_int64)]),
+    "wf_readback_begin": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "wf_readback_wait": (c_int, [c_void_p]),
     "wf_set_state": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), c_int64]),
     "wf_field_size": (c_int, [c_void_p, c_int, POINTER(c_size_t), POINTER(c_int)]),
     "wf_get_field": (c_int, [c_void_p, c_int, POINTER(c_float)]),

@@ -118,6 +118,13 @@ void free_all(wf_solver* h) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->hsum) cudaFreeHost(h->hsum);
+    if (h->cst) {
+        cudaStreamSynchronize(h->cst);
+        cudaStreamDestroy(h->cst);
+    }
+    if (h->ev_snap) cudaEventDestroy(h->ev_snap);
+    if (h->ev_done) cudaEventDestroy(h->ev_done);
+    if (h->snap) cudaFree(h->snap);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->st) cudaStreamDestroy(h->st);
@@ -723,6 +730,47 @@ int wf_get_vel(wf_solver* h, float* out, int layout) {
     const size_t per = layout == WF_LAYOUT_XYZW ? 4 : 3;
     WF_CUDA(cudaMemcpyAsync(out, h->stage, per * N * sizeof(float), cudaMemcpyDeviceToHost, h->st));
     return sync(h);
+}
+
+int wf_readback_wait(wf_solver* h) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!h->rb_pending) return WF_OK;
+    WF_CUDA(cudaSetDevice(h->device));
+    h->rb_pending = false;
+    WF_CUDA(cudaEventSynchronize(h->ev_done));
+    return WF_OK;
+}
+
+int wf_readback_begin(wf_solver* h, float* vel, float* pres, int layout) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!vel || !pres || layout < 0 || layout > 2) return set_err(h, WF_ERR_INVALID_ARG, "bad output or layout");
+    WF_CUDA(cudaSetDevice(h->device));
+    WF_TRY(wf_readback_wait(h));
+    const size_t N = h->P.N;
+    if (!h->snap) {
+        WF_TRY(alloc(h, (void**)&h->snap, 5 * sizeof(float) * N));
+        WF_CUDA(cudaStreamCreateWithFlags(&h->cst, cudaStreamNonBlocking));
+        WF_CUDA(cudaEventCreateWithFlags(&h->ev_snap, cudaEventDisableTiming));
+        WF_CUDA(cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming));
+    }
+    // snapshot on the solver stream (ordered after the last step, before the
+    // next one), then the copies to the host on the copy stream
+    const size_t per = layout == WF_LAYOUT_XYZW ? 4 : 3;
+    if (layout == WF_LAYOUT_SOA) {
+        WF_CUDA(cudaMemcpyAsync(h->snap, h->vb[h->iT], 3 * sizeof(float) * N, cudaMemcpyDeviceToDevice, h->st));
+    } else {
+        wf::launch_soa_to_interleaved(h->st, h->vb[h->iT], (int)N, h->snap, layout == WF_LAYOUT_XYZW);
+        WF_CHECK_LAUNCH();
+    }
+    float* psnap = h->snap + 4 * N;
+    WF_CUDA(cudaMemcpyAsync(psnap, h->pr, sizeof(float) * N, cudaMemcpyDeviceToDevice, h->st));
+    WF_CUDA(cudaEventRecord(h->ev_snap, h->st));
+    WF_CUDA(cudaStreamWaitEvent(h->cst, h->ev_snap, 0));
+    WF_CUDA(cudaMemcpyAsync(vel, h->snap, per * sizeof(float) * N, cudaMemcpyDeviceToHost, h->cst));
+    WF_CUDA(cudaMemcpyAsync(pres, psnap, sizeof(float) * N, cudaMemcpyDeviceToHost, h->cst));
+    WF_CUDA(cudaEventRecord(h->ev_done, h->cst));
+    h->rb_pending = true;
+    return WF_OK;
 }
 
 int wf_get_pres(wf_solver* h, float* out) {

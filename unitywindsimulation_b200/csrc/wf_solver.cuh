@@ -58,6 +58,11 @@ struct wf_solver {
     float* dref = nullptr;
     int* dbad = nullptr;
     void* stage = nullptr;    // 4N floats of device staging for host I/O
+    // asynchronous readback: snapshot (4N + N floats), copy stream, events
+    float* snap = nullptr;
+    cudaStream_t cst = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_done = nullptr;
+    bool rb_pending = false;
     double* hsum = nullptr;   // pinned
 
     float wind = 0.f;

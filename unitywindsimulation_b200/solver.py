@@ -120,6 +120,21 @@ class FvmSolverCuda:
             return out.reshape((3,) + self.shape)
         return out.reshape(self.shape + (per,))
 
+    def readback_begin(self, vel_out: np.ndarray, pres_out: np.ndarray, layout: int = _lib.LAYOUT_SOA) -> None:
+        """Starts an asynchronous copy of the current velocity (layout SOA:
+        3N floats, XYZW: 4N, XYZ: 3N) and pressure (N) into the given host
+        arrays (page-locked memory for a truly asynchronous copy); they are
+        complete after readback_wait().  Keep the arrays alive until then."""
+        n = self.n_cells
+        per = {_lib.LAYOUT_SOA: 3, _lib.LAYOUT_XYZW: 4, _lib.LAYOUT_XYZ: 3}[layout]
+        for a, size in ((vel_out, per * n), (pres_out, n)):
+            if a.dtype != np.float32 or a.size != size or not a.flags.c_contiguous:
+                raise ValueError("readback buffers must be contiguous float32 arrays of the field sizes")
+        self._check(self._lib.wf_readback_begin(self._h, vel_out.ctypes.data, pres_out.ctypes.data, int(layout)))
+
+    def readback_wait(self) -> None:
+        self._check(self._lib.wf_readback_wait(self._h))
+
     def GetPresField(self, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
             out = np.empty(self.n_cells, dtype=np.float32)
