@@ -183,7 +183,9 @@ enum { WF_LAYOUT_SOA = 0,   /* 3 planes of N floats: [c][z][y][x]           */
        WF_LAYOUT_XYZW = 1,  /* N float4 (x,y,z,0), the RenderTexture layout */
        WF_LAYOUT_XYZ = 2 }; /* N float3 interleaved                         */
 
-/* Current velocity (velFieldLastTime after a step). */
+/* Current velocity (velFieldLastTime after a step).  GetVelField (:1568-1571)
+ * returns velFieldTex, which after the end-of-step swap (:1105) holds the
+ * previous time level; wf_get_field(WF_FIELD_VEL) returns that texture. */
 int wf_get_vel(wf_solver* h, float* out, int layout);
 /* Current pressure (presFieldLastTime). N floats. */
 int wf_get_pres(wf_solver* h, float* out);

@@ -167,3 +167,163 @@ class OracleSolver:
         m = c_double(0)
         self._ok(self._lib.wfo_mass_imbalance(self._h, byref(m)))
         return m.value
+
+
+# ---- the reference's own kernels (oracle/ref_driver.cpp) --------------------
+
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libwindfvm_ref.so")
+_ref_lib = None
+
+
+def ref_available() -> bool:
+    """True when the reference-kernel library has been built into _ref/."""
+    return os.path.exists(REF_LIB_PATH)
+
+
+def build_ref(reference_root: str) -> str:
+    """Translates the reference's shaders found under `reference_root` and
+    builds _ref/libwindfvm_ref.so (make ref)."""
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_ROOT={reference_root}"], check=True)
+    return REF_LIB_PATH
+
+
+def load_ref():
+    global _ref_lib
+    if _ref_lib is not None:
+        return _ref_lib
+    if not ref_available():
+        raise FileNotFoundError(f"{REF_LIB_PATH} is not built (make -C oracle ref)")
+    lib = ctypes.CDLL(REF_LIB_PATH)
+    sig = {
+        "wfr_create": (c_int, [POINTER(WfConfig), POINTER(c_void_p)]),
+        "wfr_create_empty": (c_int, [POINTER(WfConfig), POINTER(c_void_p)]),
+        "wfr_destroy": (c_int, [c_void_p]),
+        "wfr_set_flags": (c_int, [c_void_p, POINTER(c_int32), c_size_t]),
+        "wfr_set_field": (c_int, [c_void_p, c_int, POINTER(c_float)]),
+        "wfr_get_field": (c_int, [c_void_p, c_int, POINTER(c_float)]),
+        "wfr_step": (c_int, [c_void_p, c_int]),
+        "wfr_get_flags": (c_int, [c_void_p, POINTER(c_int32)]),
+        "wfr_init_flags": (c_int, [c_void_p, POINTER(c_int32), c_size_t]),
+        "wfr_init_vel_pres_fields": (c_int, [c_void_p, c_float]),
+        "wfr_set_fixed_value_vel_bnd_cond": (c_int, [c_void_p, c_float]),
+        "wfr_init_from_background": (c_int, [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float), c_float]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _ref_lib = lib
+    return lib
+
+
+# Fields a step reads before writing them (everything else is rebuilt inside
+# the step): the three velocity textures, pressure, the pressure-correction
+# pair, face eddy viscosity and the six boundary planes.
+REF_STATE_FIELDS = (0, 1, 2, 4, 5, 6, 13, 14, 15, 16, 17, 18, 19)
+
+
+class RefSolver:
+    """FvmSolverGpu replayed with the reference's own kernels on the CPU
+    (FP32): the constructor's set-up, InitFlags, InitVelPresFields,
+    SetFixedValueVelBndCond, InitVelPresFieldsFromBackGroundFlow and Step.
+    copy_state_from takes another solver's state instead, to compare single
+    steps from identical inputs."""
+
+    def __init__(self, cfg: WfConfig, construct: bool = True):
+        """construct=False skips the constructor's set-up (every field zero),
+        for a state taken from another solver with copy_state_from."""
+        self._lib = load_ref()
+        self.cfg = cfg.copy()
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        self.n_cells = cfg.nx * cfg.ny * cfg.nz
+        h = c_void_p()
+        create = self._lib.wfr_create if construct else self._lib.wfr_create_empty
+        st = create(byref(self.cfg), byref(h))
+        if st != 0:
+            raise RuntimeError(f"wfr_create failed with status {st}")
+        self._h = h
+        self.wind_speed = cfg.wind_speed
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.wfr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, st):
+        if st != 0:
+            raise RuntimeError(f"reference-kernel call failed with status {st}")
+
+    def _points(self, field):
+        c = self.cfg
+        if field in (14, 15):
+            return c.ny * c.nz
+        if field in (16, 17):
+            return c.nx * c.nz
+        if field in (18, 19):
+            return c.nx * c.ny
+        return self.n_cells
+
+    def _comps(self, field):
+        return 1 if field in (4, 5, 6, 9, 10, 12) else 3
+
+    def set_flags(self, flags):
+        f = np.ascontiguousarray(np.asarray(flags, dtype=np.int32).reshape(-1))
+        self._ok(self._lib.wfr_set_flags(self._h, f.ctypes.data_as(POINTER(c_int32)), f.size))
+
+    def InitFlags(self, flags):
+        f = np.ascontiguousarray(np.asarray(flags, dtype=np.int32).reshape(-1))
+        self._ok(self._lib.wfr_init_flags(self._h, f.ctypes.data_as(POINTER(c_int32)), f.size))
+
+    def GetFlagField(self):
+        out = np.empty(self.n_cells, dtype=np.int32)
+        self._ok(self._lib.wfr_get_flags(self._h, out.ctypes.data_as(POINTER(c_int32))))
+        return out.reshape(self.shape)
+
+    def InitVelPresFields(self):
+        self._ok(self._lib.wfr_init_vel_pres_fields(self._h, c_float(self.wind_speed)))
+
+    def SetFixedValueVelBndCond(self, wind_speed=None):
+        if wind_speed is not None:
+            self.wind_speed = float(wind_speed)
+        self._ok(self._lib.wfr_set_fixed_value_vel_bnd_cond(self._h, c_float(self.wind_speed)))
+
+    def InitVelPresFieldsFromBackGroundFlow(self, background, pos=(0.0, 0.0, 0.0), pos_background=(0.0, 0.0, 0.0),
+                                            rot_deg=0.0):
+        p = (c_float * 3)(*[float(v) for v in pos])
+        q = (c_float * 3)(*[float(v) for v in pos_background])
+        self._ok(self._lib.wfr_init_from_background(self._h, background._h, p, q, float(rot_deg)))
+
+    def set_field(self, field, data):
+        a = np.ascontiguousarray(data, dtype=np.float32).reshape(-1)
+        if a.size != self._points(field) * self._comps(field):
+            raise ValueError(f"field {field}: {a.size} values")
+        self._ok(self._lib.wfr_set_field(self._h, int(field), a.ctypes.data_as(POINTER(c_float))))
+
+    def get_field(self, field) -> np.ndarray:
+        pts, comps = self._points(field), self._comps(field)
+        out = np.empty(pts * comps, dtype=np.float32)
+        self._ok(self._lib.wfr_get_field(self._h, int(field), out.ctypes.data_as(POINTER(c_float))))
+        return out.reshape((comps, pts)) if comps > 1 else out
+
+    def copy_state_from(self, other):
+        """Takes flags and every field a step reads from `other` (an
+        OracleSolver, or anything with get_field and GetFlagField)."""
+        self.set_flags(np.asarray(other.GetFlagField()).reshape(-1))
+        for f in REF_STATE_FIELDS:
+            self.set_field(f, np.asarray(other.get_field(f), dtype=np.float32))
+
+    def Step(self, n_steps: int = 1) -> bool:
+        self._ok(self._lib.wfr_step(self._h, int(n_steps)))
+        return True
+
+    def GetVelField(self):
+        return self.get_field(1).reshape((3,) + self.shape)
+
+    def GetPresField(self):
+        return self.get_field(4).reshape(self.shape)

@@ -7,12 +7,16 @@
  * (include/windfvm.h): only the tests, the smoke check and the CPU-baseline
  * leg of the benchmark load it.  The product path never calls it.
  *
- * Parity status: the reference ships no tests, fixtures or golden vectors for
- * this path and its own code (C# + HLSL through Unity/D3D) cannot run here, so
- * this oracle is "parity unpinned" against the reference itself; it is pinned
- * by known-answer tests (quiescent box, free-stream preservation, closed-form
- * wall function, linear-shear Smagorinsky, adjoint-stencil symmetry) and by the
- * agreement of its FP32 and FP64 instances.
+ * Parity status: pinned on the reference's own kernels.  The reference ships
+ * no tests or golden vectors for this path and its host (C# under Unity, D3D
+ * dispatch) cannot run here, but its compute shaders compile as C++ through
+ * oracle/hlsl_shim.h (oracle/ref_kernels.py, oracle/ref_driver.cpp).  The FP32
+ * instance of this oracle is bit-identical to them on every field of every
+ * step tested (tests/test_ref_pin.py, tests/golden/ref_kernels.npz).  It is
+ * also checked by known-answer tests (quiescent box, free-stream
+ * preservation, closed-form wall function, linear-shear Smagorinsky,
+ * adjoint-stencil symmetry) and by the agreement of its FP32 and FP64
+ * instances.
  *
  * Every wfo_* entry mirrors the wf_* entry of the same name in windfvm.h and
  * uses the same wf_config, field ids and layouts.
