@@ -69,6 +69,12 @@ __device__ __forceinline__ bool face_in(const Params& P, int x, int y, int z, in
     return f == 0 ? x + 1 < P.nx : f == 1 ? x > 0 : f == 2 ? y + 1 < P.ny : f == 3 ? y > 0 : f == 4 ? z + 1 < P.nz : z > 0;
 }
 __device__ __forceinline__ bool nb_fluid(unsigned mask, int f) { return (mask >> f) & 1u; }
+// Index of the neighbour across face f, or of the cell itself where that
+// neighbour is outside the domain: always a valid index, so a kernel can load
+// from every face before it knows which faces count.
+__device__ __forceinline__ int nb_idx(const Params& P, int x, int y, int z, int i, int f) {
+    return face_in(P, x, y, z, f) ? i + face_off(P, f) : i;
+}
 __device__ __forceinline__ int plane_idx(const Params& P, int bc, int x, int y, int z) {
     return bc <= WF_FACE_XN ? z * P.ny + y : (bc <= WF_FACE_YN ? z * P.nx + x : y * P.nx + x);
 }

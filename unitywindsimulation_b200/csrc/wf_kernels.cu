@@ -77,6 +77,23 @@ __device__ __forceinline__ float vis_face_m(const Params& P, unsigned m, const f
     }
     return v;
 }
+// vis_face_m with the eddy viscosities of the cell (eP) and of the neighbour
+// across f (eQ) already loaded.  Same values.
+__device__ __forceinline__ float vis_face_v(const Params& P, unsigned m, const float* face, const Cell& c, int f,
+                                            float eP, float eQ) {
+    if (!P.les) return P.nu;
+    float v = P.nu + eP;
+    if (face_in(P, c.x, c.y, c.z, f)) {
+        if (nb_fluid(m, f)) {
+            v = P.nu + 0.5f * (eP + eQ);
+        } else {
+            v = P.nu + face_read(P, face, face_sign(f) > 0 ? c.i + face_off(P, f) : c.i, face_axis(f));
+        }
+    } else if (f == 3 && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE) {
+        v = P.nu + face_read(P, face, c.i, 1);
+    }
+    return v;
+}
 // 1/D of component a at cell i: from the cached reciprocals when given
 // (computed with the same division), else divided here.
 __device__ __forceinline__ float inv_d(const float* iD, const float* Dv, size_t N, int a, int i) {
@@ -147,33 +164,31 @@ __device__ __forceinline__ void cell_grad(const Params& P, const Bnd& B, const u
         for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) / P.dx;
 }
 
-// face_vel / cell_grad from the neighbour mask (same values).
-__device__ __forceinline__ void face_vel_m(const Params& P, const Bnd& B, unsigned m, const float* uT, const Cell& c,
-                                           int f, float r[3]) {
-    r[0] = r[1] = r[2] = 0.f;
-    if (face_in(P, c.x, c.y, c.z, f)) {
-        if (nb_fluid(m, f)) {
-            const int q = c.i + face_off(P, f);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) r[k] = 0.5f * (ld(uT, (size_t)k * P.N + c.i) + ld(uT, (size_t)k * P.N + q));
-        }
-    } else {
-        const int bc = face_bc(f), bt = P.vbc[bc];
-        if (bt == WF_BND_FIXED_VALUE) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) r[k] = bnd_comp(P, B, bc, c.x, c.y, c.z, k);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) r[k] = ld(uT, (size_t)k * P.N + c.i);
-            if (bt == WF_BND_SYMMETRY) r[face_axis(f)] = 0.f;
-        }
-    }
-}
-__device__ __forceinline__ void cell_grad_m(const Params& P, const Bnd& B, unsigned m, const float* uT, const Cell& c,
-                                            float g[3][3]) {
+// cell_grad from the neighbour mask and loaded values: uP = own velocity,
+// uq[f] = velocity of the (clamped) neighbour across face f.  Same values.
+__device__ __forceinline__ void cell_grad_v(const Params& P, const Bnd& B, unsigned m, const Cell& c,
+                                            const float uP[3], const float uq[6][3], float g[3][3]) {
     float fv[6][3];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) face_vel_m(P, B, m, uT, c, f, fv[f]);
+    for (int f = 0; f < 6; ++f) {
+        fv[f][0] = fv[f][1] = fv[f][2] = 0.f;
+        if (face_in(P, c.x, c.y, c.z, f)) {
+            if (nb_fluid(m, f)) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) fv[f][k] = 0.5f * (uP[k] + uq[f][k]);
+            }
+        } else {
+            const int bc = face_bc(f), bt = P.vbc[bc];
+            if (bt == WF_BND_FIXED_VALUE) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) fv[f][k] = bnd_comp(P, B, bc, c.x, c.y, c.z, k);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) fv[f][k] = uP[k];
+                if (bt == WF_BND_SYMMETRY) fv[f][face_axis(f)] = 0.f;
+            }
+        }
+    }
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -217,11 +232,21 @@ __global__ void k_eddy_vis(const __grid_constant__ Params P, const Bnd B, const 
                            const float* __restrict__ uT, float* __restrict__ eddy, float* __restrict__ grad) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    const unsigned m = __ldg(P.nbm + c.i);
-    if (!(m & 64u)) return;
     (void)fl;
+    // Every load of the interior path before the fluid test.
+    const unsigned m = __ldg(P.nbm + c.i);
+    float uP[3], uq[6][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) uP[k] = ld(uT, (size_t)k * P.N + c.i);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int q = nb_idx(P, c.x, c.y, c.z, c.i, f);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) uq[f][k] = ld(uT, (size_t)k * P.N + q);
+    }
+    if (!(m & 64u)) return;
     float g[3][3];
-    cell_grad_m(P, B, m, uT, c, g);
+    cell_grad_v(P, B, m, c, uP, uq, g);
     if (grad) {
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -263,18 +288,31 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
                            float* __restrict__ bles) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    const unsigned m = __ldg(P.nbm + c.i);
-    if (!(m & 64u)) return;
     const size_t N = P.N;
-    float g[3][3];
+    // Every load of the interior path before the fluid test: the stored
+    // gradient tensor of the cell, row a of each (clamped) neighbour's tensor
+    // across an a-normal face, the velocity and the eddy viscosities.
+    const unsigned m = __ldg(P.nbm + c.i);
+    float g[3][3], gq[6][3], uP[3], eq[6];
     if (grad) {
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int j = 0; j < 3; ++j) g[i][j] = ld(grad, (size_t)(3 * i + j) * N + c.i);
-    } else {
-        cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
     }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int q = nb_idx(P, c.x, c.y, c.z, c.i, f);
+        const int a = face_axis(f);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) gq[f][j] = grad ? ld(grad, (size_t)(3 * a + j) * N + q) : 0.f;
+        eq[f] = P.les ? ld(eddy, q) : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) uP[k] = ld(uT, (size_t)k * N + c.i);
+    const float eP = P.les ? ld(eddy, c.i) : 0.f;
+    if (!(m & 64u)) return;
+    if (!grad) cell_grad(P, B, fl, uT, c.x, c.y, c.z, g);
     float fg[6][3];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -282,11 +320,10 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
         const int a = face_axis(f);
         const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
         if (face_in(P, c.x, c.y, c.z, f)) {
-            const int q = c.i + face_off(P, f);
             if (nb_fluid(m, f)) {
                 if (grad) {
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + ld(grad, (size_t)(3 * a + j) * N + q));
+                    for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + gq[f][j]);
                 } else {
                     float gn[3][3];
                     cell_grad(P, B, fl, uT, X, Y, Z, gn);
@@ -294,14 +331,14 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
                     for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + gn[a][j]);
                 }
             } else {
-                const float v = ld(uT, (size_t)a * N + c.i) / (0.5f * P.dx);
+                const float v = uP[a] / (0.5f * P.dx);
                 fg[f][a] = face_sign(f) > 0 ? -v : v;
             }
         } else {
             const int bc = face_bc(f), bt = P.vbc[bc];
             if (bt == WF_BND_FIXED_VALUE) {
                 const float b = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
-                const float u = ld(uT, (size_t)a * N + c.i);
+                const float u = uP[a];
                 fg[f][a] = face_sign(f) > 0 ? (b - u) / (0.5f * P.dx) : (u - b) / (0.5f * P.dx);
             } else {
 #pragma unroll
@@ -312,7 +349,7 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
     }
     float vis[6];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) vis[f] = vis_face_m(P, m, eddy, face, c, f);
+    for (int f = 0; f < 6; ++f) vis[f] = vis_face_v(P, m, face, c, f, eP, eq[f]);
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         const float t = vis[0] * fg[0][j] - vis[1] * fg[1][j] + vis[2] * fg[2][j] - vis[3] * fg[3][j] +
@@ -331,13 +368,28 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
                                  float* bv) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    const unsigned m = __ldg(P.nbm + c.i);
-    if (!(m & 64u)) return;
     (void)fl;
     const size_t N = P.N;
-    float uP[3];
+    // Every load of the interior path before the fluid test (boundary planes
+    // and wall-face viscosities stay where they are used).
+    const unsigned m = __ldg(P.nbm + c.i);
+    float uP[3], uq[6], pq[6], eq[6], bl[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) uP[k] = ld(uT, k * N + c.i);
+    const float pP = ld(pr, c.i);
+    const float eP = P.les ? ld(eddy, c.i) : 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int q = nb_idx(P, c.x, c.y, c.z, c.i, f);
+        uq[f] = ld(uT, face_axis(f) * N + q);
+        pq[f] = ld(pr, q);
+        eq[f] = P.les ? ld(eddy, q) : 0.f;
+    }
+    const bool add_les = P.les && bles;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) bl[k] = add_les ? bles[k * N + c.i] : 0.f;
+    const float dr = drag ? ld(drag, c.i) : 0.f;
+    if (!(m & 64u)) return;
     const float dvdt = P.dv / P.dt;
     float D[3] = {dvdt, dvdt, dvdt};
     float b[3] = {0.f, 0.f, 0.f};
@@ -347,7 +399,7 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
         const int a = face_axis(f);
         if (face_in(P, c.x, c.y, c.z, f)) {
             if (nb_fluid(m, f)) {
-                const float t = P.ds * 0.25f * (uP[a] + ld(uT, a * N + c.i + face_off(P, f)));
+                const float t = P.ds * 0.25f * (uP[a] + uq[f]);
 #pragma unroll
                 for (int k = 0; k < 3; ++k) D[k] = face_sign(f) > 0 ? D[k] + t : D[k] - t;
             }
@@ -368,12 +420,11 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
         }
     }
     // pressure, :1484-1591
-    const float pP = ld(pr, c.i);
     float pf[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (face_in(P, c.x, c.y, c.z, f)) {
-            pf[f] = nb_fluid(m, f) ? 0.5f * (pP + ld(pr, c.i + face_off(P, f))) : pP;
+            pf[f] = nb_fluid(m, f) ? 0.5f * (pP + pq[f]) : pP;
         } else {
             pf[f] = P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE ? 0.f : pP;
         }
@@ -383,7 +434,7 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
     // diffusion, :1593-1836
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        const float vis = vis_face_m(P, m, eddy, face, c, f);
+        const float vis = vis_face_v(P, m, face, c, f, eP, eq[f]);
         if (face_in(P, c.x, c.y, c.z, f)) {
             const float t = nb_fluid(m, f) ? vis * P.ds / P.dx : 2.f * vis * P.ds / P.dx;
 #pragma unroll
@@ -406,13 +457,13 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
     for (int k = 0; k < 3; ++k) b[k] += dvdt * uP[k];
 #pragma unroll
     for (int k = 0; k < 3; ++k) b[k] += P.dv * P.force[k];
-    if (P.les && bles) {
+    if (add_les) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) b[k] += bles[k * N + c.i];
+        for (int k = 0; k < 3; ++k) b[k] += bl[k];
     }
     // Brinkman drag of a soft obstacle mask (no reference counterpart)
     if (drag) {
-        const float t = P.dv * ld(drag, c.i);
+        const float t = P.dv * dr;
 #pragma unroll
         for (int k = 0; k < 3; ++k) D[k] += t;
     }
@@ -471,10 +522,34 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
                                   float* __restrict__ Dp, float* __restrict__ bp) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    const unsigned m = __ldg(P.nbm + c.i);
-    if (!(m & 64u)) return;
     (void)fl;
     const size_t N = P.N;
+    // Every load of the interior path before the fluid test: per face the
+    // neighbour's mask, 1/D and velocity, and the pressures at distance 1 and
+    // 2 along each axis (indices clamped in-domain; a clamped value is never
+    // used, since the mask bits that select it are then 0).
+    const unsigned m = __ldg(P.nbm + c.i);
+    const float pP = ld(pr, c.i);
+    float uP[3], dP[3], uq[6], dq[6], pq[6], pq2[6];
+    unsigned mq[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        uP[a] = ld(u, a * N + c.i);
+        dP[a] = inv_d(iD, Dv, N, a, c.i);
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int a = face_axis(f);
+        const int q = nb_idx(P, c.x, c.y, c.z, c.i, f);
+        const int X = c.x + face_ox(f), Y = c.y + face_oy(f), Z = c.z + face_oz(f);
+        const int q2 = in_region(P, X, Y, Z) ? nb_idx(P, X, Y, Z, q, f) : q;
+        mq[f] = __ldg(P.nbm + q);
+        dq[f] = inv_d(iD, Dv, N, a, q);
+        uq[f] = ld(u, a * N + q);
+        pq[f] = ld(pr, q);
+        pq2[f] = ld(pr, q2);
+    }
+    if (!(m & 64u)) return;
     const float dx2 = 2.f * P.dx;
     float DP = 0.f, bP = 0.f;
 #pragma unroll
@@ -482,26 +557,22 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
         const int a = face_axis(f), s = face_sign(f);
         if (face_in(P, c.x, c.y, c.z, f)) {
             if (!nb_fluid(m, f)) continue;
-            const int q = c.i + face_off(P, f);
-            const float DInv = 0.5f * (inv_d(iD, Dv, N, a, c.i) + inv_d(iD, Dv, N, a, q));
+            const float DInv = 0.5f * (dP[a] + dq[f]);
             DP -= (P.dv / P.den) * DInv / P.dx;
-            const float fl_ = 0.5f * (ld(u, a * N + c.i) + ld(u, a * N + q));
+            const float fl_ = 0.5f * (uP[a] + uq[f]);
             bP = s > 0 ? bP + fl_ : bP - fl_;
             // Rhie-Chow over the face between low cell L and high cell H: the
             // cell beyond Q (q + off(f)) and the cell behind P (i - off(f))
-            const unsigned mq = __ldg(P.nbm + q);
-            const bool beyondQ = nb_fluid(mq, f), behindP = nb_fluid(m, f ^ 1);
-            const int L = s > 0 ? c.i : q, H = s > 0 ? q : c.i;
+            const bool beyondQ = nb_fluid(mq[f], f), behindP = nb_fluid(m, f ^ 1);
             const bool hh = s > 0 ? beyondQ : behindP;
             const bool ll = s > 0 ? behindP : beyondQ;
-            const int HH = s > 0 ? q + face_off(P, f) : c.i + face_off(P, f ^ 1);
-            const int LL = s > 0 ? c.i + face_off(P, f ^ 1) : q + face_off(P, f);
-            const float pL = ld(pr, L), pH = ld(pr, H);
+            const float pL = s > 0 ? pP : pq[f], pH = s > 0 ? pq[f] : pP;
+            const float pHH = s > 0 ? pq2[f] : pq[f ^ 1], pLL = s > 0 ? pq[f ^ 1] : pq2[f];
             const float presGrad = (pH - pL) / P.dx;
             float ave = presGrad;
             if (hh || ll) {
-                const float gH = hh ? (ld(pr, HH) - pL) / dx2 : (pH - pL) / dx2;
-                const float gL = ll ? (pH - ld(pr, LL)) / dx2 : (pH - pL) / dx2;
+                const float gH = hh ? (pHH - pL) / dx2 : (pH - pL) / dx2;
+                const float gL = ll ? (pH - pLL) / dx2 : (pH - pL) / dx2;
                 ave = 0.5f * (gH + gL);
             }
             const float vct = -(P.dv * DInv) / P.den * (presGrad - ave);
@@ -512,13 +583,10 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
                 const float t = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
                 bP = s > 0 ? bP + t : bP - t;
             } else if (vb == WF_BND_ZERO_GRAD) {
-                const float t = ld(u, a * N + c.i);
+                const float t = uP[a];
                 bP = s > 0 ? bP + t : bP - t;
             }
-            if (P.pbc[bc] == WF_BND_FIXED_VALUE) {
-                const float DInv = inv_d(iD, Dv, N, a, c.i);
-                DP -= 2.f * (P.dv / P.den) * DInv / P.dx;
-            }
+            if (P.pbc[bc] == WF_BND_FIXED_VALUE) DP -= 2.f * (P.dv / P.den) * dP[a] / P.dx;
         }
     }
     Dp[c.i] = DP;
@@ -581,25 +649,34 @@ __global__ void k_apply_vel(const __grid_constant__ Params P, const uint8_t* __r
                             const float* __restrict__ iD, float* __restrict__ uc, float* __restrict__ u) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    const unsigned m = __ldg(P.nbm + c.i);
-    if (!(m & 64u)) return;
     (void)fl;
     const size_t N = P.N;
+    // Every load before the fluid test (one wait on memory per thread).
+    const unsigned m = __ldg(P.nbm + c.i);
     const float pP = pc ? ld(pc, c.i) : 0.f;
+    float pn[6], di[3], uo[3];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) pn[f] = pc ? ld(pc, nb_idx(P, c.x, c.y, c.z, c.i, f)) : 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        di[a] = inv_d(iD, Dv, N, a, c.i);
+        uo[a] = ld(u, a * N + c.i);
+    }
+    if (!(m & 64u)) return;
     float pf[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (face_in(P, c.x, c.y, c.z, f)) {
-            pf[f] = nb_fluid(m, f) ? 0.5f * (pP + (pc ? ld(pc, c.i + face_off(P, f)) : 0.f)) : pP;
+            pf[f] = nb_fluid(m, f) ? 0.5f * (pP + pn[f]) : pP;
         } else {
             pf[f] = P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE ? 0.f : pP;
         }
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float corr = -(P.dv / P.den) * inv_d(iD, Dv, N, a, c.i) * (pf[2 * a] - pf[2 * a + 1]) / P.dx;
+        const float corr = -(P.dv / P.den) * di[a] * (pf[2 * a] - pf[2 * a + 1]) / P.dx;
         uc[a * N + c.i] = corr;
-        u[a * N + c.i] += corr;
+        u[a * N + c.i] = uo[a] + corr;
     }
 }
 
@@ -613,22 +690,31 @@ __global__ void k_piso_aodu(const __grid_constant__ Params P, const uint8_t* __r
                             float* __restrict__ aodu) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    const unsigned m = __ldg(P.nbm + c.i);
-    if (!(m & 64u)) return;
     (void)fl;
     const size_t N = P.N;
+    // Every load of the ordinary path before the fluid test.
+    const unsigned m = __ldg(P.nbm + c.i);
+    float uTP[3], uTq[6], ucq[6][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) uTP[a] = ld(uT, a * N + c.i);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int q = nb_idx(P, c.x, c.y, c.z, c.i, f);
+        uTq[f] = ld(uT, face_axis(f) * N + q);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ucq[f][k] = ld(uc, k * N + q);
+    }
+    if (!(m & 64u)) return;
     const bool consistent = (P.compat & WF_COMPAT_PISO_CONSISTENT) != 0;
     float adv[3] = {0.f, 0.f, 0.f}, dif[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (!nb_fluid(m, f)) continue;
-        const int a = face_axis(f);
-        const int q = c.i + face_off(P, f);
-        const float sum = ld(uT, a * N + c.i) + ld(uT, a * N + q);
+        const float sum = uTP[face_axis(f)] + uTq[f];
         const float vis = consistent ? vis_face_m(P, m, eddy, face, c, f) : P.nu;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float uq = ld(uc, k * N + q);
+            const float uq = ucq[f][k];
             const float t = P.ds * 0.25f * uq * sum;
             adv[k] = face_sign(f) > 0 ? adv[k] + t : adv[k] - t;
             dif[k] -= vis * P.ds / P.dx * uq;
@@ -684,21 +770,30 @@ __global__ void k_piso_vel(const __grid_constant__ Params P, const uint8_t* __re
                            float* __restrict__ u) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
-    const unsigned m = __ldg(P.nbm + c.i);
-    if (!(m & 64u)) return;
     (void)fl;
     const size_t N = P.N;
+    // Every load before the fluid test.
+    const unsigned m = __ldg(P.nbm + c.i);
     const float pP = ld(pc, c.i);
+    float pn[6], di[3], ao[3], uo[3];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) pn[f] = ld(pc, nb_idx(P, c.x, c.y, c.z, c.i, f));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        di[a] = inv_d(iD, Dv, N, a, c.i);
+        ao[a] = ld(aodu, a * N + c.i);
+        uo[a] = ld(u, a * N + c.i);
+    }
+    if (!(m & 64u)) return;
     float pf[6];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) pf[f] = nb_fluid(m, f) ? 0.5f * (pP + ld(pc, c.i + face_off(P, f))) : pP;
+    for (int f = 0; f < 6; ++f) pf[f] = nb_fluid(m, f) ? 0.5f * (pP + pn[f]) : pP;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float grad = (pf[2 * a] - pf[2 * a + 1]) / P.dx;
-        const float DInv = inv_d(iD, Dv, N, a, c.i);
-        const float corr = -DInv * (ld(aodu, a * N + c.i) + P.dv / P.den * grad);
+        const float corr = -di[a] * (ao[a] + P.dv / P.den * grad);
         uc[a * N + c.i] = corr;
-        u[a * N + c.i] += corr;
+        u[a * N + c.i] = uo[a] + corr;
     }
 }
 

@@ -51,26 +51,13 @@ __device__ __forceinline__ float vis_face(const Params& P, const uint8_t* fl, co
     return v;
 }
 
-// vis_face from the neighbour mask (same values).
-__device__ __forceinline__ float vis_face_m(const Params& P, unsigned m, const float* eddy, const float* face, int x,
-                                            int y, int z, int i, int f) {
-    if (!P.les) return P.nu;
-    const float eP = ld(eddy, i);
-    float v = P.nu + eP;
-    if (face_in(P, x, y, z, f)) {
-        const int q = i + face_off(P, f);
-        if (nb_fluid(m, f)) v = P.nu + 0.5f * (eP + ld(eddy, q));
-        else v = P.nu + face_read(P, face, face_sign(f) > 0 ? q : i, face_axis(f));
-    } else if (f == 3 && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE) {
-        v = P.nu + face_read(P, face, i, 1);
-    }
-    return v;
-}
 __device__ __forceinline__ float inv_d(const float* iD, const float* Dv, size_t N, int a, int i) {
     return iD ? ld(iD, a * N + i) : 1.f / ld(Dv, a * N + i);
 }
 
 // Momentum coefficients.  A: 6 planes (faces E,W,N,S,U,D), iD: 3 planes.
+// A is non-zero only on fluid-fluid faces, where the face viscosity is
+// nu + (eddy_P + eddy_Q) / 2 (nu without LES), as in vis_face.
 __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                            const float* __restrict__ uT, const float* __restrict__ eddy,
                            const float* __restrict__ face, const float* __restrict__ Dv,
@@ -80,9 +67,24 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     if (x >= P.nx || y >= P.ny || z >= P.nz) return;
     (void)fl;
+    (void)face;
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
+    // Every load before the fluid test.
     const unsigned m = __ldg(P.nbm + i);
+    float uTP[3], dv[3], uTq[6], eq[6];
+    const float eP = P.les ? ld(eddy, i) : 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        uTP[a] = ld(uT, a * N + i);
+        dv[a] = ld(Dv, a * N + i);
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int q = nb_idx(P, x, y, z, i, f);
+        uTq[f] = ld(uT, face_axis(f) * N + q);
+        eq[f] = P.les ? ld(eddy, q) : 0.f;
+    }
     if (!(m & 64u)) {
 #pragma unroll
         for (int f = 0; f < 6; ++f) A[f * N + i] = 0.f;
@@ -92,23 +94,25 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
     }
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        const int a = face_axis(f);
         float c = 0.f;
         if (nb_fluid(m, f)) {
-            const int q = i + face_off(P, f);
-            const float conv = P.ds * 0.25f * (ld(uT, a * N + i) + ld(uT, a * N + q));
-            const float vis = vis_face_m(P, m, eddy, face, x, y, z, i, f);
+            const float conv = P.ds * 0.25f * (uTP[face_axis(f)] + uTq[f]);
+            const float vis = P.les ? P.nu + 0.5f * (eP + eq[f]) : P.nu;
             const float dif = vis * P.ds / P.dx;
             c = face_sign(f) > 0 ? dif - conv : dif + conv;
         }
         A[f * N + i] = c;
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) iD[k * N + i] = 1.0f / ld(Dv, k * N + i);
+    for (int k = 0; k < 3; ++k) iD[k * N + i] = 1.0f / dv[k];
 }
 
 // One momentum sweep: uo_P = iD_P (sum_f A_f ui_f + b_P) on fluid cells.
 // kCopyAll: non-fluid cells copy ui (a complete iterate in a fresh buffer).
+// Every load is issued before the fluid test: a thread waits on memory once,
+// not once for 1/D and again for the rest (76 -> 63 us per sweep on the
+// urban block; indices are clamped in-domain, so the loads of non-fluid cells
+// are harmless and their results unused).
 template <bool kCopyAll = false>
 __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Params P, const float* __restrict__ A,
                                                     const float* __restrict__ iD, const float* __restrict__ bv,
@@ -119,19 +123,14 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
     if (x >= P.nx || y >= P.ny || z >= P.nz) return;
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
-    const float d0 = ld(iD, i);
-    if (d0 == 0.f) {  // non-fluid cell
-        if (kCopyAll)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) uo[k * N + i] = ld(ui, k * N + i);
-        return;
-    }
-    const float a0 = ld(A, i), a1 = ld(A, N + i), a2 = ld(A, 2 * N + i);
-    const float a3 = ld(A, 3 * N + i), a4 = ld(A, 4 * N + i), a5 = ld(A, 5 * N + i);
     const int sx = P.nx, sz = P.nx * P.ny;
     const int iE = x + 1 < P.nx ? i + 1 : i, iW = x > 0 ? i - 1 : i;
     const int iN = y + 1 < P.ny ? i + sx : i, iS = y > 0 ? i - sx : i;
     const int iU = z + 1 < P.nz ? i + sz : i, iDn = z > 0 ? i - sz : i;
+    const float d0 = ld(iD, i), d1 = ld(iD, N + i), d2 = ld(iD, 2 * N + i);
+    const float a0 = ld(A, i), a1 = ld(A, N + i), a2 = ld(A, 2 * N + i);
+    const float a3 = ld(A, 3 * N + i), a4 = ld(A, 4 * N + i), a5 = ld(A, 5 * N + i);
+    float r[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float* u = ui + k * N;
@@ -141,9 +140,17 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
         s += a3 * ld(u, iS);
         s += a4 * ld(u, iU);
         s += a5 * ld(u, iDn);
-        const float dk = k == 0 ? d0 : ld(iD, k * N + i);
-        uo[k * N + i] = dk * (s + ld(bv, k * N + i));
+        r[k] = s + ld(bv, k * N + i);
     }
+    if (d0 == 0.f) {  // non-fluid cell
+        if (kCopyAll)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) uo[k * N + i] = ld(ui, k * N + i);
+        return;
+    }
+    uo[i] = d0 * r[0];
+    uo[N + i] = d1 * r[1];
+    uo[2 * N + i] = d2 * r[2];
 }
 
 // One momentum sweep, four consecutive x cells per thread (nx % 4 == 0):
@@ -255,7 +262,20 @@ __global__ void k_piso_pre(const __grid_constant__ Params P, const uint8_t* __re
     (void)fl;
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
+    // Every load before the fluid test.
     const unsigned m = __ldg(P.nbm + i);
+    float dP[3], aP[3], dq[6], aq[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        dP[a] = inv_d(iDc, Dv, N, a, i);
+        aP[a] = ld(aodu, a * N + i);
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int q = nb_idx(P, x, y, z, i, f);
+        dq[f] = inv_d(iDc, Dv, N, face_axis(f), q);
+        aq[f] = ld(aodu, face_axis(f) * N + q);
+    }
     if (!(m & 64u)) {
         ainv[i] = 0.f;
         rhs[i] = 0.f;
@@ -267,16 +287,12 @@ __global__ void k_piso_pre(const __grid_constant__ Params P, const uint8_t* __re
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f);
         if (!face_in(P, x, y, z, f)) {
-            if (consistent && P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE) {
-                const float DInv = inv_d(iDc, Dv, N, a, i);
-                coeff -= 2.f * (P.dv / P.den) * DInv / P.dx;
-            }
+            if (consistent && P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE) coeff -= 2.f * (P.dv / P.den) * dP[a] / P.dx;
             continue;
         }
         if (!nb_fluid(m, f)) continue;
-        const int q = i + face_off(P, f);
-        const float AdInv = 0.5f * (inv_d(iDc, Dv, N, a, i) + inv_d(iDc, Dv, N, a, q));
-        const float Aod = 0.5f * (ld(aodu, a * N + i) + ld(aodu, a * N + q));
+        const float AdInv = 0.5f * (dP[a] + dq[f]);
+        const float Aod = 0.5f * (aP[a] + aq[f]);
         if (a == 0) coeff -= (P.dv / P.den) * (AdInv / P.dx);
         else coeff -= (P.dv / P.den) * AdInv / P.dx;
         vt = face_sign(f) > 0 ? vt - AdInv * Aod : vt + AdInv * Aod;
