@@ -61,10 +61,8 @@ def parse():
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from unitywindsimulation_b200.replicas import env_ranks
+    return env_ranks()
 
 
 def make_case(name: str):
@@ -304,12 +302,11 @@ def run_windfvm(args):
 
     from unitywindsimulation_b200 import FvmSolverCuda, _lib, cases
 
+    from unitywindsimulation_b200.replicas import ReplicaGroup, whole_job_rate
+
     rank, world, local = dist_env()
-    dist = world > 1
-    if dist:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
+    group = ReplicaGroup("nccl")
 
     case = make_case(args.workload)
     cfg = case.cfg
@@ -318,16 +315,10 @@ def run_windfvm(args):
     cases.apply_case(solver, case)
 
     def barrier():
-        if dist:
-            torch.distributed.barrier()
+        group.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = group.max_over_ranks
 
     # ---- device-resident throughput ----
     solver.Step(args.warmup)
@@ -344,7 +335,7 @@ def run_windfvm(args):
     clocks = clk.stop()
     barrier()
     ms_max = max_over_ranks(ms)
-    value = world * N * args.steps / (ms_max / 1e3) / 1e6
+    value = whole_job_rate(N, args.steps, ms_max, world)
     solver.check_finite()
 
     # ---- end to end through the public API with host buffers ----
@@ -377,7 +368,7 @@ def run_windfvm(args):
         e1.synchronize()
         barrier()
         e_ms = max_over_ranks(e0.elapsed_time(e1))
-        e2e = {"value": world * N * args.steps / (e_ms / 1e3) / 1e6, "unit": METRIC,
+        e2e = {"value": whole_job_rate(N, args.steps, e_ms, world), "unit": METRIC,
                "h2d_bytes_per_step": int(inlet.size * 4), "d2h_bytes_per_step": int(4 * N * 4),
                "api": "set_inflow_plane + Step + readback_begin/readback_wait of velocity and pressure "
                       "(every step's fields copied to pinned host buffers, overlapping the next step)"}
@@ -424,9 +415,7 @@ def run_windfvm(args):
             "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
-    if dist:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    group.close()
     return 0
 
 
