@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="print the host-core baselines of every workload (no GPU) and exit")
     return ap.parse_args()
 
 
@@ -172,6 +174,69 @@ def host_step_sampler(case, max_steps: int, budget_s: float):
             break
     dt = time.perf_counter() - t0
     return case.n_cells * done / dt / 1e6, dt, done, cores, kind, what
+
+
+def _host_rate(make, cases_, max_steps: int, budget_s: float):
+    """Mcell-steps/s of whole steps over a list of cases on the host cores
+    (each case stepped until max_steps or its share of the budget)."""
+    cells_steps, secs = 0, 0.0
+    for c in cases_:
+        s = make(c)
+        done, t0 = 0, time.perf_counter()
+        while done < max_steps:
+            s.Step(1)
+            done += 1
+            if time.perf_counter() - t0 >= budget_s / len(cases_):
+                break
+        secs += time.perf_counter() - t0
+        cells_steps += c.n_cells * done
+        s.close()
+    return cells_steps / secs / 1e6
+
+
+def cpu_table(max_steps: int = 2, budget_s: float = 20.0):
+    """The CPU baselines of every workload on the host cores: the reference's
+    own kernels (FP32, where oracle/_ref/ is built) and the oracle in FP32 and
+    FP64.  The reference kernels take the oracle's set-up state; they have no
+    drag field, so the soft-mask workloads run without it there."""
+    from oracle import OracleSolver
+    from oracle.binding import RefSolver, ref_available
+    from unitywindsimulation_b200 import cases
+
+    cores = os.cpu_count() or 1
+    work = {
+        "cfg1 plain_cube": [cases.plain_cube()],
+        "cfg2 urban_block": [cases.urban_block()],
+        "cfg3 batch_directions (16 cases)": cases.batch_directions(),
+        "cfg4 adjoint_street (forward)": [cases.adjoint_street()],
+        "cfg5 adjoint_batch (one direction)": cases.adjoint_batch()[:1],
+    }
+
+    def oracle(prec):
+        def make(c):
+            o = OracleSolver(c.cfg, prec, threads=cores)
+            cases.apply_case(o, c)
+            return o
+        return make
+
+    def reference(c):
+        o = OracleSolver(c.cfg, 32, threads=cores)
+        cases.apply_case(o, c)
+        r = RefSolver(c.cfg, construct=False)
+        r.copy_state_from(o)
+        o.close()
+        return r
+
+    rows = {}
+    for name, cs in work.items():
+        row = {"cells": sum(c.n_cells for c in cs)}
+        if ref_available():
+            row["reference_kernels_f32"] = _host_rate(reference, cs, max_steps, budget_s)
+        row["oracle_f32"] = _host_rate(oracle(32), cs, max_steps, budget_s)
+        row["oracle_f64"] = _host_rate(oracle(64), cs, max_steps, budget_s)
+        rows[name] = row
+        print(json.dumps({name: row}), flush=True)
+    return {"unit": METRIC, "cores": cores, "max_steps": max_steps, "budget_s": budget_s, "rows": rows}
 
 
 def cpu_baseline(case, steps: int):
@@ -421,6 +486,9 @@ def run_windfvm(args):
 
 def main():
     args = parse()
+    if args.cpu_table:
+        print(json.dumps(cpu_table()), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_windfvm(args)
