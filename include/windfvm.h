@@ -430,17 +430,22 @@ typedef struct wf_objective {
  * interior profile of wf_init_vel_pres_fields (the current state must be that
  * profile).  dJ_ddrag (nullable, N floats): derivative with respect to the
  * drag field (WF_FIELD_DRAG), from which a soft building mask's height
- * gradients follow by the chain rule.  States are stored every
- * `checkpoint_every` steps and the others recomputed.  ms_forward / ms_total
+ * gradients follow by the chain rule.  Steps that are not taped in the
+ * forward pass are checkpointed every `checkpoint_every` steps and
+ * recomputed (see wf_adj_set_max_tapes).  ms_forward / ms_total
  * (nullable): device time of the forward pass and of the whole call.
  * Derivatives are summed with float atomics: repeated calls agree to
  * rounding, not bit for bit. */
 /* Device memory of the gradient: one step tape takes about
- * (3 nV + (nP + 1)(nC + 1) + 45) floats per cell.  A checkpoint segment is
- * reversed from checkpoint_every tapes when they fit; otherwise (or beyond
- * max_tapes, 0 = no cap) the segment's states are stored and it is reversed
- * in sub-blocks of the tapes that fit, at the cost of one more recomputed
- * step per step.  Results do not depend on the split. */
+ * (3 nV + (nP + 1)(nC + 1) + 45) floats per cell.  wf_adj_gradient keeps as
+ * many step tapes as device memory holds (at most max_tapes, 0 = no cap, and
+ * at most n_steps), leaving room for the checkpoints and 1 GB.  The last R
+ * steps of the window (R = the tapes kept) are taped during the forward pass
+ * and reversed without recomputation; the earlier steps are checkpointed
+ * every checkpoint_every steps and each segment is recomputed into tapes and
+ * reversed, in sub-blocks from stored segment states when its tapes do not
+ * all fit (one more recomputed step per step).  The tapes stay allocated
+ * until wf_adj_destroy.  Results do not depend on the split. */
 int wf_adj_set_max_tapes(wf_adjoint* a, int max_tapes);
 int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
                     double* J, double* dJ_dustar, double* dJ_dz0, float* dJ_ddrag, float* ms_forward,

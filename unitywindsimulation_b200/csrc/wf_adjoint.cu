@@ -997,13 +997,16 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     const int area = (obj->x1 - obj->x0) * (obj->z1 - obj->z0);
     const float w = 1.f / (float)(obj->window * area);
     const dim3 og((obj->x1 - obj->x0 + 31) / 32, (obj->z1 - obj->z0 + 7) / 8), ob(32, 8);
-    // checkpoints: state n for n % C == 0 (n < n_steps).  The steps of one
-    // segment are recomputed into tapes and reversed: all C at once when C
-    // tapes fit in device memory, else the segment's states are stored and
+    // Step tapes are kept for as many steps as device memory holds (up to
+    // max_tapes, and never more than the window).  The last R steps of the
+    // window are taped during the forward pass itself and reversed without
+    // recomputation; the first nf = n_steps - R steps run as the solver's own
+    // step with checkpoints every C steps (state n for n % C == 0, n < nf),
+    // and each of their segments is recomputed into tapes and reversed: all
+    // at once when the segment's tapes fit, else its states are stored and
     // it is reversed in sub-blocks of as many tapes as fit (one more
     // recomputation per step).
     const int C = std::min(checkpoint_every, n_steps);
-    const int nck = (n_steps + C - 1) / C;
     struct Scratch {
         cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
         float* states = nullptr;  // C states of 4N floats (sub-block mode)
@@ -1014,18 +1017,15 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
         }
     } E;
     for (float* p : a->ck) cudaFree(p);
-    a->ck.assign(nck, nullptr);
-    for (int i = 0; i < nck; ++i)
-        if (cudaMalloc((void**)&a->ck[i], v + s) != cudaSuccess) {
-            cudaGetLastError();
-            return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
-        }
-    const int cap = a->max_tapes > 0 ? std::min(C, a->max_tapes) : C;
+    a->ck.clear();
+    const int cap = a->max_tapes > 0 ? std::min(n_steps, a->max_tapes) : n_steps;
     int T = std::min((int)a->tapes.size(), cap);
     if (T < cap) {
-        // as many tapes as fit, keeping room for the segment states
+        // as many tapes as fit, keeping room for the checkpoints and the
+        // segment states of the sub-block mode
         const size_t tape_bytes = tape_floats(a) * sizeof(float);
-        const size_t reserve = (size_t)C * (v + s) + (size_t(1) << 30);
+        const int nck_max = (n_steps + C - 1) / C;
+        const size_t reserve = (size_t)(C + nck_max) * (v + s) + (size_t(1) << 30);
         while (T < cap) {
             size_t fr = 0, tot = 0;
             if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || fr < tape_bytes + reserve) break;
@@ -1036,15 +1036,24 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
         if (T < 1) return adj_fail(a, WF_ERR_OOM, "no device memory for one step tape");
     }
     T = std::min(T, cap);
-    if (T < C && cudaMalloc((void**)&E.states, (size_t)C * (v + s)) != cudaSuccess) {
+    const int R = T, nf = n_steps - R;
+    const int nck = nf > 0 ? (nf + C - 1) / C : 0;
+    a->ck.assign(nck, nullptr);
+    for (int i = 0; i < nck; ++i)
+        if (cudaMalloc((void**)&a->ck[i], v + s) != cudaSuccess) {
+            cudaGetLastError();
+            return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
+        }
+    if (nf > 0 && T < C && cudaMalloc((void**)&E.states, (size_t)C * (v + s)) != cudaSuccess) {
         cudaGetLastError();
         return adj_fail(a, WF_ERR_OOM, "no device memory for the segment states: lower checkpoint_every");
     }
     for (cudaEvent_t& e : E.ev) WFA_CUDA(cudaEventCreate(&e));
     WFA_CUDA(cudaMemsetAsync(a->dJ, 0, sizeof(double), h->st));
     WFA_CUDA(cudaEventRecord(E.ev[0], h->st));
-    // ---- forward: the solver's own (fast) step, checkpoints, objective
-    for (int n = 0; n < n_steps; ++n) {
+    // ---- forward: the solver's own (fast) step with checkpoints, then the
+    // taped tail; the objective on the way
+    for (int n = 0; n < nf; ++n) {
         if (n % C == 0) {
             WFA_CUDA(cudaMemcpyAsync(a->ck[n / C], h->vb[h->iT], v, cudaMemcpyDeviceToDevice, h->st));
             WFA_CUDA(cudaMemcpyAsync(a->ck[n / C] + 3 * N, h->pr, s, cudaMemcpyDeviceToDevice, h->st));
@@ -1055,16 +1064,45 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
             wf::k_objective<<<og, ob, 0, h->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
                                                   h->vb[h->iT], nullptr, a->dJ);
     }
-    WFA_CUDA(cudaEventRecord(E.ev[1], h->st));
     WFA_CUDA(cudaStreamSynchronize(h->st));
-    // ---- reverse, one segment at a time
+    int rs = WF_OK;
+    for (int j = 0; j < R; ++j) {
+        const float* ui = j == 0 ? h->vb[h->iT] : a->tapes[j - 1].uout;
+        const float* pi = j == 0 ? h->pr : a->tapes[j - 1].pout;
+        rs = record_step(a, a->tapes[j], ui, pi, 3);
+        if (rs != WF_OK) return rs;
+        if (nf + j + 1 > n_steps - obj->window)
+            wf::k_objective<<<og, ob, 0, a->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w,
+                                                  a->tapes[j].uout, nullptr, a->dJ);
+    }
+    WFA_CUDA(cudaEventRecord(E.ev[1], a->st));
+    if (R > 0) {
+        // the solver ends at the window's last state, as after R more steps
+        // (velFieldLastTime and velFieldLastIter take it; the pressure
+        // corrections restart from zero)
+        WFA_CUDA(cudaMemcpyAsync(h->vb[h->iT], a->tapes[R - 1].uout, v, cudaMemcpyDeviceToDevice, a->st));
+        WFA_CUDA(cudaMemcpyAsync(h->pr, a->tapes[R - 1].pout, s, cudaMemcpyDeviceToDevice, a->st));
+        for (int b = 0; b < 3; ++b) WFA_CUDA(cudaMemsetAsync(h->pcb[b], 0, s, a->st));
+        h->iter_alias = true;
+        h->pc_zero = true;
+        h->step += R;
+    }
+    WFA_CUDA(cudaStreamSynchronize(a->st));
+    // ---- reverse: the taped tail, then one segment at a time
     WFA_CUDA(cudaMemsetAsync(a->ub, 0, v, a->st));
     WFA_CUDA(cudaMemsetAsync(a->pb, 0, s, a->st));
     WFA_CUDA(cudaMemsetAsync(a->gb, 0, plane_floats(P) * sizeof(float), a->st));
     WFA_CUDA(cudaMemsetAsync(a->dragb, 0, s, a->st));
-    int rs = WF_OK;
+    for (int j = R - 1; j >= 0; --j) {
+        const Tape& t = a->tapes[j];
+        if (nf + j + 1 > n_steps - obj->window)
+            wf::k_objective<<<og, ob, 0, a->st>>>(P, h->fl, obj->x0, obj->x1, obj->y, obj->z0, obj->z1, w, t.uout,
+                                                  a->ub, nullptr);
+        rs = adjoint_step(a, t, 3);
+        if (rs != WF_OK) return rs;
+    }
     for (int sgi = nck - 1; sgi >= 0; --sgi) {
-        const int n0 = sgi * C, n1 = std::min(n_steps, n0 + C), L = n1 - n0;
+        const int n0 = sgi * C, n1 = std::min(nf, n0 + C), L = n1 - n0;
         // state j of the segment (state n0 + j): from the checkpoint, or
         // from the stored segment states in sub-block mode
         auto state = [&](int j) -> float* { return j == 0 ? a->ck[sgi] : E.states + (size_t)j * 4 * N; };
