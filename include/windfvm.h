@@ -443,10 +443,17 @@ typedef struct wf_objective {
  * steps of the window (R = the tapes kept) are taped during the forward pass
  * and reversed without recomputation; the earlier steps are checkpointed
  * every checkpoint_every steps and each segment is recomputed into tapes and
- * reversed, in sub-blocks from stored segment states when its tapes do not
- * all fit (one more recomputed step per step).  The tapes stay allocated
- * until wf_adj_destroy.  Results do not depend on the split. */
+ * reversed.  When a segment's tapes do not all fit, the segments are
+ * shortened to the tapes that fit (more checkpoints; each step recomputed
+ * once), or, with wf_adj_set_segment_policy(a, 0) or when the extra
+ * checkpoints do not fit, the segment's states are stored and it is
+ * reversed in sub-blocks (each step recomputed twice).  The tapes stay
+ * allocated until wf_adj_destroy.  Results do not depend on the split. */
 int wf_adj_set_max_tapes(wf_adjoint* a, int max_tapes);
+/* shorten = 1 (default): shorter segments when a segment's tapes do not fit;
+ * 0: keep checkpoint_every and reverse in sub-blocks.  No reference
+ * counterpart (the reference has no differentiated form). */
+int wf_adj_set_segment_policy(wf_adjoint* a, int shorten);
 int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
                     double* J, double* dJ_dustar, double* dJ_dz0, float* dJ_ddrag, float* ms_forward,
                     float* ms_total);

@@ -226,16 +226,18 @@ def test_checkpoint_interval_does_not_change_gradient(built):
 
 
 def test_tape_cap_does_not_change_gradient(built):
-    """Segments longer than the tape cap are reversed in sub-blocks from
+    """Tape caps below the window: the taped tail is shorter, and segments
+    longer than the cap are either shortened or reversed in sub-blocks from
     stored segment states; the gradient is the same."""
     case = cases.small_soft_case(seed=9)
     obj = Objective(x0=4, x1=20, z0=2, z1=14, y=1, window=3)
     out = []
-    for cap in (0, 2, 1):
+    for cap, shorten in ((0, True), (2, True), (1, True), (2, False), (1, False)):
         g = FvmSolverCuda(case.cfg)
         cases.apply_case(g, case)
         with AdjointSolver(g) as adj:
             adj.set_max_tapes(cap)
+            adj.set_segment_policy(shorten)
             out.append(adj.gradient(obj, 7, checkpoint_every=5, soft=case.soft))
         g.close()
     for r in out[1:]:

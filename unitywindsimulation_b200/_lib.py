@@ -192,6 +192,7 @@ _SIGNATURES = {
     "wf_adj_destroy": (c_int, [c_void_p]),
     "wf_adj_last_error": (c_char_p, [c_void_p]),
     "wf_adj_set_max_tapes": (c_int, [c_void_p, c_int]),
+    "wf_adj_set_segment_policy": (c_int, [c_void_p, c_int]),
     "wf_adj_step_forward": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "wf_adj_step_vjp": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "wf_adj_gradient": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_double), POINTER(c_double),

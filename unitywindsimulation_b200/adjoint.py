@@ -91,6 +91,13 @@ class AdjointSolver:
         fit); longer checkpoint segments are reversed in sub-blocks."""
         self._check(self._lib.wf_adj_set_max_tapes(self._a, int(max_tapes)))
 
+    def set_segment_policy(self, shorten: bool) -> None:
+        """True (default): when a checkpoint segment's tapes do not fit,
+        shorten the segments to the tapes that fit (each step recomputed
+        once); False: keep the interval and reverse in sub-blocks from stored
+        segment states (each step recomputed twice)."""
+        self._check(self._lib.wf_adj_set_segment_policy(self._a, int(bool(shorten))))
+
     def step_forward(self, phases: int = PHASE_FULL):
         """State after one step from the solver's current state, cut after
         ``phases`` parts; the solver does not advance.  Returns (u (3, N), p (N))."""

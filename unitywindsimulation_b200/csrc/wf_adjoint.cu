@@ -640,6 +640,7 @@ struct wf_adjoint {
     size_t N = 0;
     std::vector<Tape> tapes;                    // tapes[0] always allocated
     int max_tapes = 0;                          // cap on the tapes a gradient uses (0: as many as fit)
+    bool shorten = true;                        // segments no longer than the tapes that fit
     std::vector<void*> blocks;                  // allocations behind the tapes
     // adjoint work
     float *ub = nullptr, *uTb = nullptr, *pb = nullptr, *pb_in = nullptr;
@@ -931,6 +932,12 @@ int wf_adj_destroy(wf_adjoint* a) {
 
 const char* wf_adj_last_error(const wf_adjoint* a) { return a ? a->err.c_str() : "null adjoint"; }
 
+int wf_adj_set_segment_policy(wf_adjoint* a, int shorten) {
+    if (!a || (shorten != 0 && shorten != 1)) return WF_ERR_INVALID_ARG;
+    a->shorten = shorten != 0;
+    return WF_OK;
+}
+
 int wf_adj_set_max_tapes(wf_adjoint* a, int max_tapes) {
     if (!a || max_tapes < 0) return WF_ERR_INVALID_ARG;
     a->max_tapes = max_tapes;
@@ -1006,7 +1013,7 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     // at once when the segment's tapes fit, else its states are stored and
     // it is reversed in sub-blocks of as many tapes as fit (one more
     // recomputation per step).
-    const int C = std::min(checkpoint_every, n_steps);
+    int C = std::min(checkpoint_every, n_steps);
     struct Scratch {
         cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
         float* states = nullptr;  // C states of 4N floats (sub-block mode)
@@ -1037,13 +1044,33 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     }
     T = std::min(T, cap);
     const int R = T, nf = n_steps - R;
-    const int nck = nf > 0 ? (nf + C - 1) / C : 0;
-    a->ck.assign(nck, nullptr);
-    for (int i = 0; i < nck; ++i)
-        if (cudaMalloc((void**)&a->ck[i], v + s) != cudaSuccess) {
+    // When a segment's tapes do not all fit, shorter segments (one more
+    // checkpoint per T steps) recompute each step once; the sub-block mode
+    // recomputes it twice.  Fall back to the sub-block mode when the extra
+    // checkpoints do not fit.
+    int nck = nf > 0 ? (nf + C - 1) / C : 0;
+    if (a->shorten && nf > 0 && T < C) {
+        const int nck_short = (nf + T - 1) / T;
+        std::vector<float*> ck(nck_short, nullptr);
+        bool ok = true;
+        for (int i = 0; i < nck_short && ok; ++i) ok = cudaMalloc((void**)&ck[i], v + s) == cudaSuccess;
+        if (ok) {
+            C = T;
+            nck = nck_short;
+            a->ck = ck;
+        } else {
             cudaGetLastError();
-            return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
+            for (float* p : ck) cudaFree(p);
         }
+    }
+    if (a->ck.empty()) {
+        a->ck.assign(nck, nullptr);
+        for (int i = 0; i < nck; ++i)
+            if (cudaMalloc((void**)&a->ck[i], v + s) != cudaSuccess) {
+                cudaGetLastError();
+                return adj_fail(a, WF_ERR_OOM, "checkpoint memory");
+            }
+    }
     if (nf > 0 && T < C && cudaMalloc((void**)&E.states, (size_t)C * (v + s)) != cudaSuccess) {
         cudaGetLastError();
         return adj_fail(a, WF_ERR_OOM, "no device memory for the segment states: lower checkpoint_every");
