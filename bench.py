@@ -402,6 +402,9 @@ def run_windfvm(args):
     ms_max = max_over_ranks(ms)
     value = whole_job_rate(N, args.steps, ms_max, world)
     solver.check_finite()
+    # one more step, outside the timed region, traced phase by phase (no
+    # graph replay) to show where a step's time goes
+    phases = solver.step_phases()
 
     # ---- end to end through the public API with host buffers ----
     e2e = None
@@ -473,6 +476,7 @@ def run_windfvm(args):
             "e2e": e2e, "gpu_launches": launches * world, "clocks": clocks, "roofline": roofline,
             "cpu_baseline": cpu,
             "step_alg_gbs": step_gbs, "step_alg_frac": step_gbs / peak,
+            "step_phases_ms": phases,
             "vel_sweep_kernel": {"ms_per_launch": v_ms, "alg_bytes_per_launch": v_bytes,
                                  "achieved_gbs": v_bytes / (v_ms / 1e3) / 1e9, "sweeps_per_launch": v_sweeps},
             "batched": batched,

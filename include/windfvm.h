@@ -311,6 +311,26 @@ int wf_last_step_ms(const wf_solver* h, float* ms);
  * handle was created (graph replays count every kernel node). */
 int wf_kernel_launches(const wf_solver* h, int64_t* total);
 
+/* One step like wf_step(h, 1, NULL), enqueued kernel by kernel (no graph
+ * replay) with a CUDA event between its phases; phase_ms[WF_PHASE_COUNT]
+ * receives the device time of each phase (0 for phases the configuration
+ * skips).  The fields end as after wf_step.  Host NVTX ranges name the step
+ * and its phases for a profiler.  Replaces the reference's per-Step
+ * Stopwatch log (FvmSolverGpu.cs:168-170,1111-1114), which timed host
+ * dispatch only. */
+enum {
+    WF_PHASE_LES = 0,         /* wall function, eddy viscosity, LES term      */
+    WF_PHASE_VEL_PRE = 1,     /* momentum D, b                                */
+    WF_PHASE_VEL_SWEEPS = 2,  /* momentum Jacobi loop (coefficients included) */
+    WF_PHASE_PRES_PRE = 3,    /* pressure-correction Dp, bp                   */
+    WF_PHASE_PRES_SWEEPS = 4, /* pressure Jacobi loop (coefficients included) */
+    WF_PHASE_CORRECT = 5,     /* apply p', normalisation, velocity correction */
+    WF_PHASE_PISO = 6,        /* PISO correctors                              */
+    WF_PHASE_END = 7,         /* end-of-step rotation                         */
+    WF_PHASE_COUNT = 8
+};
+int wf_step_phases(wf_solver* h, float* phase_ms);
+
 /* Times `reps` launches of one hot kernel of the step on the handle's
  * current coefficients, with CUDA events on the handle's stream; when
  * flush_l2 != 0 a 256 MiB buffer is written before each launch so every

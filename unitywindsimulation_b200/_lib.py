@@ -171,6 +171,7 @@ _SIGNATURES = {
     "wf_last_step_ms": (c_int, [c_void_p, POINTER(c_float)]),
     "wf_kernel_launches": (c_int, [c_void_p, POINTER(c_int64)]),
     "wf_time_kernel": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_float), POINTER(c_double), POINTER(c_int)]),
+    "wf_step_phases": (c_int, [c_void_p, POINTER(c_float)]),
     "wf_pres_residual_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, POINTER(c_float)]),
     "wf_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)]),
     "wf_batch_destroy": (c_int, [c_void_p]),
@@ -202,6 +203,8 @@ _SIGNATURES = {
 NOALLOC_BLOCKS = 4096
 NOALLOC_MAX_CELLS = NOALLOC_BLOCKS * 256 * 64
 
+PHASE_NAMES = ("les", "vel_pre", "vel_sweeps", "pres_pre", "pres_sweeps", "correct", "piso", "end")
+PHASE_COUNT = len(PHASE_NAMES)
 KERNEL_PRES_SWEEP = 0
 KERNEL_VEL_SWEEP = 1
 

@@ -8,6 +8,7 @@
 // (end-of-step velocity copy and zeroing the pressure correction) are
 // replaced by role flags (iter_alias, pc_zero) that the kernels honour.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -700,9 +701,18 @@ int wf_prepare_graphs(wf_solver* h) {
     return WF_OK;
 }
 
+namespace {
+// Host NVTX range, closed when the scope ends.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+}  // namespace
+
 int wf_step(wf_solver* h, int n_steps, int* ready) {
     if (!h) return WF_ERR_INVALID_ARG;
     if (n_steps < 0) return set_err(h, WF_ERR_INVALID_ARG, "n_steps must be >= 0");
+    NvtxRange range("wf_step");
     WF_CUDA(cudaSetDevice(h->device));
     WF_CUDA(cudaEventRecord(h->ev0, h->st));
     for (int i = 0; i < n_steps; ++i) WF_TRY(run_step(h));
@@ -711,6 +721,71 @@ int wf_step(wf_solver* h, int n_steps, int* ready) {
     WF_CUDA(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
     if (h->cfg.check_finite) WF_TRY(check_finite(h));
     if (ready) *ready = 1;
+    return WF_OK;
+}
+
+int wf_step_phases(wf_solver* h, float* phase_ms) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (!phase_ms) return set_err(h, WF_ERR_INVALID_ARG, "phase_ms is NULL");
+    NvtxRange range("wf_step_phases");
+    WF_CUDA(cudaSetDevice(h->device));
+    for (int p = 0; p < WF_PHASE_COUNT; ++p) phase_ms[p] = 0.f;
+    struct Events {
+        cudaEvent_t e[WF_PHASE_COUNT + 1] = {};
+        ~Events() {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } E;
+    for (cudaEvent_t& e : E.e) WF_CUDA(cudaEventCreate(&e));
+    const wf_config& c = h->cfg;
+    const long long l0 = wf::g_launches;
+    int phase = -1;
+    // closes the previous phase at the current point of the stream
+    auto mark = [&](int next) -> int {
+        if (phase >= 0) nvtxRangePop();
+        WF_CUDA(cudaEventRecord(E.e[next], h->st));
+        phase = next;
+        if (next < WF_PHASE_COUNT) {
+            static const char* names[WF_PHASE_COUNT] = {"les", "vel_pre", "vel_sweeps", "pres_pre",
+                                                        "pres_sweeps", "correct", "piso", "end"};
+            nvtxRangePushA(names[next]);
+        }
+        return WF_OK;
+    };
+    h->in_step = true;
+    int st = WF_OK;
+    do {
+        if ((st = mark(WF_PHASE_LES)) != WF_OK) break;
+        if (h->P.les && (st = do_les(h)) != WF_OK) break;
+        if ((st = mark(WF_PHASE_VEL_PRE)) != WF_OK) break;
+        if ((st = do_vel_precompute(h)) != WF_OK) break;
+        if ((st = mark(WF_PHASE_VEL_SWEEPS)) != WF_OK) break;
+        if ((st = do_vel_sweeps(h, c.vel_iters, true)) != WF_OK) break;
+        if ((st = mark(WF_PHASE_PRES_PRE)) != WF_OK) break;
+        if ((st = do_pres_precompute(h)) != WF_OK) break;
+        if ((st = mark(WF_PHASE_PRES_SWEEPS)) != WF_OK) break;
+        if ((st = do_pres_sweeps(h, c.pres_iters, true)) != WF_OK) break;
+        if ((st = mark(WF_PHASE_CORRECT)) != WF_OK) break;
+        if ((st = do_apply_pres(h)) != WF_OK) break;
+        if (!any_fixed_pres(c) && (st = do_normalize(h)) != WF_OK) break;
+        if ((st = do_apply_vel(h)) != WF_OK) break;
+        h->pc_zero = true;  // SetPresCorrectFieldtoZero (:1088)
+        if ((st = mark(WF_PHASE_PISO)) != WF_OK) break;
+        if (c.solver_type == WF_SOLVER_PISO)
+            for (int n = 0; n < c.piso_correctors && st == WF_OK; ++n) st = do_piso(h, c.pres_iters, true);
+        if (st != WF_OK) break;
+        if ((st = mark(WF_PHASE_END)) != WF_OK) break;
+        if ((st = do_end_step(h)) != WF_OK) break;
+        st = mark(WF_PHASE_COUNT);
+    } while (false);
+    h->in_step = false;
+    if (phase >= 0 && phase < WF_PHASE_COUNT) nvtxRangePop();
+    h->launches += wf::g_launches - l0;
+    if (st != WF_OK) return st;
+    WF_TRY(sync(h));
+    for (int p = 0; p < WF_PHASE_COUNT; ++p) WF_CUDA(cudaEventElapsedTime(&phase_ms[p], E.e[p], E.e[p + 1]));
+    if (h->cfg.check_finite) WF_TRY(check_finite(h));
     return WF_OK;
 }
 

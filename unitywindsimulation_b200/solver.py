@@ -223,6 +223,14 @@ class FvmSolverCuda:
         self._check(self._lib.wf_kernel_launches(self._h, byref(n)))
         return n.value
 
+    def step_phases(self) -> dict:
+        """One step enqueued kernel by kernel with a CUDA event between its
+        phases (wf_step_phases): {phase name: device ms}.  The fields end as
+        after Step(1)."""
+        out = (c_float * _lib.PHASE_COUNT)()
+        self._check(self._lib.wf_step_phases(self._h, out))
+        return {n: float(out[i]) for i, n in enumerate(_lib.PHASE_NAMES)}
+
     def time_kernel(self, kernel: int, reps: int = 20, flush_l2: bool = True):
         """(ms per launch, algorithmic bytes per launch, sweeps per launch)."""
         ms, by, sw = c_float(0), c_double(0), c_int(0)
