@@ -164,11 +164,23 @@ int wf_change_phys_field_pos(wf_solver* h);
 int wf_init_from_background(wf_solver* h, const wf_solver* bg, const float pos[3], const float pos_bg[3],
                             float rot_deg);
 /* Replaces the X0 inlet plane with caller data: ny*nz*3 floats, index
- * (z*ny + y)*3 + c (perturbed inflow). */
+ * (z*ny + y)*3 + c (perturbed inflow).  The data are copied before the call
+ * returns (through a page-locked staging buffer the handle allocates on
+ * first use); the upload is ordered before the next step and does not wait
+ * for the GPU. */
 int wf_set_inflow_plane(wf_solver* h, const float* x0_plane_xyz);
 /* Step() repeated n_steps times, each a complete time step with fixed
  * iteration counts (no 30 ms time slicing).  *ready (may be NULL) = 1. */
 int wf_step(wf_solver* h, int n_steps, int* ready);
+/* The steps of wf_step enqueued on the handle's stream without waiting for
+ * them, as Unity's Dispatch calls return before the GPU runs them
+ * (FvmSolverGpu.cs:1050-1121): a host can prepare the next inputs while the
+ * GPU steps.  No finiteness check and no wf_last_step_ms update.  Every
+ * call that reads fields to the host, wf_readback_wait and wf_sync wait for
+ * the steps; a device fault surfaces at the next waiting call. */
+int wf_step_async(wf_solver* h, int n_steps);
+/* Waits for all work enqueued on the handle's stream. */
+int wf_sync(wf_solver* h);
 /* No counterpart in the reference.  The step rotates its buffers, so its
  * CUDA graph depends on which buffer holds which field; the few such states
  * repeat with a short period, and wf_step captures the graph of each state

@@ -123,6 +123,11 @@ void free_all(wf_solver* h) {
         cudaStreamSynchronize(h->cst);
         cudaStreamDestroy(h->cst);
     }
+    if (h->ev_in) {
+        cudaEventSynchronize(h->ev_in);
+        cudaEventDestroy(h->ev_in);
+    }
+    if (h->in_stage) cudaFreeHost(h->in_stage);
     if (h->ev_snap) cudaEventDestroy(h->ev_snap);
     if (h->ev_done) cudaEventDestroy(h->ev_done);
     if (h->snap) cudaFree(h->snap);
@@ -674,12 +679,26 @@ int wf_set_inflow_plane(wf_solver* h, const float* pl) {
     if (!h) return WF_ERR_INVALID_ARG;
     if (!pl) return set_err(h, WF_ERR_INVALID_ARG, "plane is NULL");
     WF_CUDA(cudaSetDevice(h->device));
-    const int n = h->P.plane[WF_FACE_X0];
-    std::vector<float> soa(3 * (size_t)n);
-    for (int i = 0; i < n; ++i)
-        for (int c = 0; c < 3; ++c) soa[(size_t)c * n + i] = pl[3 * (size_t)i + c];
-    WF_CUDA(cudaMemcpyAsync(h->bnd[WF_FACE_X0], soa.data(), soa.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
-    return sync(h);
+    const size_t n = (size_t)h->P.plane[WF_FACE_X0];
+    // The plane is transposed into a page-locked staging buffer owned by the
+    // handle and copied on the solver stream, ordered before the next step,
+    // without waiting for the GPU: the caller may reuse `pl` at once.  The
+    // staging is rewritten only after the previous upload has left it.
+    if (!h->in_stage) {
+        if (cudaMallocHost((void**)&h->in_stage, 3 * n * sizeof(float)) != cudaSuccess) {
+            h->in_stage = nullptr;
+            cudaGetLastError();
+            return set_err(h, WF_ERR_OOM, "page-locked staging for the inflow plane");
+        }
+        WF_CUDA(cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+    } else {
+        WF_CUDA(cudaEventSynchronize(h->ev_in));
+    }
+    for (size_t i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) h->in_stage[(size_t)c * n + i] = pl[3 * i + c];
+    WF_CUDA(cudaMemcpyAsync(h->bnd[WF_FACE_X0], h->in_stage, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    WF_CUDA(cudaEventRecord(h->ev_in, h->st));
+    return WF_OK;
 }
 
 int wf_prepare_graphs(wf_solver* h) {
@@ -722,6 +741,21 @@ int wf_step(wf_solver* h, int n_steps, int* ready) {
     if (h->cfg.check_finite) WF_TRY(check_finite(h));
     if (ready) *ready = 1;
     return WF_OK;
+}
+
+int wf_step_async(wf_solver* h, int n_steps) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    if (n_steps < 0) return set_err(h, WF_ERR_INVALID_ARG, "n_steps must be >= 0");
+    NvtxRange range("wf_step_async");
+    WF_CUDA(cudaSetDevice(h->device));
+    for (int i = 0; i < n_steps; ++i) WF_TRY(run_step(h));
+    return WF_OK;
+}
+
+int wf_sync(wf_solver* h) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    WF_CUDA(cudaSetDevice(h->device));
+    return sync(h);
 }
 
 int wf_step_phases(wf_solver* h, float* phase_ms) {

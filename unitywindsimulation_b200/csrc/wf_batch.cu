@@ -134,6 +134,10 @@ int wf_batch_step(wf_batch* b, int n_steps) {
     if (!b) return WF_ERR_INVALID_ARG;
     if (n_steps < 0) return fail(b, WF_ERR_INVALID_ARG, "n_steps must be >= 0");
     if (cudaSetDevice(b->device) != cudaSuccess) return fail(b, WF_ERR_CUDA, "cudaSetDevice failed");
+    // Work still queued on a case's own stream (an inflow-plane upload, an
+    // asynchronous step) finishes before the batch touches the case.
+    for (wf_solver* h : b->s)
+        if (cudaStreamSynchronize(h->st) != cudaSuccess) return fail(b, WF_ERR_CUDA, "case stream failed");
     // Cases not yet in the graph-replay state (first step after an init or
     // a field write) take one eager step on their own stream first.
     bool any_eager = false;

@@ -58,6 +58,10 @@ struct wf_solver {
     float* dref = nullptr;
     int* dbad = nullptr;
     void* stage = nullptr;    // 4N floats of device staging for host I/O
+    // inflow-plane upload: page-locked staging (3 * ny * nz floats) and the
+    // event after which the staging may be rewritten
+    float* in_stage = nullptr;
+    cudaEvent_t ev_in = nullptr;
     // asynchronous readback: snapshot (4N + N floats), copy stream, events
     float* snap = nullptr;
     cudaStream_t cst = nullptr;

@@ -223,6 +223,14 @@ class FvmSolverCuda:
         self._check(self._lib.wf_kernel_launches(self._h, byref(n)))
         return n.value
 
+    def step_async(self, n_steps: int = 1) -> None:
+        """Enqueues n_steps steps without waiting for them (wf_step_async)."""
+        self._check(self._lib.wf_step_async(self._h, int(n_steps)))
+
+    def sync(self) -> None:
+        """Waits for every step and copy enqueued on the solver's stream."""
+        self._check(self._lib.wf_sync(self._h))
+
     def step_phases(self) -> dict:
         """One step enqueued kernel by kernel with a CUDA event between its
         phases (wf_step_phases): {phase name: device ms}.  The fields end as
