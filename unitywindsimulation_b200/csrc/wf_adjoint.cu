@@ -447,6 +447,61 @@ __global__ void __launch_bounds__(256) k_adj_vsweepT(const __grid_constant__ Par
         else out[k * N + c.i] = ld(iD, k * N + c.i) * s;
     }
 }
+// k_adj_vsweepT<false> with four x-consecutive cells per thread (nx % 4 == 0,
+// 16-byte aligned planes): 128-bit loads, every load issued first, the same
+// arithmetic per cell (the forward sweep's four-cell form, transposed).
+__device__ __forceinline__ float4 ld4a(const float* p, size_t i) {
+    return __ldg(reinterpret_cast<const float4*>(p + i));
+}
+__device__ __forceinline__ float f4a(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+__global__ void __launch_bounds__(256) k_adj_vsweepT4(const __grid_constant__ Params P, const float* __restrict__ AT,
+                                                      const float* __restrict__ iD, const float* __restrict__ Wi,
+                                                      float* __restrict__ out) {
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x0 >= P.nx || y >= P.ny || z >= P.nz) return;
+    const int i = cidx(P, x0, y, z);
+    const size_t N = P.N;
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const int iN = y + 1 < P.ny ? i + sx : i, iS = y > 0 ? i - sx : i;
+    const int iU = z + 1 < P.nz ? i + sz : i, iDn = z > 0 ? i - sz : i;
+    const int iE = x0 + 4 < P.nx ? i + 4 : i + 3, iW = x0 > 0 ? i - 1 : i;
+    const float4 t0 = ld4a(AT, i), t1 = ld4a(AT, N + i), t2 = ld4a(AT, 2 * N + i);
+    const float4 t3 = ld4a(AT, 3 * N + i), t4 = ld4a(AT, 4 * N + i), t5 = ld4a(AT, 5 * N + i);
+    float4 c[3], n[3], so[3], up[3], dn[3], dd[3];
+    float e3[3], w0[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float* w = Wi + k * N;
+        c[k] = ld4a(w, i);
+        n[k] = ld4a(w, iN);
+        so[k] = ld4a(w, iS);
+        up[k] = ld4a(w, iU);
+        dn[k] = ld4a(w, iDn);
+        e3[k] = __ldg(w + iE);
+        w0[k] = __ldg(w + iW);
+        dd[k] = ld4a(iD, k * N + i);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float we = j < 3 ? f4a(c[k], j + 1) : e3[k];
+            const float ww = j > 0 ? f4a(c[k], j - 1) : w0[k];
+            float s = f4a(t0, j) * we;
+            s += f4a(t1, j) * ww;
+            s += f4a(t2, j) * f4a(n[k], j);
+            s += f4a(t3, j) * f4a(so[k], j);
+            s += f4a(t4, j) * f4a(up[k], j);
+            s += f4a(t5, j) * f4a(dn[k], j);
+            v[j] = f4a(dd[k], j) * s;
+        }
+        *reinterpret_cast<float4*>(out + k * N + i) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
 // One pass over the loop's iterates (u: stack u^0..u^n, W: stack W^1..W^n,
 // slot k at k*3N): bbar = sum_k W^k, Dbar -= sum_k W^k u^k (adjoint of 1/D
 // folded in), Abar_f = sum_k W^k . u^{k-1}_nb, and the adjoint of
@@ -846,8 +901,15 @@ int adjoint_step(wf_adjoint* a, const Tape& t, int phases) {
         wf::k_adj_vtrans<<<g, bk, 0, st>>>(P, t.A, a->AT);
         wf::k_adj_vinit<<<wf::lin_blocks(3 * (long long)N), 256, 0, st>>>(3 * (long long)N, t.iD, a->ub,
                                                                            V(a, a->Wv, n));
-        for (int k = n - 1; k >= 1; --k)
-            wf::k_adj_vsweepT<false><<<g, bk, 0, st>>>(P, a->AT, t.iD, V(a, a->Wv, k + 1), nullptr, V(a, a->Wv, k));
+        const bool v4 = n > 1 && wf::quad_ok(P, {a->AT, t.iD, V(a, a->Wv, n), V(a, a->Wv, n - 1)});
+        const dim3 g4((P.nx / 4 + bk.x - 1) / bk.x, (P.ny + bk.y - 1) / bk.y, (P.nz + bk.z - 1) / bk.z);
+        for (int k = n - 1; k >= 1; --k) {
+            if (v4)
+                wf::k_adj_vsweepT4<<<g4, bk, 0, st>>>(P, a->AT, t.iD, V(a, a->Wv, k + 1), V(a, a->Wv, k));
+            else
+                wf::k_adj_vsweepT<false><<<g, bk, 0, st>>>(P, a->AT, t.iD, V(a, a->Wv, k + 1), nullptr,
+                                                          V(a, a->Wv, k));
+        }
         wf::k_adj_vsweepT<true><<<g, bk, 0, st>>>(P, a->AT, t.iD, V(a, a->Wv, 1), a->ub, a->uTb);
         wf::k_adj_vacc<<<g, bk, 0, st>>>(P, n, h->fl, a->Wv, t.uit, a->bb, a->Db, a->uTb);
     } else {

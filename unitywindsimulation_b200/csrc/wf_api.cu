@@ -570,6 +570,7 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     for (int f = 0; f < 6; ++f) { P.vbc[f] = cfg->vel_bc[f]; P.pbc[f] = cfg->pres_bc[f]; }
     P.les = cfg->turbulence == WF_TURB_SMAGORINSKY;
     P.compat = cfg->compat_flags;
+    P.vec4 = h->vec4;
 
     int s = WF_OK;
     auto fail = [&](int code) {

@@ -10,6 +10,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <initializer_list>
 
 #include "../../include/windfvm.h"
 
@@ -30,6 +31,7 @@ struct Params {
     int vbc[6], pbc[6];
     int les;
     unsigned compat;
+    int vec4;       // != 0: four-cells-per-thread kernels where nx % 4 == 0
     // per-cell neighbour mask (see nb_fluid): bit f (0..5) = the neighbour
     // across face f is inside the domain and fluid, bit 6 = the cell is fluid
     const uint8_t* nbm;
@@ -80,6 +82,15 @@ __device__ __forceinline__ int plane_idx(const Params& P, int bc, int x, int y, 
 }
 __device__ __forceinline__ float bnd_comp(const Params& P, const Bnd& B, int bc, int x, int y, int z, int c) {
     return __ldg(B.p[bc] + (size_t)c * P.plane[bc] + plane_idx(P, bc, x, y, z));
+}
+
+// Where a four-cells-per-thread kernel applies: the switch (Params::vec4),
+// nx % 4 == 0 and 16-byte aligned planes.
+inline bool quad_ok(const Params& P, std::initializer_list<const void*> ptrs) {
+    if (!P.vec4 || P.nx % 4 != 0) return false;
+    for (const void* p : ptrs)
+        if (p && (reinterpret_cast<uintptr_t>(p) & 15u) != 0) return false;
+    return true;
 }
 
 }  // namespace wf

@@ -231,11 +231,10 @@ __global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Para
     }
 }
 
-// The four-cell sweep applies: x extent a multiple of 4 and every plane
-// 16-byte aligned.
+// The four-cell sweep applies: the switch on, x extent a multiple of 4 and
+// every plane 16-byte aligned.
 bool vec4_ok(const Params& P, const void* A, const void* iD, const void* bv, const void* ui, const void* uo) {
-    auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-    return P.nx % 4 == 0 && al(A) && al(iD) && al(bv) && al(ui) && al(uo);
+    return quad_ok(P, {A, iD, bv, ui, uo});
 }
 // Pressure face coefficients c_E, c_N, c_U (FvmColl.compute:2813-2814 form
 // ((dv/den) * DInv) / dx) for fluid-fluid faces, else 0.
@@ -712,7 +711,7 @@ void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
     const Params& P = h->P;
     const size_t N = P.N;
     WF_COUNT_LAUNCH();
-    if (h->vec4 && vec4_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst)) {
+    if (vec4_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst)) {
         k_vel_sweep4<false><<<grd4(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
     } else {
         k_vel_sweep1<false><<<grd(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
