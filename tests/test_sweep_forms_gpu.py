@@ -62,8 +62,8 @@ def test_odd_nx_uses_scalar_sweep_and_matches_oracle(built):
 
 def test_adjoint_gradient_same_in_both_forms(built):
     """The adjoint's recorded steps and its reversed momentum loop use the
-    four-cell sweeps too; J is bit-identical and the gradient agrees with the
-    one-cell forms up to the float atomics of the adjoint's scatters."""
+    four-cell sweeps and accumulation passes too; J and the gradient agree
+    with the one-cell forms up to the order of the atomic additions."""
     from unitywindsimulation_b200.adjoint import AdjointSolver, Objective
     case = cases.small_soft_case(seed=9)
     obj = Objective(x0=4, x1=20, z0=2, z1=14, y=1, window=2)
@@ -73,6 +73,7 @@ def test_adjoint_gradient_same_in_both_forms(built):
         with AdjointSolver(g) as adj:
             out.append(adj.gradient(obj, 4, 2, soft=case.soft))
         g.close()
-    assert out[0]["J"] == out[1]["J"]
+    # J sums each step's objective with double-precision atomics
+    assert out[0]["J"] == pytest.approx(out[1]["J"], rel=1e-12)
     assert out[0]["dJ_dustar"] == pytest.approx(out[1]["dJ_dustar"], rel=1e-5)
     assert out[0]["dJ_dz0"] == pytest.approx(out[1]["dJ_dz0"], rel=1e-5)

@@ -172,6 +172,72 @@ __global__ void __launch_bounds__(256) k_adj_pacc(const __grid_constant__ Params
     c3bar[2 * N + c.i] += cU;
 }
 
+// k_adj_pacc with four x-consecutive cells per thread (nx % 4 == 0, aligned
+// planes): 128-bit loads, the same per-cell sums (bit-identical).
+__device__ __forceinline__ float4 ld4p(const float* p, size_t i) {
+    return __ldg(reinterpret_cast<const float4*>(p + i));
+}
+__device__ __forceinline__ float f4p(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+__global__ void __launch_bounds__(256) k_adj_pacc4(const __grid_constant__ Params P, int n,
+                                                   const float* __restrict__ ai, const float* __restrict__ W,
+                                                   const float* __restrict__ s, float* __restrict__ rbar,
+                                                   float* __restrict__ coefbar, float* __restrict__ c3bar) {
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x0 >= P.nx || y >= P.ny || z >= P.nz) return;
+    const int i = cidx(P, x0, y, z);
+    const size_t N = P.N;
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const bool hE3 = x0 + 4 < P.nx, hN = y + 1 < P.ny, hU = z + 1 < P.nz;
+    const int iE = hE3 ? i + 4 : i + 3, iN = hN ? i + sx : i, iU = hU ? i + sz : i;
+    const float4 a4 = ld4p(ai, i);
+    float r[4] = {0.f, 0.f, 0.f, 0.f}, d[4] = {0.f, 0.f, 0.f, 0.f};
+    float cE[4] = {0.f, 0.f, 0.f, 0.f}, cN[4] = {0.f, 0.f, 0.f, 0.f}, cU[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int k = 1; k <= n; ++k) {
+        const float* Wk = W + (size_t)(n - k) * N;
+        const float* sk = s + (size_t)k * N;
+        const float* sm = s + (size_t)(k - 1) * N;
+        const float4 w = ld4p(Wk, i), sv = ld4p(sk, i);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            r[j] += f4p(w, j);
+            d[j] -= f4p(w, j) * f4p(sv, j);
+        }
+        if (k > 1) {
+            const float4 sp = ld4p(sm, i), sn = ld4p(sm, iN), su = ld4p(sm, iU);
+            const float4 wn = ld4p(Wk, iN), wu = ld4p(Wk, iU);
+            const float se3 = __ldg(sm + iE), we3 = __ldg(Wk + iE);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float wj = f4p(w, j), sP = f4p(sp, j);
+                if (j < 3 || hE3) {
+                    const float sE = j < 3 ? f4p(sp, j + 1) : se3;
+                    const float wE = j < 3 ? f4p(w, j + 1) : we3;
+                    cE[j] -= wj * sE + wE * sP;
+                }
+                if (hN) cN[j] -= wj * f4p(sn, j) + f4p(wn, j) * sP;
+                if (hU) cU[j] -= wj * f4p(su, j) + f4p(wu, j) * sP;
+            }
+        }
+    }
+    float ro[4], co[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const bool fl = f4p(a4, j) != 0.f;
+        ro[j] = fl ? r[j] : 0.f;
+        co[j] = fl ? d[j] : 0.f;
+        if (fl) {
+            c3bar[i + j] += cE[j];
+            c3bar[N + i + j] += cN[j];
+            c3bar[2 * N + i + j] += cU[j];
+        }
+    }
+    *reinterpret_cast<float4*>(rbar + i) = make_float4(ro[0], ro[1], ro[2], ro[3]);
+    *reinterpret_cast<float4*>(coefbar + i) = make_float4(co[0], co[1], co[2], co[3]);
+}
+
 // VJP of PISOPRE: coef = -sum_f (dv/den) AdInv_f / dx, ai = 1/coef,
 // r = -sum_f s_f AdInv_f Aod_f (PisoColl.compute:196-255); coefbar is the
 // adjoint of coef.
@@ -557,6 +623,97 @@ __global__ void __launch_bounds__(256) k_adj_vacc(const __grid_constant__ Params
     }
 }
 
+// k_adj_vacc with four x-consecutive cells per thread (nx % 4 == 0, aligned
+// planes): every iterate plane is read with 128-bit loads (the x neighbours
+// beyond the four cells with scalar loads), a quarter of the load
+// instructions of one cell per thread; the per-cell sums are the same
+// (bbar and the own-cell parts bit-identical, the scattered parts to the
+// order of the float atomics).  Fluid cells and fluid-fluid faces come from
+// the neighbour mask.
+__global__ void __launch_bounds__(128) k_adj_vacc4(const __grid_constant__ Params P, int n,
+                                                   const float* __restrict__ W, const float* __restrict__ u,
+                                                   float* __restrict__ bbar, float* __restrict__ Dbar,
+                                                   float* __restrict__ uTbar) {
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (x0 >= P.nx || y >= P.ny || z >= P.nz) return;
+    const int i = cidx(P, x0, y, z);
+    const size_t N = P.N, N3 = 3 * N;
+    const uchar4 m4 = __ldg(reinterpret_cast<const uchar4*>(P.nbm + i));
+    const unsigned mm[4] = {m4.x, m4.y, m4.z, m4.w};
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const int iN = y + 1 < P.ny ? i + sx : i, iS = y > 0 ? i - sx : i;
+    const int iU = z + 1 < P.nz ? i + sz : i, iDn = z > 0 ? i - sz : i;
+    const int iE = x0 + 4 < P.nx ? i + 4 : i + 3, iW = x0 > 0 ? i - 1 : i;
+    float Ab[4][6], bb[4][3], db[4][3];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) Ab[j][f] = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) bb[j][c] = db[j][c] = 0.f;
+    }
+#pragma unroll 1
+    for (int k = 1; k <= n; ++k) {
+        const float* Wk = W + k * N3;
+        const float* uk = u + k * N3;
+        const float* um = u + (k - 1) * N3;
+        float4 w[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            w[c] = ld4a(Wk, c * N + i);
+            const float4 uu = ld4a(uk, c * N + i);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                bb[j][c] += f4a(w[c], j);
+                db[j][c] -= f4a(w[c], j) * f4a(uu, j);
+            }
+        }
+        float nv[3][4][6];  // u^{k-1} at the neighbour across f of cell j
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float* p = um + c * N;
+            const float4 cc = ld4a(p, i), nn = ld4a(p, iN), ss = ld4a(p, iS), uu = ld4a(p, iU), dd = ld4a(p, iDn);
+            const float e3 = __ldg(p + iE), w0 = __ldg(p + iW);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                nv[c][j][0] = j < 3 ? f4a(cc, j + 1) : e3;
+                nv[c][j][1] = j > 0 ? f4a(cc, j - 1) : w0;
+                nv[c][j][2] = f4a(nn, j);
+                nv[c][j][3] = f4a(ss, j);
+                nv[c][j][4] = f4a(uu, j);
+                nv[c][j][5] = f4a(dd, j);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int f = 0; f < 6; ++f) {
+                if (!nb_fluid(mm[j], f)) continue;
+                Ab[j][f] += f4a(w[0], j) * nv[0][j][f] + f4a(w[1], j) * nv[1][j][f] + f4a(w[2], j) * nv[2][j][f];
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (!(mm[j] & 64u)) continue;
+        const int ij = i + j;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            bbar[c * N + ij] = bb[j][c];
+            aadd(Dbar + c * N + ij, db[j][c]);
+        }
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            if (!nb_fluid(mm[j], f)) continue;
+            const int a = face_axis(f), s = face_sign(f);
+            const float t = -s * P.ds * 0.25f * Ab[j][f];
+            aadd(uTbar + a * N + ij, t);
+            aadd(uTbar + a * N + ij + face_off(P, f), t);
+        }
+    }
+}
+
 // VJP of PRE (CSVelPredictPreCompute with LES off, FvmColl.compute:1292-1859).
 __global__ void k_adj_pre(const __grid_constant__ Params P, const Bnd B, const BndBar G,
                           const uint8_t* __restrict__ fl, const float* __restrict__ Dbar,
@@ -850,7 +1007,12 @@ void reverse_pres_loop(wf_adjoint* a, const float* ai, const float* c3, const fl
     // slot j of a->Wp holds W^{n-j}
     wf::k_adj_pinit<<<wf::lin_blocks(a->N), 256, 0, st>>>((int)a->N, ai, a->sb, a->Wp);
     if (n > 1) wf::launch_pres_stack(P, st, a->h->num_sms, c3, ai, nullptr, a->Wp, n - 1, false);
-    wf::k_adj_pacc<<<g, bk, 0, st>>>(P, n, ai, a->Wp, sstack, a->rb, a->dgb, a->c3b);
+    if (wf::quad_ok(P, {ai, a->Wp, sstack, a->rb, a->dgb, a->c3b})) {
+        const dim3 b4 = wf::cblk(), g4q((P.nx / 4 + b4.x - 1) / b4.x, (P.ny + b4.y - 1) / b4.y, (P.nz + b4.z - 1) / b4.z);
+        wf::k_adj_pacc4<<<g4q, b4, 0, st>>>(P, n, ai, a->Wp, sstack, a->rb, a->dgb, a->c3b);
+    } else {
+        wf::k_adj_pacc<<<g, bk, 0, st>>>(P, n, ai, a->Wp, sstack, a->rb, a->dgb, a->c3b);
+    }
 }
 
 // Reverse of record_step: on entry a->ub / a->pb hold the adjoints of
@@ -911,7 +1073,12 @@ int adjoint_step(wf_adjoint* a, const Tape& t, int phases) {
                                                           V(a, a->Wv, k));
         }
         wf::k_adj_vsweepT<true><<<g, bk, 0, st>>>(P, a->AT, t.iD, V(a, a->Wv, 1), a->ub, a->uTb);
-        wf::k_adj_vacc<<<g, bk, 0, st>>>(P, n, h->fl, a->Wv, t.uit, a->bb, a->Db, a->uTb);
+        if (wf::quad_ok(P, {a->Wv, t.uit, a->bb, a->Db, a->uTb})) {
+            const dim3 b4(32, 4, 1), g4q((P.nx / 4 + 31) / 32, (P.ny + 3) / 4, P.nz);
+            wf::k_adj_vacc4<<<g4q, b4, 0, st>>>(P, n, a->Wv, t.uit, a->bb, a->Db, a->uTb);
+        } else {
+            wf::k_adj_vacc<<<g, bk, 0, st>>>(P, n, h->fl, a->Wv, t.uit, a->bb, a->Db, a->uTb);
+        }
     } else {
         wf::k_axpy<<<wf::lin_blocks(3 * (long long)N), 256, 0, st>>>(3 * (long long)N, 1.f, a->ub, a->uTb);
         WFA_CUDA(cudaMemsetAsync(a->bb, 0, v, st));
