@@ -629,6 +629,22 @@ __global__ void k_apply_pres(const __grid_constant__ Params P, const uint8_t* __
     pr[c.i] += pc ? ld(pc, c.i) : 0.f;
 }
 
+// k_apply_pres on four consecutive cells per thread, every load issued before
+// the solid test; solid cells are stored back unchanged.  n4 = N / 4.
+__global__ void k_apply_pres4(int n4, const uint8_t* __restrict__ fl, const float* __restrict__ pc,
+                              float* __restrict__ pr) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n4) return;
+    const uchar4 f = __ldg(reinterpret_cast<const uchar4*>(fl) + q);
+    const float4 c = pc ? __ldg(reinterpret_cast<const float4*>(pc) + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 p = reinterpret_cast<const float4*>(pr)[q];
+    if (f.x != WF_CELL_SOLID) p.x += c.x;
+    if (f.y != WF_CELL_SOLID) p.y += c.y;
+    if (f.z != WF_CELL_SOLID) p.z += c.z;
+    if (f.w != WF_CELL_SOLID) p.w += c.w;
+    reinterpret_cast<float4*>(pr)[q] = p;
+}
+
 // CSPresNormalization, FvmColl.compute:2865-2880, split in two launches so
 // the reference value is read before any cell is updated.
 __global__ void k_norm_read(const __grid_constant__ Params P, const float* __restrict__ pr, float* __restrict__ ref) {
@@ -1047,6 +1063,12 @@ void launch_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, cons
     WF_LAUNCH(k_pres_sweep, fl, pin, Dv, Dp, bp, pout);
 }
 void launch_apply_pres(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, float* pr) {
+    if (quad_ok(P, {fl, pc, pr})) {
+        WF_COUNT_LAUNCH();
+        const int n4 = P.N / 4;
+        k_apply_pres4<<<(n4 + 255) / 256, 256, 0, st>>>(n4, fl, pc, pr);
+        return;
+    }
     WF_LAUNCH(k_apply_pres, fl, pc, pr);
 }
 void launch_normalize(const Params& P, cudaStream_t st, const uint8_t* fl, float* pr, float* ref) {
