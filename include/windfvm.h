@@ -261,7 +261,9 @@ int wf_get_field(wf_solver* h, int field, float* out);
 int wf_set_field(wf_solver* h, int field, const float* in);
 
 /* Device pointers for zero-copy consumers (e.g. torch).  Valid until the
- * next wf_step / wf_init_* / wf_set_* / wf_destroy. */
+ * next wf_step / wf_step_async / wf_init_* / wf_set_* / wf_destroy.  Work
+ * queued by wf_step_async may still be running: order reads after it on
+ * `stream`, or call wf_sync first. */
 typedef struct wf_device_fields {
     float*   vel[3];     /* velocity components (SoA planes), N floats each */
     float*   pres;       /* pressure, N floats                              */
