@@ -321,6 +321,18 @@ int wf_version(void);   /* WF_ABI_VERSION */
  * measured with CUDA events on the handle's stream. */
 int wf_last_step_ms(const wf_solver* h, float* ms);
 
+/* Building footprints rasterised into an int32 flag array (nx*ny*nz, index
+ * (z*ny + y)*nx + x, 1 = solid) on `device`: boxes[5*b .. 5*b+4] =
+ * (x0, x1, z0, z1, h) in cells, rotated by angle_deg about the domain centre
+ * in the x-z plane and tested at cell centres; columns within `margin` cells
+ * of the x/z boundaries stay fluid; a column is solid up to min(round(h),
+ * ny - 1) cells of the tallest box containing it.  The flag layout is the one
+ * BuildingVoxelizer produces for InitFlags (BuildingVoxelizer.cs:355-413);
+ * the rasterisation itself (boxes instead of Unity meshes) has no counterpart
+ * in the reference.  Allocates and frees device memory for the call. */
+int wf_rasterise_boxes(int nx, int ny, int nz, const double* boxes, int n_boxes, double angle_deg, int margin,
+                       int device, int32_t* flags);
+
 /* Number of kernels this library launched inside wf_step calls since the
  * handle was created (graph replays count every kernel node). */
 int wf_kernel_launches(const wf_solver* h, int64_t* total);

@@ -172,6 +172,8 @@ _SIGNATURES = {
     "wf_kernel_launches": (c_int, [c_void_p, POINTER(c_int64)]),
     "wf_time_kernel": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_float), POINTER(c_double), POINTER(c_int)]),
     "wf_step_phases": (c_int, [c_void_p, POINTER(c_float)]),
+    "wf_rasterise_boxes": (c_int, [c_int, c_int, c_int, POINTER(c_double), c_int, c_double, c_int, c_int,
+                                   POINTER(c_int32)]),
     "wf_step_async": (c_int, [c_void_p, c_int]),
     "wf_sync": (c_int, [c_void_p]),
     "wf_pres_residual_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, POINTER(c_float)]),

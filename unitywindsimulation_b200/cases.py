@@ -125,6 +125,21 @@ def rasterise_boxes(nx: int, ny: int, nz: int, boxes, angle_deg: float = 0.0, ma
     return flags
 
 
+def rasterise_boxes_gpu(nx: int, ny: int, nz: int, boxes, angle_deg: float = 0.0, margin: int = MARGIN,
+                        device: int = 0) -> np.ndarray:
+    """rasterise_boxes on the GPU (wf_rasterise_boxes): the same flags, bit for
+    bit, in a fraction of the time for large grids and many directions."""
+    from ctypes import POINTER, c_double, c_int32
+    lib = _lib.load()
+    b = np.ascontiguousarray([[float(v) for v in bx[:5]] for bx in boxes], dtype=np.float64).reshape(-1)
+    out = np.empty((nz, ny, nx), dtype=np.int32)
+    st = lib.wf_rasterise_boxes(nx, ny, nz, b.ctypes.data_as(POINTER(c_double)), len(boxes), float(angle_deg),
+                                int(margin), int(device), out.ctypes.data_as(POINTER(c_int32)))
+    if st != _lib.WF_OK:
+        raise RuntimeError(f"wf_rasterise_boxes failed with status {st}")
+    return out
+
+
 def street_lattice_buildings(rng: np.random.Generator, nx: int, nz: int, count: int, fp_lo: int, fp_hi: int,
                              h_lo: float, h_hi: float, block: int = 16, street: int = 2, margin: int = MARGIN,
                              integer_heights: bool = True):
