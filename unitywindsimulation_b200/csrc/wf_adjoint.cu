@@ -537,6 +537,12 @@ __global__ void __launch_bounds__(256) k_adj_vsweepT4(const __grid_constant__ Pa
     const float4 t3 = ld4a(AT, 3 * N + i), t4 = ld4a(AT, 4 * N + i), t5 = ld4a(AT, 5 * N + i);
     float4 c[3], n[3], so[3], up[3], dn[3], dd[3];
     float e3[3], w0[3];
+    // 1/D: the first component stands for all three outside d_split cells,
+    // read there from one address (an L1 hit) so no load waits on a branch
+    const size_t o1 = d_split(P, x0, x0 + 3, y, z) ? N : 0;
+    dd[0] = ld4a(iD, i);
+    dd[1] = ld4a(iD, o1 + i);
+    dd[2] = ld4a(iD, 2 * o1 + i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float* w = Wi + k * N;
@@ -547,7 +553,6 @@ __global__ void __launch_bounds__(256) k_adj_vsweepT4(const __grid_constant__ Pa
         dn[k] = ld4a(w, iDn);
         e3[k] = __ldg(w + iE);
         w0[k] = __ldg(w + iW);
-        dd[k] = ld4a(iD, k * N + i);
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {

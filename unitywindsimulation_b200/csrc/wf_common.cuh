@@ -84,6 +84,22 @@ __device__ __forceinline__ float bnd_comp(const Params& P, const Bnd& B, int bc,
     return __ldg(B.p[bc] + (size_t)c * P.plane[bc] + plane_idx(P, bc, x, y, z));
 }
 
+// The three components of the momentum diagonal D (and of 1/D) are bit-
+// identical in every cell but those with a domain-boundary face under a
+// symmetry velocity condition: there the diffusion term adds to the normal
+// component only (FvmColl.compute:1666,1699,1732,1765,1798,1831); every other
+// term of D adds one value to all three.  True when any of the cells x0..x1
+// of row (y, z) is such a cell, i.e. where a sweep must read all three
+// components of 1/D rather than the first one alone.
+__device__ __forceinline__ bool d_split(const Params& P, int x0, int x1, int y, int z) {
+    return (x0 == 0 && P.vbc[WF_FACE_X0] == WF_BND_SYMMETRY) ||
+           (x1 == P.nx - 1 && P.vbc[WF_FACE_XN] == WF_BND_SYMMETRY) ||
+           (y == 0 && P.vbc[WF_FACE_Y0] == WF_BND_SYMMETRY) ||
+           (y == P.ny - 1 && P.vbc[WF_FACE_YN] == WF_BND_SYMMETRY) ||
+           (z == 0 && P.vbc[WF_FACE_Z0] == WF_BND_SYMMETRY) ||
+           (z == P.nz - 1 && P.vbc[WF_FACE_ZN] == WF_BND_SYMMETRY);
+}
+
 // Where a four-cells-per-thread kernel applies: the switch (Params::vec4),
 // nx % 4 == 0 and 16-byte aligned planes.
 inline bool quad_ok(const Params& P, std::initializer_list<const void*> ptrs) {

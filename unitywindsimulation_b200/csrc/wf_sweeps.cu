@@ -127,7 +127,10 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
     const int iE = x + 1 < P.nx ? i + 1 : i, iW = x > 0 ? i - 1 : i;
     const int iN = y + 1 < P.ny ? i + sx : i, iS = y > 0 ? i - sx : i;
     const int iU = z + 1 < P.nz ? i + sz : i, iDn = z > 0 ? i - sz : i;
-    const float d0 = ld(iD, i), d1 = ld(iD, N + i), d2 = ld(iD, 2 * N + i);
+    // 1/D: the first component stands for all three outside d_split cells,
+    // read there from one address (an L1 hit) so no load waits on a branch
+    const size_t o1 = d_split(P, x, x, y, z) ? N : 0;
+    const float d0 = ld(iD, i), d1 = ld(iD, o1 + i), d2 = ld(iD, 2 * o1 + i);
     const float a0 = ld(A, i), a1 = ld(A, N + i), a2 = ld(A, 2 * N + i);
     const float a3 = ld(A, 3 * N + i), a4 = ld(A, 4 * N + i), a5 = ld(A, 5 * N + i);
     float r[3];
@@ -179,7 +182,11 @@ __global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Para
     const int iN = y + 1 < P.ny ? i + sx : i, iS = y > 0 ? i - sx : i;
     const int iU = z + 1 < P.nz ? i + sz : i, iDn = z > 0 ? i - sz : i;
     const int iE = x0 + 4 < P.nx ? i + 4 : i + 3, iW = x0 > 0 ? i - 1 : i;
-    const float4 dd[3] = {ld4(iD, i), ld4(iD, N + i), ld4(iD, 2 * N + i)};
+    // 1/D: the first component stands for all three outside d_split cells,
+    // read there from one address (an L1 hit, 8 of the 73 bytes a cell would
+    // otherwise move) so no load waits on a branch
+    const size_t o1 = d_split(P, x0, x0 + 3, y, z) ? N : 0;
+    const float4 dd[3] = {ld4(iD, i), ld4(iD, o1 + i), ld4(iD, 2 * o1 + i)};
     const float4 aE = ld4(A, i), aW = ld4(A, N + i), aN = ld4(A, 2 * N + i);
     const float4 aS = ld4(A, 3 * N + i), aU = ld4(A, 4 * N + i), aD = ld4(A, 5 * N + i);
     float4 c[3], n[3], so[3], up[3], dn[3], bb[3];
