@@ -16,6 +16,7 @@
  *     ChangePhysFieldPos (FvmSolverGpu.cs:1026-1032)     wf_change_phys_field_pos
  *     ChangePhysDomainSize (FvmSolverGpu.cs:1034-1046)   (re-create the handle; see below)
  *     GetVelField/GetPresField/GetFlagField (:1568-1582) wf_get_vel / wf_get_pres / wf_get_flags
+ *     gridType CollNonUniform + InitMeshBuffers (:682-788) wf_set_face_positions
  *
  * Conventions
  *   - Axes follow the reference: x streamwise, y vertical (ground at y = 0),
@@ -151,6 +152,27 @@ int wf_init_vel_pres_fields(wf_solver* h);
 int wf_set_fixed_value_vel_bnd_cond(wf_solver* h, float wind_speed);
 /* ChangePhysFieldPos(): re-initialise the fields (FvmSolverGpu.cs:1026-1032). */
 int wf_change_phys_field_pos(wf_solver* h);
+/* Non-uniform collocated grid (FluidSimConfig.gridType = CollNonUniform,
+ * FvmSolverGpu.cs:185-205; mesh buffers facePosX/Y/Z of InitMeshBuffers,
+ * :682-788).  face_x[nx+1], face_y[ny+1], face_z[nz+1]: strictly increasing
+ * face positions (cell x spans face_x[x]..face_x[x+1]).  From the next call
+ * on, the step runs FvmCollNonUniform.compute's kernels (momentum and
+ * pressure pre-computes, Jacobi sweeps, velocity correction), and
+ * wf_init_vel_pres_fields / wf_set_fixed_value_vel_bnd_cond place a log
+ * profile at the cells' centre heights (CSInitLogVelPresFieldsNonUniform,
+ * CSSetLogVelBndCondNonUniform, InitShaderColl.compute:134-154,287-300);
+ * call them after this, as the reference's constructor builds the mesh
+ * before the fields.  The face-flux texture starts at zero and is bound
+ * for the momentum kernels, which the reference leaves out (:1160,1196
+ * are commented out).  SIMPLE without a turbulence model only
+ * (WF_ERR_UNSUPPORTED otherwise); batches and the adjoint take uniform
+ * grids only.  All three NULL: back to the uniform grid. */
+int wf_set_face_positions(wf_solver* h, const float* face_x, const float* face_y, const float* face_z);
+/* The face-flux texture of the non-uniform grid (velFaceFluxField,
+ * FvmSolverGpu.cs:275, written by CSPresCorrectRhieChowPreCompute,
+ * FvmCollNonUniform.compute:1335-1341): three planes (x, y, z components)
+ * of (nx+1)*(ny+1)*(nz+1) texels, x fastest. */
+int wf_get_face_flux(wf_solver* h, float* out);
 /* InitVelPresFieldsFromBackGroundFlow (FvmSolverGpu.cs:898-929, kernel
  * CSInitVelPresFieldsFromBGFlowRotate, InitShaderColl.compute:185-226): sets
  * every cell's velocity (all iterate buffers) and pressure to the

@@ -207,6 +207,8 @@ def load_ref():
         "wfr_init_vel_pres_fields": (c_int, [c_void_p, c_float]),
         "wfr_set_fixed_value_vel_bnd_cond": (c_int, [c_void_p, c_float]),
         "wfr_init_from_background": (c_int, [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float), c_float]),
+        "wfr_set_face_positions": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
+        "wfr_get_face_flux": (c_int, [c_void_p, POINTER(c_float)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -321,6 +323,24 @@ class RefSolver:
     def Step(self, n_steps: int = 1) -> bool:
         self._ok(self._lib.wfr_step(self._h, int(n_steps)))
         return True
+
+    def set_face_positions(self, fx, fy, fz):
+        """Non-uniform collocated grid (gridType CollNonUniform) with face
+        positions fx[nx+1], fy[ny+1], fz[nz+1]; all None: uniform grid."""
+        if fx is None and fy is None and fz is None:
+            self._ok(self._lib.wfr_set_face_positions(self._h, None, None, None))
+            return
+        a = [np.ascontiguousarray(v, dtype=np.float32) for v in (fx, fy, fz)]
+        self._keep_fpos = a
+        self._ok(self._lib.wfr_set_face_positions(self._h, *[v.ctypes.data_as(POINTER(c_float)) for v in a]))
+
+    def get_face_flux(self) -> np.ndarray:
+        """velFaceFluxField: (3, nz+1, ny+1, nx+1)."""
+        c = self.cfg
+        m = (c.nx + 1) * (c.ny + 1) * (c.nz + 1)
+        out = np.empty(3 * m, dtype=np.float32)
+        self._ok(self._lib.wfr_get_face_flux(self._h, out.ctypes.data_as(POINTER(c_float))))
+        return out.reshape(3, c.nz + 1, c.ny + 1, c.nx + 1)
 
     def GetVelField(self):
         return self.get_field(1).reshape((3,) + self.shape)

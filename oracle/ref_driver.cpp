@@ -51,6 +51,10 @@ namespace ref_fvm {
 using namespace hlsl;
 #include "_ref/fvm.inc"
 }  // namespace ref_fvm
+namespace ref_fvmnu {
+using namespace hlsl;
+#include "_ref/fvmnu.inc"
+}  // namespace ref_fvmnu
 namespace ref_piso {
 using namespace hlsl;
 #include "_ref/piso.inc"
@@ -90,6 +94,12 @@ struct wfr_solver {
     std::vector<int> flag;
     float4 *vel, *velLastTime, *velLastIter, *velCorrect, *aodu, *D, *b, *face;
     float *pres, *pc, *pcLastIter, *Dp, *bp, *eddy;
+    // Non-uniform collocated grid (gridType CollNonUniform): face positions
+    // (facePosX/Y/Z, nx+1 / ny+1 / nz+1 entries, FvmSolverGpu.cs:682-788)
+    // and velFaceFluxFieldTex ((nx+1)(ny+1)(nz+1) float3, :275).
+    bool nonuniform = false;
+    std::vector<float> fpx, fpy, fpz;
+    std::vector<hlsl::float3> flux;
 };
 
 namespace {
@@ -122,6 +132,30 @@ void set_uniforms(const wfr_solver& s) {
         dx = s.dx;
         ds = s.ds;
         dv = s.dv;
+        nu = s.nu;
+        den = c.den;
+        externalForce = hlsl::float3(c.ext_force[0], c.ext_force[1], c.ext_force[2]);
+        numGroups = int3((s.nx + 7) / 8, (s.ny + 7) / 8, (s.nz + 7) / 8);
+        useLES = c.turbulence == WF_TURB_SMAGORINSKY;
+        velBndTypeX0 = c.vel_bc[WF_FACE_X0];
+        velBndTypeXn = c.vel_bc[WF_FACE_XN];
+        velBndTypeY0 = c.vel_bc[WF_FACE_Y0];
+        velBndTypeYn = c.vel_bc[WF_FACE_YN];
+        velBndTypeZ0 = c.vel_bc[WF_FACE_Z0];
+        velBndTypeZn = c.vel_bc[WF_FACE_ZN];
+        presBndTypeX0 = c.pres_bc[WF_FACE_X0];
+        presBndTypeXn = c.pres_bc[WF_FACE_XN];
+        presBndTypeY0 = c.pres_bc[WF_FACE_Y0];
+        presBndTypeYn = c.pres_bc[WF_FACE_YN];
+        presBndTypeZ0 = c.pres_bc[WF_FACE_Z0];
+        presBndTypeZn = c.pres_bc[WF_FACE_ZN];
+    }
+    {
+        // InitFvmNonUniformShader (FvmSolverGpu.cs:446-480): the same
+        // uniforms without dx/ds/dv, which the kernels take from facePos.
+        using namespace ref_fvmnu;
+        gridRes = res;
+        dt = c.dt;
         nu = s.nu;
         den = c.den;
         externalForce = hlsl::float3(c.ext_force[0], c.ext_force[1], c.ext_force[2]);
@@ -249,6 +283,36 @@ void bind_all(wfr_solver& s) {
         AodUCorrectField.bind(s.aodu, X, Y, Z);
         eddyVisField.bind(s.eddy, X, Y, Z);
         faceEddyVisField.bind(s.face, X, Y, Z);
+        bind_bnd(s, bndFieldX0, bndFieldXn, bndFieldY0, bndFieldYn, bndFieldZ0, bndFieldZn);
+    }
+    {
+        // The non-uniform shader.  velFaceFluxField is bound for every
+        // kernel here; see set_face_positions for the binding the reference
+        // leaves out.
+        using namespace ref_fvmnu;
+        velField.bind(s.vel, X, Y, Z);
+        velFieldLastTime.bind(s.velLastTime, X, Y, Z);
+        velFieldLastIter.bind(s.velLastIter, X, Y, Z);
+        velCorrectField.bind(s.velCorrect, X, Y, Z);
+        presFieldLastTime.bind(s.pres, X, Y, Z);
+        presCorrectField.bind(s.pc, X, Y, Z);
+        presCorrectFieldLastIter.bind(s.pcLastIter, X, Y, Z);
+        flagField.bind(s.flag.data(), X, Y, Z);
+        DField.bind(s.D, X, Y, Z);
+        bField.bind(s.b, X, Y, Z);
+        DFieldPresCorrect.bind(s.Dp, X, Y, Z);
+        bFieldPresCorrect.bind(s.bp, X, Y, Z);
+        AodUCorrectField.bind(s.aodu, X, Y, Z);
+        eddyVisField.bind(s.eddy, X, Y, Z);
+        if (s.nonuniform) {
+            velFaceFluxField.bind(s.flux.data(), X + 1, Y + 1, Z + 1);
+            facePosX.p = s.fpx.data();
+            facePosX.n = s.fpx.size();
+            facePosY.p = s.fpy.data();
+            facePosY.n = s.fpy.size();
+            facePosZ.p = s.fpz.data();
+            facePosZ.n = s.fpz.size();
+        }
         bind_bnd(s, bndFieldX0, bndFieldXn, bndFieldY0, bndFieldYn, bndFieldZ0, bndFieldZn);
     }
     {
@@ -380,6 +444,59 @@ void piso_correction(wfr_solver& s) {  // PisoCorrection, :1482-1535
     set_pres_correct_to_zero(s);
 }
 
+// The same stages over the non-uniform shader (gridType CollNonUniform):
+// _VelPredictPreCompute / _VelPredictCollAccelerated (:1149-1168,
+// :1185-1203), _PresCorrectPreCompute / _PresCorrectCollAccelerated
+// (:1284-1330), PresCorrect's apply and normalisation (:1367-1439) and
+// ApplyVelCorrection (:1441-1480).  SIMPLE without turbulence only (see
+// wfr_set_face_positions).
+void vel_predict_nu(wfr_solver& s) {
+    bind_all(s);
+    dispatch(res_of(s), [](uint3 id) { ref_fvmnu::CSVelPredictPreCompute(id); });
+    for (int k = 0; k < s.cfg.vel_iters; ++k) {
+        bind_all(s);
+        dispatch(res_of(s), [](uint3 id) { ref_fvmnu::CSVelPredict(id); });
+        std::swap(s.velLastIter, s.vel);
+    }
+    std::swap(s.velLastIter, s.vel);
+}
+
+void pres_correct_nu(wfr_solver& s) {
+    bind_all(s);
+    dispatch(res_of(s), [](uint3 id) { ref_fvmnu::CSPresCorrectRhieChowPreCompute(id); });
+    for (int k = 0; k < s.cfg.pres_iters; ++k) {
+        bind_all(s);
+        dispatch(res_of(s), [](uint3 id) { ref_fvmnu::CSPresCorrectRhieChow(id); });
+        std::swap(s.pcLastIter, s.pc);
+    }
+    std::swap(s.pcLastIter, s.pc);
+    bind_all(s);
+    dispatch(res_of(s), [](uint3 id) { ref_fvmnu::CSApplyPresCorrection(id); });
+    if (!has_fixed_pressure(s.cfg)) {
+        const uint3 ref_cell(2u, (unsigned)(s.ny / 2), 2u);
+        const int gx = (s.nx + 7) / 8 * 8, gy = (s.ny + 7) / 8 * 8, gz = (s.nz + 7) / 8 * 8;
+        for (int z = 0; z < gz; ++z)
+            for (int y = 0; y < gy; ++y)
+                for (int x = 0; x < gx; ++x) {
+                    const uint3 id((unsigned)x, (unsigned)y, (unsigned)z);
+                    if (id.x == ref_cell.x && id.y == ref_cell.y && id.z == ref_cell.z) continue;
+                    ref_fvmnu::CSPresNormalization(id);
+                }
+        ref_fvmnu::CSPresNormalization(ref_cell);
+    }
+}
+
+void step_once_nu(wfr_solver& s) {
+    set_uniforms(s);
+    vel_predict_nu(s);
+    pres_correct_nu(s);
+    bind_all(s);
+    dispatch(res_of(s), [](uint3 id) { ref_fvmnu::CSApplyVelCorrectionDivergenceTheorem(id); });
+    set_pres_correct_to_zero(s);
+    std::swap(s.velLastTime, s.vel);
+    copy_vel_field(s, s.velLastIter, s.velLastTime);
+}
+
 void step_once(wfr_solver& s) {  // Step, :1050-1121, every stage finishing in one call
     set_uniforms(s);
     if (s.cfg.turbulence == WF_TURB_SMAGORINSKY) {
@@ -411,21 +528,35 @@ void bind_init(wfr_solver& s) {
     flagField.bind(s.flag.data(), X, Y, Z);
     faceEddyVisField.bind(s.face, X, Y, Z);
     bind_bnd(s, bndFieldX0, bndFieldXn, bndFieldY0, bndFieldYn, bndFieldZ0, bndFieldZn);
+    facePosX.p = s.nonuniform ? s.fpx.data() : nullptr;
+    facePosX.n = s.fpx.size();
+    facePosY.p = s.nonuniform ? s.fpy.data() : nullptr;
+    facePosY.n = s.fpy.size();
+    facePosZ.p = s.nonuniform ? s.fpz.data() : nullptr;
+    facePosZ.n = s.fpz.size();
 }
 
-void init_vel_pres_fields(wfr_solver& s) {  // InitVelPresFields, :786-860 (collocated)
+// InitVelPresFields, :786-860; on the non-uniform grid the log profile is
+// CSInitLogVelPresFieldsNonUniform (:835-876, kernel looked up at :329-332).
+void init_vel_pres_fields(wfr_solver& s) {
     set_uniforms(s);
     bind_init(s);
-    if (s.cfg.inflow_type == WF_INFLOW_LOG)
+    if (s.cfg.inflow_type == WF_INFLOW_LOG && s.nonuniform)
+        dispatch(res_of(s), [](uint3 id) { ref_init::CSInitLogVelPresFieldsNonUniform(id); });
+    else if (s.cfg.inflow_type == WF_INFLOW_LOG)
         dispatch(res_of(s), [](uint3 id) { ref_init::CSInitLogVelPresFields(id); });
     else
         dispatch(res_of(s), [](uint3 id) { ref_init::CSInitVelPresFields(id); });
 }
 
-void set_fixed_value_vel_bnd_cond(wfr_solver& s) {  // SetFixedValueVelBndCond, :998-1022
+// SetFixedValueVelBndCond, :998-1022 (CSSetLogVelBndCondNonUniform on the
+// non-uniform grid, :338-341).
+void set_fixed_value_vel_bnd_cond(wfr_solver& s) {
     set_uniforms(s);
     bind_init(s);
-    if (s.cfg.inflow_type == WF_INFLOW_LOG)
+    if (s.cfg.inflow_type == WF_INFLOW_LOG && s.nonuniform)
+        dispatch(res_of(s), [](uint3 id) { ref_init::CSSetLogVelBndCondNonUniform(id); });
+    else if (s.cfg.inflow_type == WF_INFLOW_LOG)
         dispatch(res_of(s), [](uint3 id) { ref_init::CSSetLogVelBndCond(id); });
     else
         dispatch(res_of(s), [](uint3 id) { ref_init::CSSetFixedValueVelBndCond(id); });
@@ -664,7 +795,61 @@ int wfr_get_field(wfr_solver* s, int field, float* out) {
 
 int wfr_step(wfr_solver* s, int n_steps) {
     if (!s || n_steps < 0) return WF_ERR_INVALID_ARG;
-    for (int i = 0; i < n_steps; ++i) step_once(*s);
+    for (int i = 0; i < n_steps; ++i) {
+        if (s->nonuniform)
+            step_once_nu(*s);
+        else
+            step_once(*s);
+    }
+    return WF_OK;
+}
+
+/* Switches the solver to the non-uniform collocated grid (gridType
+ * CollNonUniform): face positions fx[nx+1], fy[ny+1], fz[nz+1], strictly
+ * increasing (InitMeshBuffers, FvmSolverGpu.cs:682-788, fills the same
+ * buffers from a hard-coded stretching pattern).  All three NULL returns to
+ * the uniform grid.  The face-flux texture starts at zero.
+ *
+ * Binding.  The reference binds velFaceFluxField only for the pressure
+ * pre-compute, which writes it (:1295); the two momentum kernels that read
+ * it (FvmCollNonUniform.compute:204-335, 799-841) have their SetTexture calls
+ * commented out (:1160, :1196).  Here the texture is bound for them too, so
+ * that the momentum equation sees the face fluxes of the last pressure
+ * pre-compute, the intended data flow.  Only SIMPLE without turbulence is
+ * replayed: the reference pairs PISO and LES with the uniform-grid shaders'
+ * constant dx. */
+int wfr_set_face_positions(wfr_solver* s, const float* fx, const float* fy, const float* fz) {
+    if (!s) return WF_ERR_INVALID_ARG;
+    if (!fx && !fy && !fz) {
+        s->nonuniform = false;
+        return WF_OK;
+    }
+    if (!fx || !fy || !fz) return WF_ERR_INVALID_ARG;
+    if (s->cfg.solver_type != WF_SOLVER_SIMPLE || s->cfg.turbulence != WF_TURB_NONE) return WF_ERR_UNSUPPORTED;
+    auto ok = [](const float* f, int n) {
+        for (int i = 0; i < n; ++i)
+            if (!(f[i + 1] > f[i])) return false;
+        return true;
+    };
+    if (!ok(fx, s->nx) || !ok(fy, s->ny) || !ok(fz, s->nz)) return WF_ERR_INVALID_ARG;
+    s->fpx.assign(fx, fx + s->nx + 1);
+    s->fpy.assign(fy, fy + s->ny + 1);
+    s->fpz.assign(fz, fz + s->nz + 1);
+    s->flux.assign((size_t)(s->nx + 1) * (s->ny + 1) * (s->nz + 1), hlsl::float3());
+    s->nonuniform = true;
+    return WF_OK;
+}
+
+/* The face-flux texture, three planes (x, y, z components) of
+ * (nx+1)*(ny+1)*(nz+1) points, x fastest. */
+int wfr_get_face_flux(wfr_solver* s, float* out) {
+    if (!s || !out || !s->nonuniform) return WF_ERR_INVALID_ARG;
+    const size_t m = s->flux.size();
+    for (size_t i = 0; i < m; ++i) {
+        out[i] = s->flux[i].x;
+        out[m + i] = s->flux[i].y;
+        out[2 * m + i] = s->flux[i].z;
+    }
     return WF_OK;
 }
 

@@ -1,5 +1,8 @@
 """Build recipe: the reference's own hot-path compute shaders as C++.
 
+The non-uniform collocated shader (FvmCollNonUniform.compute) is translated
+beside the uniform one.
+
 Reads the shader sources where they lie in the reference checkout and writes
 C++ translations into oracle/_ref/ (never committed): the HLSL subset these
 kernels use maps onto oracle/hlsl_shim.h after a few textual rewrites
@@ -21,6 +24,7 @@ OUT = os.path.join(HERE, "_ref")
 SHADER_DIR = "Assets/Resources/Shaders"
 SHADERS = {
     "fvm": "SimShaders/FvmColl.compute",
+    "fvmnu": "SimShaders/FvmCollNonUniform.compute",
     "piso": "SimShaders/PisoColl.compute",
     "les": "LESShaders/LES.compute",
     "wall": "WallFuncShaders/WallFunc.compute",

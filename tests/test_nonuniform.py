@@ -1,0 +1,181 @@
+"""Non-uniform collocated grid (gridType CollNonUniform).
+
+Parity is pinned on the reference's own kernels: FvmCollNonUniform.compute
+and InitShaderColl.compute translated to C++ (oracle/ref_kernels.py) and
+replayed in FvmSolverGpu's order (oracle/ref_driver.cpp), recorded in
+tests/golden/nonuniform_ref.npz by tests/golden/make_nu_golden.py.  The
+CUDA library must match every recorded field within REL_TOL = 1e-5 relative
+L2 per field and step.  The mesh generator restates InitMeshBuffers
+(FvmSolverGpu.cs:682-788).
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from unitywindsimulation_b200 import _lib, cases
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import make_nu_golden as G  # noqa: E402
+
+from helpers import REL_TOL, rel_l2  # noqa: E402
+
+FIXTURE = np.load(G.FIXTURE)
+
+
+# ---- mesh (CPU) -------------------------------------------------------------
+
+def test_wind_tunnel_mesh_follows_init_mesh_buffers():
+    """WindTunnelBoxConfig: 25 cells growing by 1.08 towards x0 (largest at
+    the boundary), 50 cells of dx = 1, then 25 cells growing away from the
+    core; y uniform."""
+    fx = cases.stretched_faces(100, 1.0, 50, 25)
+    d = np.diff(fx.astype(np.float64))
+    assert fx[0] == 0.0 and np.all(d > 0)
+    sizes = np.empty(25, dtype=np.float32)
+    sizes[0] = 1.0
+    for i in range(1, 25):
+        sizes[i] = np.float32(sizes[i - 1] * np.float32(1.08))
+    np.testing.assert_allclose(d[:25], sizes[::-1], rtol=0, atol=4e-5)  # differences of FP32 sums
+    np.testing.assert_allclose(d[25:75], 1.0, rtol=0, atol=4e-5)
+    np.testing.assert_allclose(d[75:], sizes, rtol=0, atol=4e-5)
+    fy = cases.stretched_faces(50, 1.0, 50, 0)
+    assert np.array_equal(fy, np.arange(51, dtype=np.float32))
+
+
+def test_mesh_upper_side_reuses_lower_sizes():
+    """The upper side takes the lower side's sizes (FvmSolverGpu.cs:758-762):
+    a longer upper side has no sizes to take."""
+    f = cases.stretched_faces(10, 0.5, 6, 3)
+    d = np.diff(f)
+    assert np.allclose(d[:3], [0.5 * 1.08 ** 2, 0.5 * 1.08, 0.5], rtol=1e-6)
+    assert np.allclose(d[9:], [0.5], rtol=1e-6)
+    with pytest.raises(ValueError):
+        cases.stretched_faces(10, 0.5, 4, 2)  # 4 upper cells, 2 lower sizes
+
+
+def test_fixture_covers_cases():
+    for name in G.CASES:
+        assert f"{name}/0/vel" in FIXTURE.files
+        for k in range(1, G.STEPS + 1):
+            for key in ("vel", "pres", "flux"):
+                a = FIXTURE[f"{name}/{k}/{key}"]
+                assert np.isfinite(a).all() and np.abs(a).max() > 0.01, (name, k, key)
+        for key, _ in G.LAST_FIELDS:
+            assert np.isfinite(FIXTURE[f"{name}/{G.STEPS}/{key}"]).all()
+
+
+def test_reference_kernels_reproduce_fixture():
+    """Where the translated kernels are built (the reference checkout is
+    present), they reproduce the committed fixture bit for bit."""
+    from oracle.binding import RefSolver, ref_available
+    if not ref_available():
+        pytest.skip("reference kernels not built (oracle/_ref)")
+    for name in G.CASES:
+        got = {}
+
+        def rec(step, key, a):
+            got[f"{name}/{step}/{key}"] = a
+        G.run_case(lambda cfg: RefSolver(cfg), name, rec)
+        for k, a in got.items():
+            assert np.array_equal(a, FIXTURE[k]), k
+
+
+def test_reference_kernels_reject_piso_and_les():
+    from oracle.binding import RefSolver, ref_available
+    if not ref_available():
+        pytest.skip("reference kernels not built (oracle/_ref)")
+    case = cases.small_nonuniform_case()
+    cfg = case.cfg.copy()
+    cfg.solver_type = _lib.SOLVER_PISO
+    r = RefSolver(cfg)
+    with pytest.raises(RuntimeError):
+        r.set_face_positions(*case.faces)
+
+
+# ---- CUDA library against the fixture (GPU) --------------------------------
+
+def _cuda(**over):
+    from unitywindsimulation_b200.solver import FvmSolverCuda
+
+    def make(cfg):
+        c = cfg.copy()
+        for k, v in over.items():
+            setattr(c, k, v)
+        return FvmSolverCuda(c)
+    return make
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(G.CASES))
+def test_cuda_matches_reference_kernels(name):
+    got = {}
+
+    def rec(step, key, a):
+        got[f"{name}/{step}/{key}"] = a
+    G.run_case(_cuda(), name, rec)
+    assert set(got) == {k for k in FIXTURE.files if k.startswith(name + "/")}
+    for k, a in got.items():
+        err = rel_l2(a, FIXTURE[k])
+        assert err <= REL_TOL, (k, err)
+
+
+@pytest.mark.gpu
+def test_graph_replay_equals_eager_steps():
+    name = "const_tunnel"
+    outs = []
+    for graph in (1, 0):
+        got = {}
+
+        def rec(step, key, a):
+            got[f"{step}/{key}"] = a
+        G.run_case(_cuda(use_graph=graph), name, rec)
+        outs.append(got)
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+@pytest.mark.gpu
+def test_residual_path_runs_the_same_sweeps():
+    """calc_residual with tolerances no sweep reaches: the loop with residual
+    reads gives the same fields as the plain loop."""
+    name = "log_urban_normalised"
+    outs = []
+    for resid in (0, 1):
+        got = {}
+
+        def rec(step, key, a):
+            got[f"{step}/{key}"] = a
+        over = dict(calc_residual=resid)
+        if resid:
+            over.update(vel_tol=0.0, pres_tol=0.0, vel_res_interval=3, pres_res_interval=5)
+        G.run_case(_cuda(**over), name, rec)
+        outs.append(got)
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+@pytest.mark.gpu
+def test_unsupported_combinations_are_refused():
+    from unitywindsimulation_b200.solver import FvmSolverCuda
+    from unitywindsimulation_b200._lib import WindFvmError
+    case = cases.small_nonuniform_case()
+    for over in (dict(solver_type=_lib.SOLVER_PISO), dict(turbulence=_lib.TURB_SMAGORINSKY)):
+        cfg = case.cfg.copy()
+        for k, v in over.items():
+            setattr(cfg, k, v)
+        s = FvmSolverCuda(cfg)
+        with pytest.raises(WindFvmError):
+            s.set_face_positions(*case.faces)
+    s = FvmSolverCuda(case.cfg)
+    with pytest.raises(WindFvmError):
+        s.set_face_positions(case.faces[0][::-1].copy(), case.faces[1], case.faces[2])  # decreasing
+    s.set_face_positions(*case.faces)
+    from unitywindsimulation_b200.adjoint import AdjointSolver
+    with pytest.raises(WindFvmError):
+        AdjointSolver(s)
+    s.set_face_positions(None, None, None)  # back to the uniform grid
+    s.Step(1)

@@ -19,6 +19,8 @@ Workloads (synthetic, seeded):
                   buildings each, wind rotated by k * 22.5 degrees
   adjoint_street  128 x 64(up) x 96, 12 soft buildings with continuous heights
   adjoint_batch   8 directions x 256 x 96(up) x 256, 64 soft buildings
+  wind_tunnel     100 x 50(up) x 100 on the reference's non-uniform mesh
+                  (Assets/Code/Config/WindTunnelBoxConfig.asset)
 """
 from __future__ import annotations
 
@@ -45,6 +47,7 @@ class Case:
     seed: int | None = None
     buildings: list = dataclasses.field(default_factory=list)  # (x0, x1, z0, z1, height[, angle])
     soft: SoftBuildings | None = None  # soft building mask (drag field), all cells fluid
+    faces: tuple | None = None         # (fx, fy, fz) face positions of a non-uniform grid
 
     @property
     def n_cells(self) -> int:
@@ -377,9 +380,105 @@ def small_soft_case(nx=24, ny=12, nz=16, piso=True, seed=0, nv=6, np_=8, buildin
     return Case(f"small_soft_{nx}x{ny}x{nz}_s{seed}", base.cfg, base.flags, None, 1, seed, [], soft)
 
 
+def stretched_faces(n: int, dx: float, n_uniform: int, n_side: int, ratio: float = 1.08) -> np.ndarray:
+    """Face positions (n + 1, float32) of one axis of the reference's
+    non-uniform mesh (InitMeshBuffers, FvmSolverGpu.cs:682-788): n_side cells
+    growing by `ratio` towards the lower boundary, n_uniform cells of dx,
+    then n - n_uniform - n_side cells towards the upper boundary.  The
+    reference sizes the upper side from the lower side's array too
+    (:758-762), so that side may not be longer than n_side; it fails there
+    with an index error, this raises ValueError.  FP32 throughout, as the
+    reference's float arrays."""
+    n_upper = n - n_uniform - n_side
+    if n_uniform < 0 or n_side < 0 or n_upper < 0 or n_upper > n_side:
+        raise ValueError(f"{n} cells cannot be split as {n_side} + {n_uniform} + {n_upper} "
+                         f"(the upper side reuses the lower side's {n_side} sizes)")
+    d = np.float32(dx)
+    r = np.float32(ratio)
+    sizes = np.zeros(n_side, dtype=np.float32)
+    if n_side > 0:
+        sizes[0] = d
+        for i in range(1, n_side):
+            sizes[i] = np.float32(sizes[i - 1] * r)
+    f = np.zeros(n + 1, dtype=np.float32)
+    for i in range(1, n_side + 1):                    # largest cell at the boundary
+        f[i] = np.float32(f[i - 1] + sizes[n_side - i])
+    for i in range(n_side + 1, n_side + n_uniform + 1):
+        f[i] = np.float32(f[i - 1] + d)
+    for i in range(n_side + n_uniform + 1, n + 1):    # :758-762
+        f[i] = np.float32(f[i - 1] + sizes[i - (n_side + n_uniform + 1)])
+    return f
+
+
+def wind_tunnel(nv: int = 800, np_: int = 2000, steps: int = 1) -> Case:
+    """The reference's non-uniform grid case, Assets/Code/Config/
+    WindTunnelBoxConfig.asset: 100 x 50(up) x 100 cells (physDomainSize
+    100 x 50 x 100, gridResX 100, so dx = 1), gridType CollNonUniform with
+    the mesh InitMeshBuffers builds (uniform core 50 x 50 x 50, 25 cells per
+    side in x and z growing by 1.08, none in y), dt 0.02, mu 1, den 1,
+    SIMPLE, no turbulence model, constant inflow at RuntimeConfig.windSpeed
+    10 m/s, velocity BCs X0 fixed, Xn zero-gradient, the rest symmetry;
+    pressure X0 zero-gradient, Xn fixed, the rest symmetry; velMaxNumIter
+    800, presMaxNumIter 2000, and the box of CSInitBoxFlag (x 20..24,
+    y 0..8, z 18..22, InitShaderColl.compute:320; solidType Box)."""
+    nx, ny, nz = 100, 50, 100
+    cfg = default_config(nx=nx, ny=ny, nz=nz, dx=1.0, dt=0.02, mu=1.0, den=1.0,
+                         solver_type=_lib.SOLVER_SIMPLE, turbulence=_lib.TURB_NONE,
+                         inflow_type=_lib.INFLOW_CONSTANT, wind_speed=10.0, vel_iters=nv, pres_iters=np_)
+    vel = {_lib.FACE_X0: _lib.BND_FIXED_VALUE, _lib.FACE_XN: _lib.BND_ZERO_GRAD}
+    pres = {_lib.FACE_X0: _lib.BND_ZERO_GRAD, _lib.FACE_XN: _lib.BND_FIXED_VALUE}
+    for f in range(6):
+        cfg.vel_bc[f] = vel.get(f, _lib.BND_SYMMETRY)
+        cfg.pres_bc[f] = pres.get(f, _lib.BND_SYMMETRY)
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    flags[18:22, 0:8, 20:24] = 1
+    faces = (stretched_faces(nx, 1.0, 50, 25), stretched_faces(ny, 1.0, 50, 0), stretched_faces(nz, 1.0, 50, 25))
+    return Case("wind_tunnel", cfg, flags, None, steps, None, [(20, 24, 18, 22, 8)], None, faces)
+
+
+def small_nonuniform_case(nx=16, ny=10, nz=12, log_inflow=False, seed=0, nv=8, np_=12) -> Case:
+    """Small non-uniform case for parity tests: stretched x (4 + 8 + 4
+    cells), y (2 + 6 + 2) and z (3 + 6 + 3) axes of 0.5 m cores, one box.
+    log_inflow=False: the wind-tunnel boundary set with a constant 3 m/s
+    inflow; True: the urban set (no-slip ground, symmetry top and sides)
+    with a log inflow and no fixed-pressure face (the pressure is
+    normalised)."""
+    rng = np.random.default_rng(seed)
+    dx = 0.5
+    cfg = default_config(nx=nx, ny=ny, nz=nz, dx=dx, mu=0.01, den=1.0, solver_type=_lib.SOLVER_SIMPLE,
+                         turbulence=_lib.TURB_NONE, vel_iters=nv, pres_iters=np_)
+    if log_inflow:
+        cfg.inflow_type = _lib.INFLOW_LOG
+        cfg.wind_speed = 4.0
+        cfg.inflow_kappa, cfg.inflow_z0, cfg.inflow_href = 0.4, 1.0, 10.0
+        cfg.pres_bc[_lib.FACE_XN] = _lib.BND_ZERO_GRAD
+    else:
+        cfg.inflow_type = _lib.INFLOW_CONSTANT
+        cfg.wind_speed = 3.0
+        vel = {_lib.FACE_X0: _lib.BND_FIXED_VALUE, _lib.FACE_XN: _lib.BND_ZERO_GRAD}
+        pres = {_lib.FACE_X0: _lib.BND_ZERO_GRAD, _lib.FACE_XN: _lib.BND_FIXED_VALUE}
+        for f in range(6):
+            cfg.vel_bc[f] = vel.get(f, _lib.BND_SYMMETRY)
+            cfg.pres_bc[f] = pres.get(f, _lib.BND_SYMMETRY)
+    cfg.dt = cfl_dt(6.0, dx)
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    x0 = int(rng.integers(4, 8))
+    z0_ = int(rng.integers(3, 6))
+    h = int(rng.integers(2, 5))
+    flags[z0_:z0_ + 3, 0:h, x0:x0 + 2] = 1
+    faces = (stretched_faces(nx, dx, 8, 4), stretched_faces(ny, dx, 6, 2), stretched_faces(nz, dx, 6, 3))
+    name = f"small_nu_{nx}x{ny}x{nz}_{'log' if log_inflow else 'const'}_s{seed}"
+    return Case(name, cfg, flags, None, 1, seed, [(x0, x0 + 2, z0_, z0_ + 3, h)], None, faces)
+
+
 def apply_case(solver, case: Case) -> None:
-    """Reference set-up order: flags after the fields (FvmSolverController.cs:
-    368-375), then the inlet plane."""
+    """Reference set-up order: the mesh first (InitMeshBuffers before
+    InitVelPresFields, FvmSolverGpu.cs:204-213), flags after the fields
+    (FvmSolverController.cs:368-375), then the inlet plane."""
+    if case.faces is not None:
+        solver.set_face_positions(*case.faces)
+        solver.InitVelPresFields()
+        solver.SetFixedValueVelBndCond()
     solver.InitFlags(case.flags)
     if case.inlet is not None:
         solver.set_inflow_plane(case.inlet)
@@ -393,4 +492,5 @@ WORKLOADS = {
     "urban_block": urban_block,
     "adjoint_street": adjoint_street,
     "aij_building": aij_building,
+    "wind_tunnel": wind_tunnel,
 }

@@ -1118,6 +1118,7 @@ int wf_adj_create(wf_solver* h, wf_adjoint** out) {
     if (!h || !out) return WF_ERR_INVALID_ARG;
     *out = nullptr;
     if (h->P.les) return WF_ERR_UNSUPPORTED;
+    if (h->nonuniform) return WF_ERR_UNSUPPORTED;  // the uniform-grid step is differentiated
     if (h->cfg.calc_residual) return WF_ERR_UNSUPPORTED;  // early exits change the iteration counts
     if (h->cfg.compat_flags & WF_COMPAT_PISO_CONSISTENT) return WF_ERR_UNSUPPORTED;
     bool fixed_p = false;

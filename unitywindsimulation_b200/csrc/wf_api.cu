@@ -115,7 +115,7 @@ void free_all(wf_solver* h) {
     wf::drop_graphs(h);
     void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->vb[3], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
                     h->pcb[0], h->pcb[1], h->pcb[2], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->grad, h->part, h->dsum, h->dref,
-                    h->dbad, h->stage, h->bnd[0], h->drag, h->nbm};
+                    h->dbad, h->stage, h->bnd[0], h->drag, h->nbm, h->fpos, h->flux};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->hsum) cudaFreeHost(h->hsum);
@@ -176,6 +176,11 @@ const float* cur_inv_d(const wf_solver* h) { return h->id_gen == h->d_gen ? h->v
 
 int do_vel_precompute(wf_solver* h) {
     ++h->d_gen;
+    if (h->nonuniform) {
+        wf::launch_nu_vel_precompute(h);
+        WF_CHECK_LAUNCH();
+        return WF_OK;
+    }
     wf::launch_vel_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->pr, h->eddy, h->face,
                               h->P.les ? h->bv : nullptr, h->drag, h->Dv, h->bv);
     WF_CHECK_LAUNCH();
@@ -194,14 +199,17 @@ int do_vel_sweeps(wf_solver* h, int n, bool allow_fast) {
     const Params& P = h->P;
     const bool resid = h->cfg.calc_residual != 0;
     int k = 0;
-    if (allow_fast && h->fast && !resid && n > 0) {
+    if (allow_fast && h->fast && !resid && n > 0 && !h->nonuniform) {
         // Multi-sweep path: same buffer roles, several sweeps per launch.
         WF_TRY(wf::vel_sweeps_fast(h, n));
         return WF_OK;
     }
     for (; k < n; ++k) {
         const float* src = h->iter_alias ? h->vb[h->iT] : h->vb[h->iI];
-        wf::launch_vel_sweep(P, h->st, h->fl, src, h->vb[h->iT], h->eddy, h->face, h->Dv, h->bv, h->vb[h->iF]);
+        if (h->nonuniform)
+            wf::launch_nu_vel_sweep(h, src, h->vb[h->iF]);
+        else
+            wf::launch_vel_sweep(P, h->st, h->fl, src, h->vb[h->iT], h->eddy, h->face, h->Dv, h->bv, h->vb[h->iF]);
         WF_CHECK_LAUNCH();
         if (resid && k % h->cfg.vel_res_interval == 0) {
             wf::launch_vel_residual(P, h->st, h->Dv, h->vb[h->iF], src, h->part, h->dsum);
@@ -221,6 +229,11 @@ int do_vel_sweeps(wf_solver* h, int n, bool allow_fast) {
 }
 
 int do_pres_precompute(wf_solver* h) {
+    if (h->nonuniform) {
+        wf::launch_nu_pres_precompute(h, h->vb[h->iF]);
+        WF_CHECK_LAUNCH();
+        return WF_OK;
+    }
     wf::launch_pres_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iF], h->pr, h->Dv, cur_inv_d(h), h->Dp, h->bp);
     WF_CHECK_LAUNCH();
     return WF_OK;
@@ -230,13 +243,16 @@ int do_pres_precompute(wf_solver* h) {
 int do_pres_sweeps(wf_solver* h, int n, bool allow_fast) {
     const Params& P = h->P;
     const bool resid = h->cfg.calc_residual != 0;
-    if (allow_fast && h->fast && !resid && n > 0) {
+    if (allow_fast && h->fast && !resid && n > 0 && !h->nonuniform) {
         WF_TRY(wf::pres_sweeps_fast(h, n, /*piso=*/false));
         return WF_OK;
     }
     for (int k = 0; k < n; ++k) {
         const float* src = h->pc_zero ? nullptr : h->pcb[h->iPCL];
-        wf::launch_pres_sweep(P, h->st, h->fl, src, h->Dv, h->Dp, h->bp, h->pcb[h->iPC]);
+        if (h->nonuniform)
+            wf::launch_nu_pres_sweep(h, src, h->pcb[h->iPC]);
+        else
+            wf::launch_pres_sweep(P, h->st, h->fl, src, h->Dv, h->Dp, h->bp, h->pcb[h->iPC]);
         WF_CHECK_LAUNCH();
         h->pc_zero = false;
         if (resid && k % h->cfg.pres_res_interval == 0) {
@@ -265,6 +281,11 @@ int do_normalize(wf_solver* h) {
     return WF_OK;
 }
 int do_apply_vel(wf_solver* h) {
+    if (h->nonuniform) {
+        wf::launch_nu_apply_vel(h, pc_cur(h), h->vb[h->iF]);
+        WF_CHECK_LAUNCH();
+        return WF_OK;
+    }
     wf::launch_apply_vel(h->P, h->st, h->fl, pc_cur(h), h->Dv, cur_inv_d(h), h->uc, h->vb[h->iF]);
     WF_CHECK_LAUNCH();
     return WF_OK;
@@ -274,6 +295,7 @@ int do_apply_vel(wf_solver* h) {
 // starts from the zero state.
 int do_piso(wf_solver* h, int n, bool allow_fast) {
     const Params& P = h->P;
+    if (h->nonuniform) return set_err(h, WF_ERR_UNSUPPORTED, "PISO runs on the uniform grid only");
     wf::launch_piso_aodu(P, h->st, h->fl, h->uc, h->vb[h->iT], h->eddy, h->face, h->aodu);
     WF_CHECK_LAUNCH();
     if (allow_fast && h->fast && n > 0) {
@@ -648,8 +670,11 @@ int wf_init_vel_pres_fields(wf_solver* h) {
     const int logp = c.inflow_type == WF_INFLOW_LOG;
     const float fric = logp ? fric_vel(h) : 0.f;
     const int centre = (c.compat_flags & WF_COMPAT_INIT_PROFILE_CELL_CENTRE) != 0;
-    wf::launch_init_fields(h->P, h->st, logp, h->wind, fric, c.inflow_kappa, c.inflow_z0, centre, h->vb[0],
-                           h->vb[1], h->vb[2], h->uc, h->pr);
+    if (logp && h->nonuniform)
+        wf::launch_nu_init_log(h, fric, c.inflow_kappa, c.inflow_z0);
+    else
+        wf::launch_init_fields(h->P, h->st, logp, h->wind, fric, c.inflow_kappa, c.inflow_z0, centre, h->vb[0],
+                               h->vb[1], h->vb[2], h->uc, h->pr);
     WF_CHECK_LAUNCH();
     WF_CUDA(cudaMemcpyAsync(h->vb[3], h->vb[0], 3 * sizeof(float) * h->P.N, cudaMemcpyDeviceToDevice, h->st));
     for (int b = 0; b < 3; ++b) WF_CUDA(cudaMemsetAsync(h->pcb[b], 0, sizeof(float) * h->P.N, h->st));
@@ -664,7 +689,9 @@ int wf_set_fixed_value_vel_bnd_cond(wf_solver* h, float wind_speed) {
     WF_CUDA(cudaSetDevice(h->device));
     h->wind = wind_speed;
     const wf_config& c = h->cfg;
-    if (c.inflow_type == WF_INFLOW_LOG) {
+    if (c.inflow_type == WF_INFLOW_LOG && h->nonuniform) {
+        wf::launch_nu_log_inlet(h, fric_vel(h), c.inflow_kappa, c.inflow_z0);
+    } else if (c.inflow_type == WF_INFLOW_LOG) {
         wf::launch_set_log_inlet(h->P, h->st, fric_vel(h), c.inflow_kappa, c.inflow_z0, h->bnd[WF_FACE_X0]);
     } else {
         wf::launch_fill3(h->st, h->bnd[WF_FACE_X0], h->P.plane[WF_FACE_X0], wind_speed, 0.f, 0.f);
@@ -675,6 +702,46 @@ int wf_set_fixed_value_vel_bnd_cond(wf_solver* h, float wind_speed) {
 }
 
 int wf_change_phys_field_pos(wf_solver* h) { return wf_init_vel_pres_fields(h); }
+
+int wf_set_face_positions(wf_solver* h, const float* fx, const float* fy, const float* fz) {
+    if (!h) return WF_ERR_INVALID_ARG;
+    WF_CUDA(cudaSetDevice(h->device));
+    const Params& P = h->P;
+    if (!fx && !fy && !fz) {
+        h->nonuniform = false;
+        wf::drop_graphs(h);
+        return WF_OK;
+    }
+    if (!fx || !fy || !fz) return set_err(h, WF_ERR_INVALID_ARG, "face positions: all three axes or none");
+    if (h->cfg.solver_type != WF_SOLVER_SIMPLE || h->cfg.turbulence != WF_TURB_NONE)
+        return set_err(h, WF_ERR_UNSUPPORTED, "the non-uniform grid runs SIMPLE without a turbulence model");
+    const int n[3] = {P.nx, P.ny, P.nz};
+    const float* f[3] = {fx, fy, fz};
+    for (int a = 0; a < 3; ++a)
+        for (int i = 0; i < n[a]; ++i)
+            if (!(std::isfinite(f[a][i]) && std::isfinite(f[a][i + 1]) && f[a][i + 1] > f[a][i]))
+                return set_err(h, WF_ERR_INVALID_ARG, "face positions must be finite and strictly increasing");
+    const size_t nf = (size_t)(P.nx + 1) + (P.ny + 1) + (P.nz + 1);
+    if (!h->fpos) WF_TRY(alloc(h, (void**)&h->fpos, nf * sizeof(float)));
+    if (!h->flux) WF_TRY(alloc(h, (void**)&h->flux, 3 * wf::nu_flux_texels(P) * sizeof(float)));
+    WF_CUDA(cudaMemcpyAsync(h->fpos, fx, (P.nx + 1) * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    WF_CUDA(cudaMemcpyAsync(h->fpos + P.nx + 1, fy, (P.ny + 1) * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    WF_CUDA(cudaMemcpyAsync(h->fpos + P.nx + 1 + P.ny + 1, fz, (P.nz + 1) * sizeof(float), cudaMemcpyHostToDevice,
+                            h->st));
+    WF_CUDA(cudaMemsetAsync(h->flux, 0, 3 * wf::nu_flux_texels(P) * sizeof(float), h->st));
+    h->nonuniform = true;
+    wf::drop_graphs(h);
+    return sync(h);
+}
+
+int wf_get_face_flux(wf_solver* h, float* out) {
+    if (!h || !out) return WF_ERR_INVALID_ARG;
+    if (!h->nonuniform) return set_err(h, WF_ERR_INVALID_ARG, "no non-uniform grid set");
+    WF_CUDA(cudaSetDevice(h->device));
+    WF_CUDA(cudaMemcpyAsync(out, h->flux, 3 * wf::nu_flux_texels(h->P) * sizeof(float), cudaMemcpyDeviceToHost,
+                            h->st));
+    return sync(h);
+}
 
 int wf_set_inflow_plane(wf_solver* h, const float* pl) {
     if (!h) return WF_ERR_INVALID_ARG;

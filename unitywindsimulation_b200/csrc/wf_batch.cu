@@ -101,6 +101,7 @@ int wf_batch_create(wf_solver* const* solvers, int n, wf_batch** out) {
     for (int i = 0; i < n; ++i) {
         if (!solvers[i]) return WF_ERR_INVALID_ARG;
         if (solvers[i]->device != solvers[0]->device) return WF_ERR_INVALID_ARG;
+        if (solvers[i]->nonuniform) return WF_ERR_UNSUPPORTED;  // uniform-grid cases only
         for (int j = 0; j < i; ++j)
             if (solvers[j] == solvers[i]) return WF_ERR_INVALID_ARG;
     }

@@ -58,3 +58,17 @@ void launch_soa_to_interleaved(cudaStream_t st, const float* s, int n, float* d,
 void launch_flags_to_i32(cudaStream_t st, const uint8_t* f, int n, int32_t* o);
 
 }  // namespace wf
+
+// Non-uniform collocated grid (wf_nonuniform.cu); the launchers take the
+// handle (mesh, face-flux texture and stream live there).
+struct wf_solver;
+namespace wf {
+size_t nu_flux_texels(const Params& P);
+void launch_nu_vel_precompute(const wf_solver* h);
+void launch_nu_vel_sweep(const wf_solver* h, const float* uI, float* uo);
+void launch_nu_pres_precompute(wf_solver* h, const float* u);
+void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout);
+void launch_nu_apply_vel(wf_solver* h, const float* pc, float* u);
+void launch_nu_init_log(wf_solver* h, float fric, float kappa, float z0);
+void launch_nu_log_inlet(wf_solver* h, float fric, float kappa, float z0);
+}  // namespace wf

@@ -42,6 +42,12 @@ struct wf_solver {
     bool pc_zero = true;
     float *Dp = nullptr, *bp = nullptr, *eddy = nullptr;
     float* drag = nullptr;    // Brinkman drag per cell (allocated when first set)
+    // non-uniform collocated grid (wf_nonuniform.cu): face positions
+    // fx[nx+1], fy[ny+1], fz[nz+1] back to back, and the face-flux texture
+    // (three planes of (nx+1)(ny+1)(nz+1)); nonuniform selects its kernels
+    float* fpos = nullptr;
+    float* flux = nullptr;
+    bool nonuniform = false;
     float* bnd[6] = {};
     // sweep coefficient caches of the fast path (wf_sweeps.cu)
     float* pcoef = nullptr;   // pressure: c_E, c_N, c_U, 1/Dp, PISO rhs (5 planes)

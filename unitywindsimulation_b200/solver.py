@@ -89,6 +89,28 @@ class FvmSolverCuda:
     def ChangePhysFieldPos(self) -> None:
         self._check(self._lib.wf_change_phys_field_pos(self._h))
 
+    def set_face_positions(self, fx, fy, fz) -> None:
+        """Non-uniform collocated grid (gridType CollNonUniform): face
+        positions fx[nx+1], fy[ny+1], fz[nz+1] (wf_set_face_positions).
+        Re-initialise the fields afterwards, as the reference's constructor
+        builds the mesh first.  All None: back to the uniform grid."""
+        if fx is None and fy is None and fz is None:
+            self._check(self._lib.wf_set_face_positions(self._h, None, None, None))
+            return
+        a = [np.ascontiguousarray(v, dtype=np.float32) for v in (fx, fy, fz)]
+        c = self.cfg
+        if [v.size for v in a] != [c.nx + 1, c.ny + 1, c.nz + 1]:
+            raise ValueError("face positions need nx+1, ny+1 and nz+1 values")
+        self._check(self._lib.wf_set_face_positions(self._h, *[v.ctypes.data_as(POINTER(c_float)) for v in a]))
+
+    def get_face_flux(self) -> np.ndarray:
+        """Face-flux texture of the non-uniform grid, (3, nz+1, ny+1, nx+1)."""
+        c = self.cfg
+        m = (c.nx + 1) * (c.ny + 1) * (c.nz + 1)
+        out = np.empty(3 * m, dtype=np.float32)
+        self._check(self._lib.wf_get_face_flux(self._h, out.ctypes.data_as(POINTER(c_float))))
+        return out.reshape(3, c.nz + 1, c.ny + 1, c.nx + 1)
+
     def InitVelPresFieldsFromBackGroundFlow(self, background: "FvmSolverCuda", pos=(0.0, 0.0, 0.0),
                                             pos_background=(0.0, 0.0, 0.0), rot_deg: float = 0.0) -> None:
         """Velocity and pressure from a background solver's current fields,
