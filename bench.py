@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-nonuniform", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the host-core baselines of every workload (no GPU) and exit")
@@ -327,6 +328,76 @@ def adjoint_section(local: int):
             "dJ_dz0": r["dJ_dz0"], "dJ_dheights": [float(x) for x in r["dJ_dheights"]]}
 
 
+def b_alg_nonuniform(nv: int, np_: int) -> int:
+    """Compulsory bytes per cell-step of the non-uniform SIMPLE step
+    (FvmCollNonUniform.compute; vector 12 B, scalar 4 B, flag 1 B): momentum
+    pre-compute 53 (u_T, p, face fluxes, flag in; D, b out), sweep 61 per
+    iteration (iterate, face fluxes, D, b, flag in; iterate out), pressure
+    pre-compute 49 (u, p, D, flag in; fluxes, Dp, bp out), sweep 29 per
+    iteration (p', D, Dp, bp, flag in; p' out), apply-p 13, apply-u 53,
+    zero-p' 8, end copy 24."""
+    return 53 + 61 * nv + 49 + 29 * np_ + 13 + 53 + 8 + 24
+
+
+def nonuniform_section(local: int, steps: int, cpu: bool):
+    """The non-uniform grid (gridType CollNonUniform) on the reference's own
+    configuration for it, WindTunnelBoxConfig: 100 x 50(up) x 100 cells on
+    the InitMeshBuffers mesh, SIMPLE, laminar, nV=800 nP=2000.  Device time
+    of graph-replayed steps (CUDA events).  The fields (about 50 MB) stay in
+    L2, so the algorithmic-byte rate may exceed the HBM copy peak.  With
+    cpu=True one full step of the reference's own kernels (where built) on
+    the host cores is timed beside it."""
+    from unitywindsimulation_b200 import FvmSolverCuda, cases
+
+    case = cases.wind_tunnel()
+    c = case.cfg
+    s = FvmSolverCuda(c, device=local)
+    cases.apply_case(s, case)
+    s.Step(1)
+    s.prepare_graphs()
+    l0 = s.kernel_launches()
+    s.Step(steps)
+    ms = s.last_step_ms() / steps
+    launches = (s.kernel_launches() - l0) // steps
+    s.close()
+    rate = case.n_cells / (ms / 1e3) / 1e6
+    b = b_alg_nonuniform(c.vel_iters, c.pres_iters)
+    peak, src = measured_peaks()
+    out = {"workload": f"wind_tunnel: {c.nx}x{c.ny}(up)x{c.nz} cells on the reference's non-uniform mesh "
+                       f"(25 + 50 + 25 cells in x and z, ratio 1.08), SIMPLE laminar, nV={c.vel_iters} "
+                       f"nP={c.pres_iters}, one box",
+           "mcell_steps_s": rate, "ms_per_step": ms, "steps": steps, "gpu_launches_per_step": launches,
+           "b_alg_bytes_per_cell_step": b, "alg_gbs": rate * b / 1e3, "alg_frac_of_hbm_peak": rate * b / 1e3 / peak,
+           "peak_source": f"hbm_gbs of {src}", "l2": "fields resident in L2 (about 50 MB)"}
+    if cpu:
+        from oracle.binding import RefSolver, ref_available
+        if ref_available():
+            # A full step is 2800 sweeps (about a minute on 16 cores): time one
+            # step with a tenth of each loop's sweeps and one without sweeps,
+            # and take fixed part + 10 x the sweep part.
+            def one_step(nv, np_):
+                cs = cases.wind_tunnel(nv=nv, np_=np_)
+                r = RefSolver(cs.cfg)
+                cases.apply_case(r, cs)
+                t0 = time.perf_counter()
+                r.Step(1)
+                dt = time.perf_counter() - t0
+                r.close()
+                return dt
+            t_tenth = one_step(c.vel_iters // 10, c.pres_iters // 10)
+            t_fixed = one_step(0, 0)
+            t_full = t_fixed + 10.0 * (t_tenth - t_fixed)
+            cores = os.cpu_count() or 1
+            out["cpu_baseline"] = {"value": case.n_cells / t_full / 1e6, "unit": METRIC, "cores": cores,
+                                   "kind": "reference",
+                                   "sample": f"wind_tunnel with the reference's own FvmCollNonUniform kernels "
+                                             f"compiled as C++ (FP32, {cores} threads): one step with "
+                                             f"nV={c.vel_iters // 10} nP={c.pres_iters // 10} ({t_tenth:.1f} s) and "
+                                             f"one without sweeps ({t_fixed:.1f} s); full step = fixed part + 10 x "
+                                             f"the sweep part = {t_full:.1f} s"}
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -475,6 +546,10 @@ def run_windfvm(args):
     if world == 1 and not args.no_adjoint:
         adjoint = adjoint_section(local)
 
+    nonuniform = None
+    if world == 1 and not args.no_nonuniform:
+        nonuniform = nonuniform_section(local, 3, cpu=rank == 0 and not args.no_cpu_baseline)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case, args.cpu_sample_steps)
@@ -493,6 +568,7 @@ def run_windfvm(args):
             "batched": batched,
             "batched_small_cases": batched_small,
             "adjoint": adjoint,
+            "nonuniform": nonuniform,
         }
         print(json.dumps(line), flush=True)
     group.close()

@@ -179,3 +179,21 @@ def test_unsupported_combinations_are_refused():
         AdjointSolver(s)
     s.set_face_positions(None, None, None)  # back to the uniform grid
     s.Step(1)
+
+
+@pytest.mark.gpu
+def test_four_cell_sweeps_equal_one_cell_sweeps(monkeypatch):
+    """The four-cells-per-thread momentum and pressure sweeps (nx % 4 == 0)
+    give the same fields, bit for bit, as the one-cell sweeps (WF_VEC4=0)."""
+    name = "const_tunnel"
+    outs = []
+    for vec4 in ("1", "0"):
+        monkeypatch.setenv("WF_VEC4", vec4)
+        got = {}
+
+        def rec(step, key, a):
+            got[f"{step}/{key}"] = a
+        G.run_case(_cuda(), name, rec)
+        outs.append(got)
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k

@@ -115,7 +115,7 @@ void free_all(wf_solver* h) {
     wf::drop_graphs(h);
     void* ptrs[] = {h->fl, h->vb[0], h->vb[1], h->vb[2], h->vb[3], h->uc, h->Dv, h->bv, h->aodu, h->face, h->pr,
                     h->pcb[0], h->pcb[1], h->pcb[2], h->Dp, h->bp, h->eddy, h->pcoef, h->vcoef, h->grad, h->part, h->dsum, h->dref,
-                    h->dbad, h->stage, h->bnd[0], h->drag, h->nbm, h->fpos, h->flux};
+                    h->dbad, h->stage, h->bnd[0], h->drag, h->nbm, h->fpos, h->flux, h->nucoef};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->hsum) cudaFreeHost(h->hsum);
@@ -199,15 +199,16 @@ int do_vel_sweeps(wf_solver* h, int n, bool allow_fast) {
     const Params& P = h->P;
     const bool resid = h->cfg.calc_residual != 0;
     int k = 0;
-    if (allow_fast && h->fast && !resid && n > 0 && !h->nonuniform) {
+    if (allow_fast && h->fast && !resid && n > 0) {
         // Multi-sweep path: same buffer roles, several sweeps per launch.
+        // On the non-uniform grid too: its pre-compute stored A and 1/D.
         WF_TRY(wf::vel_sweeps_fast(h, n));
         return WF_OK;
     }
     for (; k < n; ++k) {
         const float* src = h->iter_alias ? h->vb[h->iT] : h->vb[h->iI];
-        if (h->nonuniform)
-            wf::launch_nu_vel_sweep(h, src, h->vb[h->iF]);
+        if (h->nonuniform)  // the pre-compute's A and 1/D (vcoef)
+            wf::launch_vel_sweep1_ptr(P, h->st, h->vcoef, h->vcoef + 6 * (size_t)P.N, h->bv, src, h->vb[h->iF]);
         else
             wf::launch_vel_sweep(P, h->st, h->fl, src, h->vb[h->iT], h->eddy, h->face, h->Dv, h->bv, h->vb[h->iF]);
         WF_CHECK_LAUNCH();
@@ -724,6 +725,7 @@ int wf_set_face_positions(wf_solver* h, const float* fx, const float* fy, const 
     const size_t nf = (size_t)(P.nx + 1) + (P.ny + 1) + (P.nz + 1);
     if (!h->fpos) WF_TRY(alloc(h, (void**)&h->fpos, nf * sizeof(float)));
     if (!h->flux) WF_TRY(alloc(h, (void**)&h->flux, 3 * wf::nu_flux_texels(P) * sizeof(float)));
+    if (!h->nucoef) WF_TRY(alloc(h, (void**)&h->nucoef, (size_t)wf::kNuCoefPlanes * P.N * sizeof(float)));
     WF_CUDA(cudaMemcpyAsync(h->fpos, fx, (P.nx + 1) * sizeof(float), cudaMemcpyHostToDevice, h->st));
     WF_CUDA(cudaMemcpyAsync(h->fpos + P.nx + 1, fy, (P.ny + 1) * sizeof(float), cudaMemcpyHostToDevice, h->st));
     WF_CUDA(cudaMemcpyAsync(h->fpos + P.nx + 1 + P.ny + 1, fz, (P.nz + 1) * sizeof(float), cudaMemcpyHostToDevice,
@@ -1227,6 +1229,7 @@ int wf_kernel_launches(const wf_solver* h, int64_t* total) {
 int wf_time_kernel(wf_solver* h, int kernel, int reps, int flush_l2, float* ms_per_launch,
                    double* alg_bytes_per_launch, int* sweeps_per_launch) {
     if (!h) return WF_ERR_INVALID_ARG;
+    if (h->nonuniform) return set_err(h, WF_ERR_UNSUPPORTED, "times the uniform-grid Jacobi kernels");
     if (!ms_per_launch || !alg_bytes_per_launch || !sweeps_per_launch || reps <= 0 ||
         (kernel != WF_KERNEL_PRES_SWEEP && kernel != WF_KERNEL_VEL_SWEEP))
         return set_err(h, WF_ERR_INVALID_ARG, "bad kernel id, reps or output pointer");

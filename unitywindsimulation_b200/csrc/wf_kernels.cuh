@@ -63,9 +63,9 @@ void launch_flags_to_i32(cudaStream_t st, const uint8_t* f, int n, int32_t* o);
 // handle (mesh, face-flux texture and stream live there).
 struct wf_solver;
 namespace wf {
+constexpr int kNuCoefPlanes = 7;  // per-step pressure-sweep coefficients of the non-uniform grid (N floats each)
 size_t nu_flux_texels(const Params& P);
 void launch_nu_vel_precompute(const wf_solver* h);
-void launch_nu_vel_sweep(const wf_solver* h, const float* uI, float* uo);
 void launch_nu_pres_precompute(wf_solver* h, const float* u);
 void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout);
 void launch_nu_apply_vel(wf_solver* h, const float* pc, float* u);

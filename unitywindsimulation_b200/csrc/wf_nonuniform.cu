@@ -1,6 +1,8 @@
 // wf_nonuniform.cu - the non-uniform collocated grid (the reference's gridType
 // CollNonUniform): FvmCollNonUniform.compute's SIMPLE kernels and the two
-// mesh-aware set-up kernels of InitShaderColl.compute, one thread per cell.
+// mesh-aware set-up kernels of InitShaderColl.compute, one thread per cell;
+// the momentum sweeps are the uniform grid's (wf_sweeps.cu) over the
+// coefficient planes the non-uniform pre-compute stores.
 //
 // The mesh is given by face positions along each axis (facePosX/Y/Z,
 // FvmSolverGpu.cs:682-788): cell x spans fx[x]..fx[x+1].  Every kernel
@@ -26,6 +28,12 @@ namespace wf {
 namespace {
 
 __device__ __forceinline__ float ldn(const float* p, size_t i) { return __ldg(p + i); }
+
+// Pressure coefficient planes (N floats each) the pressure pre-compute
+// stores for the sweeps: face coefficients ((dv / den) DInv) / h, zero at
+// faces without a fluid neighbour, and 1/Dp.
+constexpr int kCoefP = 0, kCoefInvDp = 6;
+static_assert(kCoefInvDp + 1 == kNuCoefPlanes, "plane count");
 
 // Spacing of cell i along one axis and of its neighbours; a neighbour
 // outside the domain takes the cell's own spacing (FvmCollNonUniform.compute:
@@ -106,18 +114,33 @@ __device__ __forceinline__ bool fluid_far(const Params& P, const uint8_t* fl, in
 }
 
 // CSVelPredictPreCompute, FvmCollNonUniform.compute:111-721 (useLES off).
+// Besides D and b it stores the sweep's coefficients for the step: per
+// fluid-neighbour face A_f = (nu ds) / h -+ (ds w_neighbour) F_f (the
+// diffusion and advection factors CSVelPredict multiplies u_neighbour by,
+// :797-907) and 1/D, in the layout of the uniform grid's momentum sweep
+// (A: 6 planes, 1/D: 3 planes; zero on non-fluid cells), so the same
+// four-cells-per-thread sweep runs on both grids.  Summing A_f u rather
+// than the advection and diffusion sums apart reorders the additions: the
+// fields agree with the reference's kernels within FP32 rounding.
 __global__ void k_nu_vel_precompute(const __grid_constant__ Params P, const Bnd B, const float* __restrict__ fx,
                                     const float* __restrict__ fy, const float* __restrict__ fz,
                                     const uint8_t* __restrict__ fl, const float* __restrict__ uT,
                                     const float* __restrict__ pr, const float* __restrict__ flux,
-                                    float* __restrict__ Dv, float* __restrict__ bv) {
+                                    float* __restrict__ Dv, float* __restrict__ bv, float* __restrict__ A,
+                                    float* __restrict__ iD) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
     if (x >= P.nx || y >= P.ny || z >= P.nz) return;
     const int i = cidx(P, x, y, z);
-    if (!fluid_cell(fl, i)) return;
     const size_t N = P.N;
+    if (!fluid_cell(fl, i)) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) A[f * N + i] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) iD[k * N + i] = 0.f;
+        return;
+    }
     const unsigned m = __ldg(P.nbm + i);
     const Geo g = geo_of(P, fx, fy, fz, x, y, z);
     const Flux F = flux_of(P, flux);
@@ -199,53 +222,33 @@ __global__ void k_nu_vel_precompute(const __grid_constant__ Params P, const Bnd 
         Dv[k * N + i] = D[k];
         bv[k * N + i] = b[k];
     }
+    // sweep coefficients (FvmCollNonUniform.compute:797-842 and 844-907
+    // evaluate them inline in every sweep)
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        float c = 0.f;
+        if (nb_fluid(m, f)) {
+            const int a = face_axis(f);
+            const float adv = g.ds[a] * (1.0f - w_self(g, f)) * face_flux(F, x, y, z, f);
+            const float dif = vis * g.ds[a] / h_face(g, f);
+            c = face_sign(f) > 0 ? dif - adv : dif + adv;
+        }
+        A[f * N + i] = c;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) iD[k * N + i] = 1.0f / D[k];
 }
 
-// CSVelPredict, FvmCollNonUniform.compute:725-917 (useLES off): one Jacobi
-// sweep over the fluid cells.
-__global__ void k_nu_vel_sweep(const __grid_constant__ Params P, const float* __restrict__ fx,
-                               const float* __restrict__ fy, const float* __restrict__ fz,
-                               const uint8_t* __restrict__ fl, const float* __restrict__ uI,
-                               const float* __restrict__ flux, const float* __restrict__ Dv,
-                               const float* __restrict__ bv, float* __restrict__ uo) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
-    if (x >= P.nx || y >= P.ny || z >= P.nz) return;
-    const int i = cidx(P, x, y, z);
-    if (!fluid_cell(fl, i)) return;
-    const size_t N = P.N;
-    const unsigned m = __ldg(P.nbm + i);
-    const Geo g = geo_of(P, fx, fy, fz, x, y, z);
-    const Flux F = flux_of(P, flux);
-    float adv[3] = {0.f, 0.f, 0.f}, dif[3] = {0.f, 0.f, 0.f};
-    // advection, :797-842
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        if (!nb_fluid(m, f)) continue;
-        const int a = face_axis(f);
-        const int q = i + face_off(P, f);
-        const float wQ = 1.0f - w_self(g, f);
-        const float Fv = face_flux(F, x, y, z, f);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float t = g.ds[a] * wQ * ldn(uI, k * N + q) * Fv;
-            adv[k] = face_sign(f) > 0 ? adv[k] - t : adv[k] + t;
-        }
-    }
-    // diffusion, :844-907
-    const float vis = P.nu;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        if (!nb_fluid(m, f)) continue;
-        const int a = face_axis(f);
-        const int q = i + face_off(P, f);
-        const float c = vis * g.ds[a] / h_face(g, f);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) dif[k] += c * ldn(uI, k * N + q);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) uo[k * N + i] = 1.0f / ldn(Dv, k * N + i) * (adv[k] + dif[k] + ldn(bv, k * N + i));
+// One thread per cell over a 1-D grid (no idle threads at the x edge of a
+// non-multiple-of-32 grid); every load leaves before the fluid test.
+__device__ __forceinline__ bool linear_cell(const Params& P, int& x, int& y, int& z, int& i) {
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.N) return false;
+    x = i % P.nx;
+    const int r = i / P.nx;
+    y = r % P.ny;
+    z = r / P.ny;
+    return true;
 }
 
 // Rhie-Chow average of the pressure gradient at face f
@@ -296,7 +299,8 @@ __global__ void k_nu_pres_precompute(const __grid_constant__ Params P, const Bnd
                                      const float* __restrict__ fy, const float* __restrict__ fz,
                                      const uint8_t* __restrict__ fl, const float* __restrict__ u,
                                      const float* __restrict__ pr, const float* __restrict__ Dv,
-                                     float* __restrict__ flux, float* __restrict__ Dp, float* __restrict__ bp) {
+                                     float* __restrict__ flux, float* __restrict__ Dp, float* __restrict__ bp,
+                                     float* __restrict__ coef) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -309,6 +313,7 @@ __global__ void k_nu_pres_precompute(const __grid_constant__ Params P, const Bnd
     const float pP = ldn(pr, i);
     float dp = 0.f, b = 0.f;
     float uf[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float cf[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f);
@@ -319,7 +324,10 @@ __global__ void k_nu_pres_precompute(const __grid_constant__ Params P, const Bnd
             const float wP = w_self(g, f), wQ = 1.0f - wP;
             const float DInv = wP * (1.0f / ldn(Dv, a * N + i)) + wQ * (1.0f / ldn(Dv, a * N + q));
             const float h2 = h_face(g, f);
-            dp -= (g.dv / P.den) * DInv / h2;
+            // the sweeps' face coefficient (CSPresCorrectRhieChow evaluates
+            // the same expression, FvmCollNonUniform.compute:1398-1449)
+            cf[f] = (g.dv / P.den) * DInv / h2;
+            dp -= cf[f];
             float v = wP * ldn(u, a * N + i) + wQ * ldn(u, a * N + q);
             const float pQ = ldn(pr, q);
             const float grad = pos ? (pQ - pP) / h2 : (pP - pQ) / h2;
@@ -370,36 +378,89 @@ __global__ void k_nu_pres_precompute(const __grid_constant__ Params P, const Bnd
     }
     Dp[i] = dp;
     bp[i] = b;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) coef[(kCoefP + f) * N + i] = cf[f];
+    coef[kCoefInvDp * N + i] = 1.0f / dp;
 }
 
-// CSPresCorrectRhieChow, FvmCollNonUniform.compute:1346-1452.  pin null:
+// CSPresCorrectRhieChow, FvmCollNonUniform.compute:1346-1452, with the
+// step's face coefficients: p' = (1/Dp) (-sum_f c_f p'_Q + bp).  pin null:
 // the previous iterate is zero.
-__global__ void k_nu_pres_sweep(const __grid_constant__ Params P, const float* __restrict__ fx,
-                                const float* __restrict__ fy, const float* __restrict__ fz,
-                                const uint8_t* __restrict__ fl, const float* __restrict__ pin,
-                                const float* __restrict__ Dv, const float* __restrict__ Dp,
-                                const float* __restrict__ bp, float* __restrict__ pout) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
-    if (x >= P.nx || y >= P.ny || z >= P.nz) return;
-    const int i = cidx(P, x, y, z);
-    if (!fluid_cell(fl, i)) return;
+__global__ void __launch_bounds__(256) k_nu_pres_sweep(const __grid_constant__ Params P,
+                                                       const float* __restrict__ pin,
+                                                       const float* __restrict__ coef,
+                                                       const float* __restrict__ bp, float* __restrict__ pout) {
+    int x, y, z, i;
+    if (!linear_cell(P, x, y, z, i)) return;
     const size_t N = P.N;
     const unsigned m = __ldg(P.nbm + i);
-    const Geo g = geo_of(P, fx, fy, fz, x, y, z);
-    float term = 0.f;
+    float pq[6], c[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        if (!nb_fluid(m, f)) continue;
-        const int a = face_axis(f);
-        const int q = i + face_off(P, f);
-        const float wP = w_self(g, f), wQ = 1.0f - wP;
-        const float DInv = wP * (1.0f / ldn(Dv, a * N + i)) + wQ * (1.0f / ldn(Dv, a * N + q));
-        const float pq = pin ? ldn(pin, q) : 0.f;
-        term -= (g.dv / P.den) * DInv / h_face(g, f) * pq;
+        pq[f] = pin ? ldn(pin, nb_idx(P, x, y, z, i, f)) : 0.f;
+        c[f] = ldn(coef, (kCoefP + f) * N + i);
     }
-    pout[i] = (1.0f / ldn(Dp, i)) * (term + ldn(bp, i));
+    const float inv = ldn(coef, kCoefInvDp * N + i), b = ldn(bp, i);
+    if (!(m & 64u)) return;
+    float term = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        if (nb_fluid(m, f)) term -= c[f] * pq[f];
+    pout[i] = inv * (term + b);
+}
+
+// k_nu_pres_sweep with four x-consecutive cells per thread (nx % 4 == 0,
+// 16-byte aligned planes): 128-bit loads of the coefficient planes, the
+// iterate and its y/z neighbours, two scalar loads for the x neighbours
+// beyond the four cells; the same arithmetic per cell.
+__device__ __forceinline__ float4 ld4n(const float* p, size_t i) {
+    return __ldg(reinterpret_cast<const float4*>(p + i));
+}
+__device__ __forceinline__ float c4(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+
+__global__ void __launch_bounds__(256) k_nu_pres_sweep4(const __grid_constant__ Params P,
+                                                        const float* __restrict__ pin,
+                                                        const float* __restrict__ coef,
+                                                        const float* __restrict__ bp, float* __restrict__ pout) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.N / 4) return;
+    const int i = 4 * q;
+    const int x0 = i % P.nx, r = i / P.nx, y = r % P.ny, z = r / P.ny;
+    const size_t N = P.N;
+    const int sx = P.nx, sz = P.nx * P.ny;
+    const int iN = y + 1 < P.ny ? i + sx : i, iS = y > 0 ? i - sx : i;
+    const int iU = z + 1 < P.nz ? i + sz : i, iDn = z > 0 ? i - sz : i;
+    const int iE = x0 + 4 < P.nx ? i + 4 : i + 3, iW = x0 > 0 ? i - 1 : i;
+    const uchar4 mq = __ldg(reinterpret_cast<const uchar4*>(P.nbm + i));
+    float4 c[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) c[f] = ld4n(coef, (kCoefP + f) * N + i);
+    const float4 inv = ld4n(coef, kCoefInvDp * N + i), b = ld4n(bp, i);
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 pc = pin ? ld4n(pin, i) : z4, pn = pin ? ld4n(pin, iN) : z4, ps = pin ? ld4n(pin, iS) : z4;
+    const float4 pu = pin ? ld4n(pin, iU) : z4, pd = pin ? ld4n(pin, iDn) : z4;
+    const float pe3 = pin ? __ldg(pin + iE) : 0.f, pw0 = pin ? __ldg(pin + iW) : 0.f;
+    const unsigned ms[4] = {mq.x, mq.y, mq.z, mq.w};
+    float v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const unsigned m = ms[j];
+        const float pq[6] = {j < 3 ? c4(pc, j + 1) : pe3, j > 0 ? c4(pc, j - 1) : pw0, c4(pn, j), c4(ps, j),
+                             c4(pu, j), c4(pd, j)};
+        float term = 0.f;
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if (nb_fluid(m, f)) term -= c4(c[f], j) * pq[f];
+        v[j] = c4(inv, j) * (term + c4(b, j));
+    }
+    const bool all = (ms[0] & ms[1] & ms[2] & ms[3] & 64u) != 0;
+    if (all) {
+        *reinterpret_cast<float4*>(pout + i) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (ms[j] & 64u) pout[i + j] = v[j];
+    }
 }
 
 // CSApplyVelCorrectionDivergenceTheorem, FvmCollNonUniform.compute:1487-1731.
@@ -497,16 +558,7 @@ void launch_nu_vel_precompute(const wf_solver* h) {
     const float* fz = fy + P.ny + 1;
     WF_COUNT_LAUNCH();
     k_nu_vel_precompute<<<nu_grid(P), nu_block(), 0, h->st>>>(P, h->B, fx, fy, fz, h->fl, h->vb[h->iT], h->pr,
-                                                               h->flux, h->Dv, h->bv);
-}
-
-void launch_nu_vel_sweep(const wf_solver* h, const float* uI, float* uo) {
-    const Params& P = h->P;
-    const float* fx = h->fpos;
-    const float* fy = fx + P.nx + 1;
-    const float* fz = fy + P.ny + 1;
-    WF_COUNT_LAUNCH();
-    k_nu_vel_sweep<<<nu_grid(P), nu_block(), 0, h->st>>>(P, fx, fy, fz, h->fl, uI, h->flux, h->Dv, h->bv, uo);
+                                                               h->flux, h->Dv, h->bv, h->vcoef, h->vcoef + 6 * (size_t)P.N);
 }
 
 void launch_nu_pres_precompute(wf_solver* h, const float* u) {
@@ -516,16 +568,18 @@ void launch_nu_pres_precompute(wf_solver* h, const float* u) {
     const float* fz = fy + P.ny + 1;
     WF_COUNT_LAUNCH();
     k_nu_pres_precompute<<<nu_grid(P), nu_block(), 0, h->st>>>(P, h->B, fx, fy, fz, h->fl, u, h->pr, h->Dv,
-                                                                h->flux, h->Dp, h->bp);
+                                                                h->flux, h->Dp, h->bp, h->nucoef);
 }
 
 void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout) {
     const Params& P = h->P;
-    const float* fx = h->fpos;
-    const float* fy = fx + P.nx + 1;
-    const float* fz = fy + P.ny + 1;
     WF_COUNT_LAUNCH();
-    k_nu_pres_sweep<<<nu_grid(P), nu_block(), 0, h->st>>>(P, fx, fy, fz, h->fl, pin, h->Dv, h->Dp, h->bp, pout);
+    if (quad_ok(P, {pin, h->nucoef, h->bp, pout, P.nbm})) {
+        const int nq = P.N / 4;
+        k_nu_pres_sweep4<<<(nq + 255) / 256, 256, 0, h->st>>>(P, pin, h->nucoef, h->bp, pout);
+    } else {
+        k_nu_pres_sweep<<<(P.N + 255) / 256, 256, 0, h->st>>>(P, pin, h->nucoef, h->bp, pout);
+    }
 }
 
 void launch_nu_apply_vel(wf_solver* h, const float* pc, float* u) {

@@ -47,6 +47,7 @@ struct wf_solver {
     // (three planes of (nx+1)(ny+1)(nz+1)); nonuniform selects its kernels
     float* fpos = nullptr;
     float* flux = nullptr;
+    float* nucoef = nullptr;  // the pressure sweeps' per-step coefficient planes (wf::kNuCoefPlanes)
     bool nonuniform = false;
     float* bnd[6] = {};
     // sweep coefficient caches of the fast path (wf_sweeps.cu)

@@ -727,6 +727,10 @@ dim3 grd4(const Params& P) {
 void vel_coef(wf_solver* h) {
     const Params& P = h->P;
     const size_t N = P.N;
+    if (h->nonuniform) {  // the non-uniform momentum pre-compute stored A and 1/D
+        h->id_gen = h->d_gen;
+        return;
+    }
     WF_COUNT_LAUNCH();
     k_vel_coef<<<grd(P), blk(), 0, h->st>>>(P, h->fl, h->vb[h->iT], h->eddy, h->face, h->Dv, h->vcoef,
                                             h->vcoef + 6 * N);
