@@ -197,3 +197,23 @@ def test_four_cell_sweeps_equal_one_cell_sweeps(monkeypatch):
         outs.append(got)
     for k in outs[0]:
         assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+@pytest.mark.gpu
+def test_chained_launches_equal_plain_stream_order(monkeypatch):
+    """Programmatic dependent launch of the sweep chains (default) gives the
+    same fields, bit for bit, as plain stream order (WF_PDL=0), with and
+    without graph replay."""
+    name = "log_urban_normalised"
+    outs = []
+    for pdl, graph in (("1", 1), ("0", 1), ("1", 0)):
+        monkeypatch.setenv("WF_PDL", pdl)
+        got = {}
+
+        def rec(step, key, a):
+            got[f"{step}/{key}"] = a
+        G.run_case(_cuda(use_graph=graph), name, rec)
+        outs.append(got)
+    for other in outs[1:]:
+        for k in outs[0]:
+            assert np.array_equal(outs[0][k], other[k]), k

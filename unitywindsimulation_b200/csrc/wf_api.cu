@@ -575,6 +575,7 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     if (const char* pk = std::getenv("WF_PRES_K")) h->pres_k = std::min(std::max(std::atoi(pk), 1), 4);
     if (const char* vk = std::getenv("WF_VEL_K")) h->vel_k = std::min(std::max(std::atoi(vk), 1), 2);
     if (const char* v4 = std::getenv("WF_VEC4")) h->vec4 = std::atoi(v4);
+    if (const char* pd = std::getenv("WF_PDL")) h->pdl = std::atoi(pd);
 
     Params& P = h->P;
     P.nx = cfg->nx; P.ny = cfg->ny; P.nz = cfg->nz;

@@ -100,6 +100,35 @@ __device__ __forceinline__ bool d_split(const Params& P, int x0, int x1, int y, 
            (z == P.nz - 1 && P.vbc[WF_FACE_ZN] == WF_BND_SYMMETRY);
 }
 
+// Programmatic dependent launch inside a chain of Jacobi sweeps: the block
+// lets the next launch of the chain be scheduled (all blocks of this grid
+// have started once every block has passed this point), then waits until
+// the previous grid in the stream has completed and its writes are visible.
+// Every global access of the kernel follows it.  Without the launch
+// attribute both calls return at once.
+__device__ __forceinline__ void chain_entry() {
+    cudaTriggerProgrammaticLaunchCompletion();
+    cudaGridDependencySynchronize();
+}
+
+// Launches kernel<<<grid, block, 0, st>>>(args...), as a programmatic
+// dependent launch when `chained` (the kernel must start with chain_entry).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, bool chained,
+                                  Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = chained ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Where a four-cells-per-thread kernel applies: the switch (Params::vec4),
 // nx % 4 == 0 and 16-byte aligned planes.
 inline bool quad_ok(const Params& P, std::initializer_list<const void*> ptrs) {

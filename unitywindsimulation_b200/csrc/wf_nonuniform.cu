@@ -390,6 +390,7 @@ __global__ void __launch_bounds__(256) k_nu_pres_sweep(const __grid_constant__ P
                                                        const float* __restrict__ pin,
                                                        const float* __restrict__ coef,
                                                        const float* __restrict__ bp, float* __restrict__ pout) {
+    chain_entry();
     int x, y, z, i;
     if (!linear_cell(P, x, y, z, i)) return;
     const size_t N = P.N;
@@ -422,6 +423,7 @@ __global__ void __launch_bounds__(256) k_nu_pres_sweep4(const __grid_constant__ 
                                                         const float* __restrict__ pin,
                                                         const float* __restrict__ coef,
                                                         const float* __restrict__ bp, float* __restrict__ pout) {
+    chain_entry();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.N / 4) return;
     const int i = 4 * q;
@@ -574,11 +576,13 @@ void launch_nu_pres_precompute(wf_solver* h, const float* u) {
 void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout) {
     const Params& P = h->P;
     WF_COUNT_LAUNCH();
+    const float* c = h->nucoef;
+    const float* b = h->bp;
     if (quad_ok(P, {pin, h->nucoef, h->bp, pout, P.nbm})) {
         const int nq = P.N / 4;
-        k_nu_pres_sweep4<<<(nq + 255) / 256, 256, 0, h->st>>>(P, pin, h->nucoef, h->bp, pout);
+        launch_chained(k_nu_pres_sweep4, dim3((nq + 255) / 256), dim3(256), h->st, h->pdl != 0, P, pin, c, b, pout);
     } else {
-        k_nu_pres_sweep<<<(P.N + 255) / 256, 256, 0, h->st>>>(P, pin, h->nucoef, h->bp, pout);
+        launch_chained(k_nu_pres_sweep, dim3((P.N + 255) / 256), dim3(256), h->st, h->pdl != 0, P, pin, c, b, pout);
     }
 }
 

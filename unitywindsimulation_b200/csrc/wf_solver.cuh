@@ -84,6 +84,8 @@ struct wf_solver {
     int pres_k = 4;           // pressure sweeps per multi-sweep pass (1..4)
     int vel_k = 1;            // momentum sweeps per multi-sweep pass (1..2)
     int num_sms = 148;        // multiprocessors of the device
+    int pdl = 1;              // programmatic dependent launch in the non-uniform grid's sweep chains
+                              // (WF_PDL=0: plain stream order)
     int vec4 = 1;             // 4-cell vector momentum sweep when nx % 4 == 0 and the
                               // planes are 16-byte aligned (WF_VEC4=0: one cell per thread)
     bool in_step = false;     // inside wf_step: skip iterates no later kernel reads
