@@ -53,7 +53,10 @@ enum {
     WF_ERR_NONFINITE = 4,    /* NaN/Inf found in the solution                */
     WF_ERR_TIMEOUT = 5,      /* a bounded device wait gave up                */
     WF_ERR_UNSUPPORTED = 6,  /* option not implemented for this build        */
-    WF_NOT_FINISHED = 7,     /* step stopped early (time budget)             */
+    WF_NOT_FINISHED = 7,     /* reserved for a time-budgeted step; no entry  */
+                             /* point returns it: every step completes (the  */
+                             /* reference's 30 ms slicing, FvmSolverGpu.cs:  */
+                             /* 1267-1275, is dropped)                       */
     WF_ERR_STATE = 8,        /* call not valid in the handle's current state */
     WF_ERR_IO = 9            /* a file could not be created or written       */
 };
