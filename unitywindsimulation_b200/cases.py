@@ -436,9 +436,11 @@ def wind_tunnel(nv: int = 800, np_: int = 2000, steps: int = 1) -> Case:
     return Case("wind_tunnel", cfg, flags, None, steps, None, [(20, 24, 18, 22, 8)], None, faces)
 
 
-def small_nonuniform_case(nx=16, ny=10, nz=12, log_inflow=False, seed=0, nv=8, np_=12) -> Case:
-    """Small non-uniform case for parity tests: stretched x (4 + 8 + 4
-    cells), y (2 + 6 + 2) and z (3 + 6 + 3) axes of 0.5 m cores, one box.
+def small_nonuniform_case(nx=16, ny=10, nz=12, log_inflow=False, seed=0, nv=8, np_=12,
+                          x_split=(8, 4)) -> Case:
+    """Small non-uniform case for parity tests: stretched x (x_split =
+    (uniform, per side) cells: 4 + 8 + 4 by default), y (2 + 6 + 2) and z
+    (3 + 6 + 3) axes of 0.5 m cores, one box.
     log_inflow=False: the wind-tunnel boundary set with a constant 3 m/s
     inflow; True: the urban set (no-slip ground, symmetry top and sides)
     with a log inflow and no fixed-pressure face (the pressure is
@@ -466,7 +468,7 @@ def small_nonuniform_case(nx=16, ny=10, nz=12, log_inflow=False, seed=0, nv=8, n
     z0_ = int(rng.integers(3, 6))
     h = int(rng.integers(2, 5))
     flags[z0_:z0_ + 3, 0:h, x0:x0 + 2] = 1
-    faces = (stretched_faces(nx, dx, 8, 4), stretched_faces(ny, dx, 6, 2), stretched_faces(nz, dx, 6, 3))
+    faces = (stretched_faces(nx, dx, *x_split), stretched_faces(ny, dx, 6, 2), stretched_faces(nz, dx, 6, 3))
     name = f"small_nu_{nx}x{ny}x{nz}_{'log' if log_inflow else 'const'}_s{seed}"
     return Case(name, cfg, flags, None, 1, seed, [(x0, x0 + 2, z0_, z0_ + 3, h)], None, faces)
 

@@ -745,7 +745,7 @@ void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
     if (vec4_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst)) {
         // the non-uniform grid's short sweeps chain with programmatic
         // dependent launch (chain_entry)
-        launch_chained(k_vel_sweep4<false>, grd4(P), blk(), h->st, h->nonuniform && h->pdl, P,
+        launch_chained(k_vel_sweep4<false>, grd4(P), blk(), h->st, h->pdl != 0, P,
                        (const float*)h->vcoef, (const float*)(h->vcoef + 6 * N), (const float*)h->bv, src, dst);
     } else {
         k_vel_sweep1<false><<<grd(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
