@@ -40,6 +40,8 @@ def load():
         "wfo_set_inflow_plane": (c_int, [c_void_p, POINTER(c_float)]),
         "wfo_init_from_background": (c_int, [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float), c_float]),
         "wfo_step": (c_int, [c_void_p, c_int]),
+        "wfo_set_face_positions": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
+        "wfo_get_face_flux": (c_int, [c_void_p, POINTER(c_double)]),
         "wfo_field_size": (c_int, [c_void_p, c_int, POINTER(c_size_t), POINTER(c_int)]),
         "wfo_get_field": (c_int, [c_void_p, c_int, POINTER(c_double)]),
         "wfo_set_field": (c_int, [c_void_p, c_int, POINTER(c_double)]),
@@ -128,6 +130,22 @@ class OracleSolver:
         out = np.empty(self.n_cells, dtype=np.int32)
         self._ok(self._lib.wfo_get_flags(self._h, out.ctypes.data_as(POINTER(c_int32))))
         return out.reshape(self.shape)
+
+    def set_face_positions(self, fx, fy, fz):
+        """Non-uniform collocated grid (gridType CollNonUniform): face
+        positions fx[nx+1], fy[ny+1], fz[nz+1]; all None: uniform grid."""
+        if fx is None and fy is None and fz is None:
+            self._ok(self._lib.wfo_set_face_positions(self._h, None, None, None))
+            return
+        a = [np.ascontiguousarray(v, dtype=np.float32) for v in (fx, fy, fz)]
+        self._ok(self._lib.wfo_set_face_positions(self._h, *[v.ctypes.data_as(POINTER(c_float)) for v in a]))
+
+    def get_face_flux(self) -> np.ndarray:
+        """velFaceFluxField: (3, nz+1, ny+1, nx+1)."""
+        nz, ny, nx = self.shape
+        out = np.empty(3 * (nx + 1) * (ny + 1) * (nz + 1), dtype=np.float64)
+        self._ok(self._lib.wfo_get_face_flux(self._h, out.ctypes.data_as(POINTER(c_double))))
+        return out.reshape(3, nz + 1, ny + 1, nx + 1)
 
     def field_size(self, field):
         pts, comps = c_size_t(0), c_int(0)

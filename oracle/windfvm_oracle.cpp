@@ -159,7 +159,7 @@ template <class R> struct Oracle {
             size_t P = idx(x, y, z);
             V3<R> u{{R(wind), R(0), R(0)}};
             if (logp) {
-                R yPhys = centre ? (R(y) + R(0.5)) * dx : R(y) * dx;
+                R yPhys = nonuniform ? nu_centre_height(y) : centre ? (R(y) + R(0.5)) * dx : R(y) * dx;
                 u = V3<R>{{log_profile(yPhys), R(0), R(0)}};
             }
             vel[P] = u; velT[P] = u; velI[P] = u;
@@ -220,7 +220,7 @@ template <class R> struct Oracle {
         if (cf.inflow_type == WF_INFLOW_LOG) {
             for (int z = 0; z < nz; ++z)
                 for (int y = 0; y < ny; ++y) {
-                    R yPhys = (R(y) + R(0.5)) * dx;
+                    R yPhys = nonuniform ? nu_centre_height(y) : (R(y) + R(0.5)) * dx;
                     bnd[WF_FACE_X0][size_t(z) * ny + y] = V3<R>{{log_profile(yPhys), R(0), R(0)}};
                 }
         } else {
@@ -405,10 +405,315 @@ template <class R> struct Oracle {
         });
     }
 
+    // ------------------------------------------- non-uniform collocated grid
+    // gridType CollNonUniform (FvmSolverGpu.cs:185-205): face positions
+    // facePosX/Y/Z (InitMeshBuffers, :682-788) and the face-flux texture
+    // velFaceFluxField ((nx+1)(ny+1)(nz+1) texels, :275) that the pressure
+    // pre-compute writes and the momentum kernels read (bound for them here;
+    // the reference's SetTexture calls for them are commented out,
+    // :1160,1196).  Restates FvmCollNonUniform.compute term by term; SIMPLE
+    // without turbulence only.
+    bool nonuniform = false;
+    std::vector<R> fpx, fpy, fpz;
+    std::vector<V3<R>> flux;
+    size_t fidx(int x, int y, int z) const { return (size_t(z) * (ny + 1) + y) * (nx + 1) + x; }
+    // Spacing of cell i and its neighbours along one axis; a neighbour outside
+    // the domain takes the cell's own spacing (:130-142, :954-977).
+    struct Sp {
+        R d, dp, dm, dpp, dmm;
+    };
+    static Sp spacing(const std::vector<R>& f, int i, int n) {
+        Sp s;
+        s.d = f[i + 1] - f[i];
+        s.dp = i + 1 < n ? f[i + 2] - f[i + 1] : s.d;
+        s.dm = i > 0 ? f[i] - f[i - 1] : s.d;
+        s.dpp = i + 2 < n ? f[i + 3] - f[i + 2] : s.d;
+        s.dmm = i > 1 ? f[i - 1] - f[i - 2] : s.d;
+        return s;
+    }
+    struct Geo {
+        Sp s[3];
+        R ds[3], dv;
+    };
+    Geo geo(int x, int y, int z) const {
+        Geo g;
+        g.s[0] = spacing(fpx, x, nx);
+        g.s[1] = spacing(fpy, y, ny);
+        g.s[2] = spacing(fpz, z, nz);
+        const R dX = g.s[0].d, dY = g.s[1].d, dZ = g.s[2].d;
+        g.ds[0] = dY * dZ;  // dsx
+        g.ds[1] = dX * dZ;  // dsy
+        g.ds[2] = dX * dY;  // dsz
+        g.dv = dX * dY * dZ;
+        return g;
+    }
+    // Own-cell interpolation weight at face f: wPe = dxE / (dx + dxE) etc.
+    static R w_self(const Geo& g, int f) {
+        const Sp& s = g.s[kFaces[f].axis];
+        const R dq = kFaces[f].sign > 0 ? s.dp : s.dm;
+        return dq / (s.d + dq);
+    }
+    // Centre distance across face f: 0.5 * dx + 0.5 * dxE etc.
+    static R h_face(const Geo& g, int f) {
+        const Sp& s = g.s[kFaces[f].axis];
+        return R(0.5) * s.d + R(0.5) * (kFaces[f].sign > 0 ? s.dp : s.dm);
+    }
+    // velFaceFluxField read of face f: the neighbour's texel for E/N/U, the
+    // cell's own for W/S/D.
+    R face_flux(int x, int y, int z, int f) const {
+        const Face& F = kFaces[f];
+        const size_t t = F.sign > 0 ? fidx(x + F.ox, y + F.oy, z + F.oz) : fidx(x, y, z);
+        return flux[t].c[F.axis];
+    }
+
+    // CSVelPredictPreCompute, FvmCollNonUniform.compute:111-721 (useLES off).
+    void nu_vel_precompute() {
+        for_cells([&](int x, int y, int z) {
+            if (!fluid(x, y, z)) return;
+            const size_t P = idx(x, y, z);
+            const Geo g = geo(x, y, z);
+            R D[3] = {g.dv / dt, g.dv / dt, g.dv / dt};
+            R b[3] = {R(0), R(0), R(0)};
+            // advection, :200-335
+            for (int f = 0; f < 6; ++f) {
+                const Face& F = kFaces[f];
+                const int a = F.axis;
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (in_fluid(X, Y, Z)) {
+                    const R t = g.ds[a] * w_self(g, f) * face_flux(x, y, z, f);
+                    for (int k = 0; k < 3; ++k) D[k] = F.sign > 0 ? D[k] + t : D[k] - t;
+                } else if (!in_region(X, Y, Z)) {
+                    const int bt = cf.vel_bc[F.bc];
+                    const R Fv = face_flux(x, y, z, f);
+                    if (bt == WF_BND_FIXED_VALUE) {
+                        const V3<R>& bb = bndv(F.bc, x, y, z);
+                        for (int k = 0; k < 3; ++k) {
+                            const R t = g.ds[a] * bb.c[k] * Fv;
+                            b[k] = F.sign > 0 ? b[k] - t : b[k] + t;
+                        }
+                    } else if (bt == WF_BND_ZERO_GRAD) {
+                        const R t = g.ds[a] * Fv;
+                        for (int k = 0; k < 3; ++k) D[k] = F.sign > 0 ? D[k] + t : D[k] - t;
+                    }
+                }
+            }
+            // pressure, :337-466
+            R pf[6];
+            for (int f = 0; f < 6; ++f) {
+                const Face& F = kFaces[f];
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (in_region(X, Y, Z)) {
+                    if (fluid(X, Y, Z)) {
+                        const R wP = w_self(g, f), wQ = R(1.0f) - wP;
+                        pf[f] = wP * p[P] + wQ * p[idx(X, Y, Z)];
+                    } else {
+                        pf[f] = p[P];
+                    }
+                } else {
+                    pf[f] = cf.pres_bc[F.bc] == WF_BND_FIXED_VALUE ? R(0) : p[P];
+                }
+            }
+            for (int a = 0; a < 3; ++a) b[a] += -(R(1.0) / den) * g.ds[a] * (pf[2 * a] - pf[2 * a + 1]);
+            // diffusion, :468-697
+            const R vis = nu;
+            for (int f = 0; f < 6; ++f) {
+                const Face& F = kFaces[f];
+                const int a = F.axis;
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (in_region(X, Y, Z)) {
+                    const R t = fluid(X, Y, Z) ? vis * g.ds[a] / h_face(g, f)
+                                               : vis * g.ds[a] / (R(0.5) * g.s[a].d);
+                    for (int k = 0; k < 3; ++k) D[k] += t;
+                } else {
+                    const int bt = cf.vel_bc[F.bc];
+                    if (bt == WF_BND_FIXED_VALUE) {
+                        const V3<R>& bb = bndv(F.bc, x, y, z);
+                        for (int k = 0; k < 3; ++k) b[k] += vis * g.ds[a] / (R(0.5) * g.s[a].d) * bb.c[k];
+                        for (int k = 0; k < 3; ++k) D[k] += vis * g.ds[a] / (R(0.5) * g.s[a].d);
+                    } else if (bt == WF_BND_SYMMETRY) {
+                        D[a] += vis * g.ds[a] / (R(0.5) * g.s[a].d);
+                    }
+                }
+            }
+            // time and force, :699-710
+            for (int k = 0; k < 3; ++k) b[k] += g.dv / dt * velT[P].c[k];
+            for (int k = 0; k < 3; ++k) b[k] += g.dv * force[k];
+            Dv[P] = V3<R>{{D[0], D[1], D[2]}};
+            bv[P] = V3<R>{{b[0], b[1], b[2]}};
+        });
+    }
+    // CSVelPredict, FvmCollNonUniform.compute:725-917 (useLES off).
+    void nu_vel_sweep() {
+        for_cells([&](int x, int y, int z) {
+            if (!fluid(x, y, z)) return;
+            const size_t P = idx(x, y, z);
+            const Geo g = geo(x, y, z);
+            R adv[3] = {R(0), R(0), R(0)}, dif[3] = {R(0), R(0), R(0)};
+            for (int f = 0; f < 6; ++f) {  // :797-842
+                const Face& F = kFaces[f];
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (!in_fluid(X, Y, Z)) continue;
+                const R wQ = R(1.0f) - w_self(g, f);
+                const R Fv = face_flux(x, y, z, f);
+                const V3<R>& uQ = velI[idx(X, Y, Z)];
+                for (int k = 0; k < 3; ++k) {
+                    const R t = g.ds[F.axis] * wQ * uQ.c[k] * Fv;
+                    adv[k] = F.sign > 0 ? adv[k] - t : adv[k] + t;
+                }
+            }
+            const R vis = nu;
+            for (int f = 0; f < 6; ++f) {  // :844-907
+                const Face& F = kFaces[f];
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (!in_fluid(X, Y, Z)) continue;
+                const V3<R>& uQ = velI[idx(X, Y, Z)];
+                for (int k = 0; k < 3; ++k) dif[k] += vis * g.ds[F.axis] / h_face(g, f) * uQ.c[k];
+            }
+            V3<R> u;
+            for (int k = 0; k < 3; ++k) u.c[k] = R(1.0) / Dv[P].c[k] * (adv[k] + dif[k] + bv[P].c[k]);
+            vel[P] = u;
+        });
+    }
+    // CSPresCorrectRhieChowPreCompute, FvmCollNonUniform.compute:920-1344.
+    void nu_pres_precompute() {
+        for_cells([&](int x, int y, int z) {
+            if (!fluid(x, y, z)) return;
+            const size_t P = idx(x, y, z);
+            const Geo g = geo(x, y, z);
+            R dp = R(0), b = R(0);
+            R uf[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+            for (int f = 0; f < 6; ++f) {
+                const Face& F = kFaces[f];
+                const int a = F.axis;
+                const Sp& s = g.s[a];
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (in_region(X, Y, Z)) {
+                    if (!fluid(X, Y, Z)) continue;  // solid neighbour: no flux
+                    const size_t Q = idx(X, Y, Z);
+                    const R wP = w_self(g, f), wQ = R(1.0f) - wP;
+                    const R DInv = wP * (R(1) / Dv[P].c[a]) + wQ * (R(1) / Dv[Q].c[a]);
+                    const R h2 = h_face(g, f);
+                    dp -= (g.dv / den) * DInv / h2;
+                    R v = wP * vel[P].c[a] + wQ * vel[Q].c[a];
+                    const R pP = p[P], pQ = p[Q];
+                    const R grad = F.sign > 0 ? (pQ - pP) / h2 : (pP - pQ) / h2;
+                    const int X2 = x + 2 * F.ox, Y2 = y + 2 * F.oy, Z2 = z + 2 * F.oz;
+                    const int Xr = x - F.ox, Yr = y - F.oy, Zr = z - F.oz;
+                    const bool fqq = in_fluid(X2, Y2, Z2), fr = in_fluid(Xr, Yr, Zr);
+                    R ave;
+                    if (F.sign > 0) {  // :1011-1020 (E), :1121-1130 (N), :1231-1240 (U)
+                        const R h = s.d, hQ = s.dp, hQQ = s.dpp, hR = s.dm;
+                        if (fqq && fr)
+                            ave = R(0.5) * ((p[idx(X2, Y2, Z2)] - pP) / (R(0.5) * hQQ + hQ + R(0.5) * h) +
+                                            (pQ - p[idx(Xr, Yr, Zr)]) / (R(0.5) * hQ + h + R(0.5) * hR));
+                        else if (fqq)
+                            ave = R(0.5) * ((p[idx(X2, Y2, Z2)] - pP) / (R(0.5) * hQQ + hQ + R(0.5) * h) +
+                                            (pQ - pP) / (R(0.5) * hQ + R(1.5) * h));
+                        else if (fr)
+                            ave = R(0.5) * ((pQ - pP) / (R(1.5) * hQ + R(0.5) * h) +
+                                            (pQ - p[idx(Xr, Yr, Zr)]) / (R(0.5) * hQ + h + R(0.5) * hR));
+                        else
+                            ave = grad;
+                    } else {  // :1066-1075 (W), :1176-1185 (S), :1298-1305 (D)
+                        const R h = s.d, hQ = s.dm, hQQ = s.dmm, hR = s.dp;
+                        if (fqq && fr)
+                            ave = R(0.5) * ((p[idx(Xr, Yr, Zr)] - pQ) / (R(0.5) * hR + h + R(0.5) * hQ) +
+                                            (pP - p[idx(X2, Y2, Z2)]) / (R(0.5) * h + hQ + R(0.5) * hQQ));
+                        else if (fqq)
+                            ave = R(0.5) * ((pP - pQ) / (R(1.5) * h + R(0.5) * hQ) +
+                                            (pP - p[idx(X2, Y2, Z2)]) / (R(0.5) * h + hQ + R(0.5) * hQQ));
+                        else if (fr)
+                            ave = R(0.5) * ((p[idx(Xr, Yr, Zr)] - pQ) / (R(0.5) * hR + h + R(0.5) * hQ) +
+                                            (pP - pQ) / (R(0.5) * h + R(1.5) * hQ));
+                        else
+                            ave = grad;
+                    }
+                    v -= (g.dv * DInv) / den * (grad - ave);
+                    uf[f] = v;
+                    b = F.sign > 0 ? b + v : b - v;
+                } else {
+                    const int vb = cf.vel_bc[F.bc];
+                    if (vb == WF_BND_FIXED_VALUE) {
+                        const R v = bndv(F.bc, x, y, z).c[a];
+                        uf[f] = v;
+                        b = F.sign > 0 ? b + v : b - v;
+                    } else if (vb == WF_BND_ZERO_GRAD) {
+                        const R v = vel[P].c[a];
+                        uf[f] = v;
+                        b = F.sign > 0 ? b + v : b - v;
+                    }
+                    if (cf.pres_bc[F.bc] == WF_BND_FIXED_VALUE) {
+                        const R DInv = R(1) / Dv[P].c[a];
+                        dp -= (g.dv / den) * DInv / (R(0.5) * s.d);
+                    }
+                }
+            }
+            // :1335-1341
+            flux[fidx(x, y, z)] = V3<R>{{uf[1], uf[3], uf[5]}};
+            if (x + 1 == nx) flux[fidx(x + 1, y, z)] = V3<R>{{uf[0], R(0), R(0)}};
+            if (y + 1 == ny) flux[fidx(x, y + 1, z)] = V3<R>{{R(0), uf[2], R(0)}};
+            if (z + 1 == nz) flux[fidx(x, y, z + 1)] = V3<R>{{R(0), R(0), uf[4]}};
+            Dp[P] = dp;
+            bp[P] = b;
+        });
+    }
+    // CSPresCorrectRhieChow, FvmCollNonUniform.compute:1346-1452.
+    void nu_pres_sweep() {
+        for_cells([&](int x, int y, int z) {
+            if (!fluid(x, y, z)) return;
+            const size_t P = idx(x, y, z);
+            const Geo g = geo(x, y, z);
+            R t = R(0);
+            for (int f = 0; f < 6; ++f) {
+                const Face& F = kFaces[f];
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (!in_fluid(X, Y, Z)) continue;
+                const size_t Q = idx(X, Y, Z);
+                const R wP = w_self(g, f), wQ = R(1.0f) - wP;
+                const R DInv = wP * (R(1) / Dv[P].c[F.axis]) + wQ * (R(1) / Dv[Q].c[F.axis]);
+                t -= (g.dv / den) * DInv / h_face(g, f) * pcL[Q];
+            }
+            pc[P] = (R(1) / Dp[P]) * (t + bp[P]);
+        });
+    }
+    // CSApplyVelCorrectionDivergenceTheorem, FvmCollNonUniform.compute:1487-1731.
+    void nu_apply_vel() {
+        for_cells([&](int x, int y, int z) {
+            if (!fluid(x, y, z)) return;
+            const size_t P = idx(x, y, z);
+            const Geo g = geo(x, y, z);
+            R pf[6];
+            for (int f = 0; f < 6; ++f) {
+                const Face& F = kFaces[f];
+                const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+                if (in_region(X, Y, Z)) {
+                    if (fluid(X, Y, Z)) {
+                        const R wP = w_self(g, f), wQ = R(1.0f) - wP;
+                        pf[f] = wP * pc[P] + wQ * pc[idx(X, Y, Z)];
+                    } else {
+                        pf[f] = pc[P];
+                    }
+                } else {
+                    pf[f] = cf.pres_bc[F.bc] == WF_BND_FIXED_VALUE ? R(0) : pc[P];
+                }
+            }
+            V3<R> corr;
+            for (int a = 0; a < 3; ++a)
+                corr.c[a] = -(g.dv / den) * (R(1) / Dv[P].c[a]) * (pf[2 * a] - pf[2 * a + 1]) / g.s[a].d;
+            velC[P] = corr;
+            for (int a = 0; a < 3; ++a) vel[P].c[a] += corr.c[a];
+        });
+    }
+    // CSInitLogVelPresFieldsNonUniform / CSSetLogVelBndCondNonUniform
+    // (InitShaderColl.compute:134-154, 287-300): the log profile at the cell
+    // centre height 0.5 (fy[y] + fy[y+1]).
+    R nu_centre_height(int y) const { return R(0.5) * (fpy[y] + fpy[y + 1]); }
+
     // ------------------------------------------------ momentum predictor
     // CSVelPredictPreCompute, FvmColl.compute:1292-1859.  bField holds the
     // LES term on entry (when LES is on) and b on exit.
     void op_vel_precompute() {
+        if (nonuniform) return nu_vel_precompute();
         for_cells([&](int x, int y, int z) {
             if (!fluid(x, y, z)) return;
             const size_t P = idx(x, y, z);
@@ -488,6 +793,7 @@ template <class R> struct Oracle {
     // CSVelPredict, FvmColl.compute:1863-2069: velField <- one Jacobi sweep
     // from velFieldLastIter.
     void vel_sweep() {
+        if (nonuniform) return nu_vel_sweep();
         for_cells([&](int x, int y, int z) {
             if (!fluid(x, y, z)) return;
             const size_t P = idx(x, y, z);
@@ -547,6 +853,7 @@ template <class R> struct Oracle {
     // ------------------------------------------------ pressure correction
     // CSPresCorrectRhieChowPreCompute, FvmColl.compute:2481-2787
     void op_pres_precompute() {
+        if (nonuniform) return nu_pres_precompute();
         const R dx2 = R(2) * dx;
         for_cells([&](int x, int y, int z) {
             if (!fluid(x, y, z)) return;
@@ -606,6 +913,7 @@ template <class R> struct Oracle {
     }
     // CSPresCorrectRhieChow, FvmColl.compute:2790-2848
     void pres_sweep() {
+        if (nonuniform) return nu_pres_sweep();
         for_cells([&](int x, int y, int z) {
             if (!fluid(x, y, z)) return;
             const size_t P = idx(x, y, z);
@@ -669,6 +977,7 @@ template <class R> struct Oracle {
     }
     // CSApplyVelCorrectionDivergenceTheorem, FvmColl.compute:2951-3121
     void op_apply_vel() {
+        if (nonuniform) return nu_apply_vel();
         for_cells([&](int x, int y, int z) {
             if (!fluid(x, y, z)) return;
             const size_t P = idx(x, y, z);
@@ -988,6 +1297,37 @@ int wfo_set_inflow_plane(wfo_solver* h, const float* pl) {
         using R = std::decay_t<decltype(o.dx)>;
         for (size_t i = 0; i < o.bnd[0].size(); ++i)
             for (int c = 0; c < 3; ++c) o.bnd[0][i].c[c] = R(pl[i * 3 + c]);
+        return int(WF_OK);
+    });
+}
+int wfo_set_face_positions(wfo_solver* h, const float* fx, const float* fy, const float* fz) {
+    return dispatch(h, [&](auto& o) {
+        using R = std::decay_t<decltype(o.dx)>;
+        if (!fx && !fy && !fz) {
+            o.nonuniform = false;
+            return int(WF_OK);
+        }
+        if (!fx || !fy || !fz) return int(WF_ERR_INVALID_ARG);
+        if (o.cf.solver_type != WF_SOLVER_SIMPLE || o.cf.turbulence != WF_TURB_NONE) return int(WF_ERR_UNSUPPORTED);
+        const float* f[3] = {fx, fy, fz};
+        const int n[3] = {o.nx, o.ny, o.nz};
+        for (int a = 0; a < 3; ++a)
+            for (int i = 0; i < n[a]; ++i)
+                if (!(f[a][i + 1] > f[a][i])) return int(WF_ERR_INVALID_ARG);
+        o.fpx.assign(fx, fx + o.nx + 1);
+        o.fpy.assign(fy, fy + o.ny + 1);
+        o.fpz.assign(fz, fz + o.nz + 1);
+        o.flux.assign(size_t(o.nx + 1) * (o.ny + 1) * (o.nz + 1), V3<R>{{R(0), R(0), R(0)}});
+        o.nonuniform = true;
+        return int(WF_OK);
+    });
+}
+int wfo_get_face_flux(wfo_solver* h, double* out) {
+    return dispatch(h, [&](auto& o) {
+        if (!out || !o.nonuniform) return int(WF_ERR_INVALID_ARG);
+        const size_t m = o.flux.size();
+        for (size_t i = 0; i < m; ++i)
+            for (int c = 0; c < 3; ++c) out[c * m + i] = double(o.flux[i].c[c]);
         return int(WF_OK);
     });
 }

@@ -42,6 +42,8 @@ int wfo_set_inflow_plane(wfo_solver* h, const float* x0_plane_xyz);
 int wfo_init_from_background(wfo_solver* h, const wfo_solver* bg, const float pos[3], const float pos_bg[3],
                              float rot_deg);
 int wfo_step(wfo_solver* h, int n_steps);
+int wfo_set_face_positions(wfo_solver* h, const float* fx, const float* fy, const float* fz);
+int wfo_get_face_flux(wfo_solver* h, double* out);
 
 /* Field transfer in FP64 (so the FP64 instance loses nothing); vectors SoA. */
 int wfo_field_size(const wfo_solver* h, int field, size_t* points, int* comps);

@@ -4,8 +4,9 @@ Parity is pinned on the reference's own kernels: FvmCollNonUniform.compute
 and InitShaderColl.compute translated to C++ (oracle/ref_kernels.py) and
 replayed in FvmSolverGpu's order (oracle/ref_driver.cpp), recorded in
 tests/golden/nonuniform_ref.npz by tests/golden/make_nu_golden.py.  The
-CUDA library must match every recorded field within REL_TOL = 1e-5 relative
-L2 per field and step.  The mesh generator restates InitMeshBuffers
+oracle's restatement must reproduce every recorded field bit for bit in
+FP32 and within 1e-5 in FP64; the CUDA library must match every recorded
+field within REL_TOL = 1e-5 relative L2 per field and step.  The mesh generator restates InitMeshBuffers
 (FvmSolverGpu.cs:682-788).
 """
 import os
@@ -66,6 +67,31 @@ def test_fixture_covers_cases():
                 assert np.isfinite(a).all() and np.abs(a).max() > 0.01, (name, k, key)
         for key, _ in G.LAST_FIELDS:
             assert np.isfinite(FIXTURE[f"{name}/{G.STEPS}/{key}"]).all()
+
+
+def _oracle_outputs(precision):
+    from oracle import OracleSolver
+    out = {}
+    for name in G.CASES:
+        def rec(step, key, a, name=name):
+            out[f"{name}/{step}/{key}"] = np.asarray(a)
+        G.run_case(lambda cfg: OracleSolver(cfg, precision), name, rec)
+    return out
+
+
+def test_oracle_fp32_bit_identical_to_reference_kernels(built):
+    """The oracle's C++ restatement of FvmCollNonUniform.compute (FP32, no
+    contraction) reproduces the reference's own kernels bit for bit."""
+    out = _oracle_outputs(32)
+    assert set(out) == set(FIXTURE.files)
+    for k, a in out.items():
+        assert np.array_equal(a.astype(np.float32), FIXTURE[k]), (k, float(np.abs(a - FIXTURE[k]).max()))
+
+
+def test_oracle_fp64_within_fp32_rounding_of_reference_kernels(built):
+    out = _oracle_outputs(64)
+    for k, a in out.items():
+        assert rel_l2(a, FIXTURE[k]) <= 1e-5, k
 
 
 def test_reference_kernels_reproduce_fixture():
