@@ -516,24 +516,26 @@ def run_windfvm(args):
                       "runs the next step)"}
 
     # ---- roofline of the dominant kernel ----
-    # The momentum sweep (50 launches, 40.4 % of the step's kernel time) and
-    # the four-sweep pressure wavefront (30 launches, 40.2 %) share the step;
-    # the roofline object is the momentum sweep, the pressure kernel's
-    # figures ride beside it.
+    # The four-sweep pressure wavefront (30 launches, 42 % of the step's
+    # kernel time) leads the momentum sweep (50 launches, 39 %); the roofline
+    # object is the pressure wavefront, the momentum sweep's figures ride
+    # beside it.  Achieved = algorithmic bytes of the launch's sweeps over
+    # its CUDA-event time; traffic = DRAM bytes of one launch (ncu), below
+    # the algorithmic bytes because the wavefront keeps 4 sweeps on chip.
     peak, peak_kind = measured_peaks()
     v_ms, v_bytes, v_sweeps = solver.time_kernel(_lib.KERNEL_VEL_SWEEP, reps=20, flush_l2=True)
     k_ms, k_bytes, k_sweeps = solver.time_kernel(_lib.KERNEL_PRES_SWEEP, reps=20, flush_l2=True)
     v_gbs = v_bytes / (v_ms / 1e3) / 1e9
     k_gbs = k_bytes / (k_ms / 1e3) / 1e9
     tv, tp = committed_traffic("vel_sweep"), committed_traffic("pres_sweep")
-    roofline = {"bound": "hbm", "achieved": v_gbs, "peak": peak, "unit": "GB/s", "frac": v_gbs / peak,
-                "traffic": (tv * N) if tv is not None else None,
-                "kernel": "momentum Jacobi sweep (four cells per thread)", "ms_per_launch": v_ms,
-                "sweeps_per_launch": v_sweeps, "alg_bytes_per_launch": v_bytes,
+    roofline = {"bound": "hbm", "achieved": k_gbs, "peak": peak, "unit": "GB/s", "frac": k_gbs / peak,
+                "traffic": (tp * N) if tp is not None else None,
+                "kernel": "pressure Jacobi wavefront (4 sweeps per launch)", "ms_per_launch": k_ms,
+                "sweeps_per_launch": k_sweeps, "alg_bytes_per_launch": k_bytes,
                 "peak_source": f"hbm_gbs of {peak_kind}"}
-    pres_kernel = {"kernel": "pressure Jacobi wavefront", "ms_per_launch": k_ms, "sweeps_per_launch": k_sweeps,
-                   "alg_bytes_per_launch": k_bytes, "achieved_gbs": k_gbs, "frac": k_gbs / peak,
-                   "traffic": (tp * N) if tp is not None else None}
+    vel_kernel = {"kernel": "momentum Jacobi sweep (four cells per thread)", "ms_per_launch": v_ms,
+                  "sweeps_per_launch": v_sweeps, "alg_bytes_per_launch": v_bytes, "achieved_gbs": v_gbs,
+                  "frac": v_gbs / peak, "traffic": (tv * N) if tv is not None else None}
     step_gbs = value / world * b_alg(cfg.vel_iters, cfg.pres_iters, cfg.piso_correctors) / 1e3
 
     solver.close()
@@ -564,7 +566,7 @@ def run_windfvm(args):
             "cpu_baseline": cpu,
             "step_alg_gbs": step_gbs, "step_alg_frac": step_gbs / peak,
             "step_phases_ms": phases,
-            "pres_sweep_kernel": pres_kernel,
+            "vel_sweep_kernel": vel_kernel,
             "batched": batched,
             "batched_small_cases": batched_small,
             "adjoint": adjoint,
