@@ -243,3 +243,23 @@ def test_chained_launches_equal_plain_stream_order(monkeypatch):
     for other in outs[1:]:
         for k in outs[0]:
             assert np.array_equal(outs[0][k], other[k]), k
+
+
+@pytest.mark.parametrize("name", list(G.CASES))
+def test_momentum_diagonal_components_equal_off_symmetry(built, name):
+    """On the non-uniform grid too, the three components of D
+    (CSVelPredictPreCompute, FvmCollNonUniform.compute:111-721) are
+    bit-identical outside cells with a symmetry domain face, which the
+    momentum sweeps rely on when they read one component of 1/D there
+    (FP32 oracle after 3 steps)."""
+    from oracle import OracleSolver
+    from test_oracle import _d_split_mask
+    case = G.make_case(name)
+    o = OracleSolver(case.cfg, 32)
+    cases.apply_case(o, case)
+    o.Step(3)
+    D = np.asarray(o.get_field(_lib.FIELD_D), dtype=np.float32).reshape(3, -1)
+    keep = (case.flags.reshape(-1) == 0) & ~_d_split_mask(case.cfg, o.shape)
+    assert keep.sum() > 0
+    assert np.array_equal(D[0][keep].view(np.uint32), D[1][keep].view(np.uint32))
+    assert np.array_equal(D[0][keep].view(np.uint32), D[2][keep].view(np.uint32))

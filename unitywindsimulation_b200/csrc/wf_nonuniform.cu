@@ -17,7 +17,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <string>
 
 #include "wf_common.cuh"
 #include "wf_kernels.cuh"
