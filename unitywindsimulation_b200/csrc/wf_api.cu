@@ -251,7 +251,7 @@ int do_pres_sweeps(wf_solver* h, int n, bool allow_fast) {
     for (int k = 0; k < n; ++k) {
         const float* src = h->pc_zero ? nullptr : h->pcb[h->iPCL];
         if (h->nonuniform)
-            wf::launch_nu_pres_sweep(h, src, h->pcb[h->iPC]);
+            wf::launch_nu_pres_sweep(h, src, h->pcb[h->iPC], k > 0);
         else
             wf::launch_pres_sweep(P, h->st, h->fl, src, h->Dv, h->Dp, h->bp, h->pcb[h->iPC]);
         WF_CHECK_LAUNCH();

@@ -100,19 +100,20 @@ __device__ __forceinline__ bool d_split(const Params& P, int x0, int x1, int y, 
            (z == P.nz - 1 && P.vbc[WF_FACE_ZN] == WF_BND_SYMMETRY);
 }
 
-// Programmatic dependent launch inside a chain of Jacobi sweeps: the block
-// lets the next launch of the chain be scheduled (all blocks of this grid
-// have started once every block has passed this point), then waits until
-// the previous grid in the stream has completed and its writes are visible.
-// Every global access of the kernel follows it.  Without the launch
-// attribute both calls return at once.
-__device__ __forceinline__ void chain_entry() {
-    cudaTriggerProgrammaticLaunchCompletion();
-    cudaGridDependencySynchronize();
-}
+// Programmatic dependent launch inside a chain of Jacobi sweeps.
+// chain_wait: wait until the previous grid in the stream has completed and
+// its writes are visible.  chain_release (after chain_wait): let the next
+// launch of the chain be scheduled; it then starts once every block of
+// this grid has passed this point, i.e. after the grid before this one has
+// completed, so data written before that grid (the step's coefficient
+// planes) may be read before the next grid's own chain_wait.  Without the
+// launch attribute both calls return at once.
+__device__ __forceinline__ void chain_wait() { cudaGridDependencySynchronize(); }
+__device__ __forceinline__ void chain_release() { cudaTriggerProgrammaticLaunchCompletion(); }
 
 // Launches kernel<<<grid, block, 0, st>>>(args...), as a programmatic
-// dependent launch when `chained` (the kernel must start with chain_entry).
+// dependent launch when `chained` (the kernel calls chain_wait before it
+// reads the previous grid's output, then chain_release).
 template <typename... KArgs, typename... Args>
 inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, bool chained,
                                   Args... args) {

@@ -67,7 +67,7 @@ constexpr int kNuCoefPlanes = 7;  // per-step pressure-sweep coefficients of the
 size_t nu_flux_texels(const Params& P);
 void launch_nu_vel_precompute(const wf_solver* h);
 void launch_nu_pres_precompute(wf_solver* h, const float* u);
-void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout);
+void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout, bool pre);
 void launch_nu_apply_vel(wf_solver* h, const float* pc, float* u);
 void launch_nu_init_log(wf_solver* h, float fric, float kappa, float z0);
 void launch_nu_log_inlet(wf_solver* h, float fric, float kappa, float z0);

@@ -389,7 +389,8 @@ __global__ void __launch_bounds__(256) k_nu_pres_sweep(const __grid_constant__ P
                                                        const float* __restrict__ pin,
                                                        const float* __restrict__ coef,
                                                        const float* __restrict__ bp, float* __restrict__ pout) {
-    chain_entry();
+    chain_wait();
+    chain_release();
     int x, y, z, i;
     if (!linear_cell(P, x, y, z, i)) return;
     const size_t N = P.N;
@@ -418,25 +419,48 @@ __device__ __forceinline__ float4 ld4n(const float* p, size_t i) {
 }
 __device__ __forceinline__ float c4(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
 
+// The per-step inputs of four cells' pressure updates: neighbour masks,
+// face coefficients, 1/Dp and bp.
+struct NuPresCoef {
+    uchar4 mq;
+    float4 c[6], inv, b;
+};
+__device__ __forceinline__ NuPresCoef nu_pres_coef(const Params& P, const float* coef, const float* bp, int i) {
+    const size_t N = P.N;
+    NuPresCoef k;
+    k.mq = __ldg(reinterpret_cast<const uchar4*>(P.nbm + i));
+#pragma unroll
+    for (int f = 0; f < 6; ++f) k.c[f] = ld4n(coef, (kCoefP + f) * N + i);
+    k.inv = ld4n(coef, kCoefInvDp * N + i);
+    k.b = ld4n(bp, i);
+    return k;
+}
+
 __global__ void __launch_bounds__(256) k_nu_pres_sweep4(const __grid_constant__ Params P,
                                                         const float* __restrict__ pin,
                                                         const float* __restrict__ coef,
-                                                        const float* __restrict__ bp, float* __restrict__ pout) {
-    chain_entry();
+                                                        const float* __restrict__ bp, float* __restrict__ pout,
+                                                        int pre) {
+    // pre: the coefficient planes, bp and the masks were written before the
+    // previous grid of the chain (every sweep after the first): they load
+    // before chain_wait.
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= P.N / 4) return;
-    const int i = 4 * q;
+    const bool in = q < P.N / 4;
+    const int i = in ? 4 * q : 0;
+    NuPresCoef k{};
+    if (pre && in) k = nu_pres_coef(P, coef, bp, i);
+    chain_wait();
+    chain_release();
+    if (!in) return;
+    if (!pre) k = nu_pres_coef(P, coef, bp, i);
+    const uchar4 mq = k.mq;
+    const float4* c = k.c;
+    const float4 inv = k.inv, b = k.b;
     const int x0 = i % P.nx, r = i / P.nx, y = r % P.ny, z = r / P.ny;
-    const size_t N = P.N;
     const int sx = P.nx, sz = P.nx * P.ny;
     const int iN = y + 1 < P.ny ? i + sx : i, iS = y > 0 ? i - sx : i;
     const int iU = z + 1 < P.nz ? i + sz : i, iDn = z > 0 ? i - sz : i;
     const int iE = x0 + 4 < P.nx ? i + 4 : i + 3, iW = x0 > 0 ? i - 1 : i;
-    const uchar4 mq = __ldg(reinterpret_cast<const uchar4*>(P.nbm + i));
-    float4 c[6];
-#pragma unroll
-    for (int f = 0; f < 6; ++f) c[f] = ld4n(coef, (kCoefP + f) * N + i);
-    const float4 inv = ld4n(coef, kCoefInvDp * N + i), b = ld4n(bp, i);
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 pc = pin ? ld4n(pin, i) : z4, pn = pin ? ld4n(pin, iN) : z4, ps = pin ? ld4n(pin, iS) : z4;
     const float4 pu = pin ? ld4n(pin, iU) : z4, pd = pin ? ld4n(pin, iDn) : z4;
@@ -572,14 +596,15 @@ void launch_nu_pres_precompute(wf_solver* h, const float* u) {
                                                                 h->flux, h->Dp, h->bp, h->nucoef);
 }
 
-void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout) {
+void launch_nu_pres_sweep(const wf_solver* h, const float* pin, float* pout, bool pre) {
     const Params& P = h->P;
     WF_COUNT_LAUNCH();
     const float* c = h->nucoef;
     const float* b = h->bp;
     if (quad_ok(P, {pin, h->nucoef, h->bp, pout, P.nbm})) {
         const int nq = P.N / 4;
-        launch_chained(k_nu_pres_sweep4, dim3((nq + 255) / 256), dim3(256), h->st, h->pdl != 0, P, pin, c, b, pout);
+        launch_chained(k_nu_pres_sweep4, dim3((nq + 255) / 256), dim3(256), h->st, h->pdl != 0, P, pin, c, b, pout,
+                       (h->pdl != 0 && pre) ? 1 : 0);
     } else {
         launch_chained(k_nu_pres_sweep, dim3((P.N + 255) / 256), dim3(256), h->st, h->pdl != 0, P, pin, c, b, pout);
     }

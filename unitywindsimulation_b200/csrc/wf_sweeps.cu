@@ -171,7 +171,8 @@ template <bool kCopyAll = false>
 __global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Params P, const float* __restrict__ A,
                                                     const float* __restrict__ iD, const float* __restrict__ bv,
                                                     const float* __restrict__ ui, float* __restrict__ uo) {
-    chain_entry();
+    chain_wait();
+    chain_release();
     const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -743,8 +744,8 @@ void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
     const size_t N = P.N;
     WF_COUNT_LAUNCH();
     if (vec4_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst)) {
-        // the non-uniform grid's short sweeps chain with programmatic
-        // dependent launch (chain_entry)
+        // consecutive sweeps chain as programmatic dependent launches
+        // (chain_wait / chain_release)
         launch_chained(k_vel_sweep4<false>, grd4(P), blk(), h->st, h->pdl != 0, P,
                        (const float*)h->vcoef, (const float*)(h->vcoef + 6 * N), (const float*)h->bv, src, dst);
     } else {
