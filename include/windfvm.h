@@ -176,6 +176,10 @@ int wf_set_face_positions(wf_solver* h, const float* face_x, const float* face_y
  * FvmCollNonUniform.compute:1335-1341): three planes (x, y, z components)
  * of (nx+1)*(ny+1)*(nz+1) texels, x fastest. */
 int wf_get_face_flux(wf_solver* h, float* out);
+/* Writes the face-flux texture (same layout).  With wf_get_state /
+ * wf_set_state it makes a checkpoint of a non-uniform handle exact: the
+ * next step's momentum pre-compute reads the fluxes of the previous step. */
+int wf_set_face_flux(wf_solver* h, const float* in);
 /* InitVelPresFieldsFromBackGroundFlow (FvmSolverGpu.cs:898-929, kernel
  * CSInitVelPresFieldsFromBGFlowRotate, InitShaderColl.compute:185-226): sets
  * every cell's velocity (all iterate buffers) and pressure to the

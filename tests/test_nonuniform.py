@@ -263,3 +263,43 @@ def test_momentum_diagonal_components_equal_off_symmetry(built, name):
     assert keep.sum() > 0
     assert np.array_equal(D[0][keep].view(np.uint32), D[1][keep].view(np.uint32))
     assert np.array_equal(D[0][keep].view(np.uint32), D[2][keep].view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_checkpoint_with_face_flux_resumes_exactly():
+    """wf_get_state / wf_set_state plus the face-flux texture restore a
+    non-uniform handle exactly: two more steps from the checkpoint on a
+    fresh handle give the fields of two more steps on the original."""
+    from unitywindsimulation_b200.solver import FvmSolverCuda
+    case = G.make_case("log_urban_normalised")
+    a = FvmSolverCuda(case.cfg)
+    cases.apply_case(a, case)
+    a.Step(2)
+    vel, pres, step = a.get_state()
+    flux = a.get_face_flux()
+    b = FvmSolverCuda(case.cfg)
+    cases.apply_case(b, case)
+    b.set_state(vel, pres, step)
+    b.set_face_flux(flux)
+    a.Step(2)
+    b.Step(2)
+    for f in (_lib.FIELD_VEL_LAST_TIME, _lib.FIELD_PRES):
+        assert np.array_equal(a.get_field(f), b.get_field(f)), f
+    assert np.array_equal(a.get_face_flux(), b.get_face_flux())
+
+
+@pytest.mark.gpu
+def test_traced_step_equals_plain_step():
+    """wf_step_phases on a non-uniform handle leaves the same fields as a
+    plain step."""
+    from unitywindsimulation_b200.solver import FvmSolverCuda
+    case = G.make_case("const_tunnel")
+    a, b = FvmSolverCuda(case.cfg), FvmSolverCuda(case.cfg)
+    for s in (a, b):
+        cases.apply_case(s, case)
+    a.Step(2)
+    b.Step(1)
+    ms = b.step_phases()
+    assert all(v >= 0.0 for v in ms.values())
+    for f in (_lib.FIELD_VEL_LAST_TIME, _lib.FIELD_PRES):
+        assert np.array_equal(a.get_field(f), b.get_field(f)), f

@@ -135,6 +135,7 @@ _SIGNATURES = {
     "wf_change_phys_field_pos": (c_int, [c_void_p]),
     "wf_set_face_positions": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
     "wf_get_face_flux": (c_int, [c_void_p, POINTER(c_float)]),
+    "wf_set_face_flux": (c_int, [c_void_p, POINTER(c_float)]),
     "wf_init_from_background": (c_int, [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float), c_float]),
     "wf_set_inflow_plane": (c_int, [c_void_p, POINTER(c_float)]),
     "wf_step": (c_int, [c_void_p, c_int, POINTER(c_int)]),

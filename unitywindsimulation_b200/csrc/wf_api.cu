@@ -737,6 +737,15 @@ int wf_set_face_positions(wf_solver* h, const float* fx, const float* fy, const 
     return sync(h);
 }
 
+int wf_set_face_flux(wf_solver* h, const float* in) {
+    if (!h || !in) return WF_ERR_INVALID_ARG;
+    if (!h->nonuniform) return set_err(h, WF_ERR_INVALID_ARG, "no non-uniform grid set");
+    WF_CUDA(cudaSetDevice(h->device));
+    WF_CUDA(cudaMemcpyAsync(h->flux, in, 3 * wf::nu_flux_texels(h->P) * sizeof(float), cudaMemcpyHostToDevice,
+                            h->st));
+    return sync(h);
+}
+
 int wf_get_face_flux(wf_solver* h, float* out) {
     if (!h || !out) return WF_ERR_INVALID_ARG;
     if (!h->nonuniform) return set_err(h, WF_ERR_INVALID_ARG, "no non-uniform grid set");

@@ -103,6 +103,14 @@ class FvmSolverCuda:
             raise ValueError("face positions need nx+1, ny+1 and nz+1 values")
         self._check(self._lib.wf_set_face_positions(self._h, *[v.ctypes.data_as(POINTER(c_float)) for v in a]))
 
+    def set_face_flux(self, flux) -> None:
+        """Writes the face-flux texture, (3, nz+1, ny+1, nx+1) (wf_set_face_flux)."""
+        c = self.cfg
+        a = np.ascontiguousarray(flux, dtype=np.float32).reshape(-1)
+        if a.size != 3 * (c.nx + 1) * (c.ny + 1) * (c.nz + 1):
+            raise ValueError("face flux needs 3 (nx+1)(ny+1)(nz+1) values")
+        self._check(self._lib.wf_set_face_flux(self._h, a.ctypes.data_as(POINTER(c_float))))
+
     def get_face_flux(self) -> np.ndarray:
         """Face-flux texture of the non-uniform grid, (3, nz+1, ny+1, nx+1)."""
         c = self.cfg
