@@ -36,6 +36,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s"
 B_ALG_FIXED = 287  # compulsory bytes per cell-step of the non-iterative kernels
+# Wall-clock bound of the reference arm (warm-up and timed steps together):
+# at 9-16 s per urban-block step on 16 host cores, 25 steps fit.
+REFERENCE_BUDGET_S = 900.0
 
 
 def b_alg(nv: int, np_: int, nc: int) -> int:
@@ -60,6 +63,11 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the host-core baselines of every workload (no GPU) and exit")
+    ap.add_argument("--kernels", action="store_true",
+                    help="step the workload --steps times and time its two Jacobi kernels, nothing else "
+                         "(the target program of an ncu capture); prints one JSON line")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="with --kernels: also run the objective gradient over --steps steps")
     return ap.parse_args()
 
 
@@ -145,13 +153,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def host_step_sampler(case, max_steps: int, budget_s: float):
-    """Times whole steps of the workload on all host cores until `max_steps`
-    steps or `budget_s` seconds (at least one step).  With the reference's
-    own kernels built (oracle/_ref/: its compute shaders translated to C++,
-    dispatched in FvmSolverGpu's order) they are what is timed, kind
-    "reference"; otherwise the FP32 oracle, kind "port".  The state (flags,
-    inflow plane, initial fields) is set up by the oracle in both cases."""
+def host_state(case):
+    """The workload's set-up state on the host cores, ready to step: the
+    reference's own kernels where they are built (oracle/_ref/: its compute
+    shaders translated to C++, dispatched in FvmSolverGpu's order), kind
+    "reference", else the FP32 oracle, kind "port".  The state (flags, inflow
+    plane, initial fields) is set up by the oracle in both cases: the
+    workload's friction-velocity inflow and perturbed inlet plane have no
+    set-up kernel in the reference."""
     from oracle import OracleSolver
     from oracle.binding import RefSolver, ref_available
     cores = os.cpu_count() or 1
@@ -163,10 +172,16 @@ def host_step_sampler(case, max_steps: int, budget_s: float):
         s = RefSolver(case.cfg, construct=False)
         s.copy_state_from(o)
         o.close()
-        kind, what = "reference", "the reference's own kernels (FvmColl/PisoColl/LES/WallFunc compute shaders " \
-                                  "compiled as C++, FP32, OpenMP over z)"
-    else:
-        s, kind, what = o, "port", "the FP32 oracle (C++ restatement, OpenMP over z)"
+        return s, cores, "reference", "the reference's own kernels (FvmColl/PisoColl/LES/WallFunc compute " \
+                                      "shaders compiled as C++, FP32, OpenMP over z)"
+    return o, cores, "port", "the FP32 oracle (C++ restatement, OpenMP over z)"
+
+
+def host_step_sampler(case, max_steps: int, budget_s: float):
+    """Times whole steps of the workload on all host cores until `max_steps`
+    steps or `budget_s` seconds (at least one step), from the state of
+    host_state()."""
+    s, cores, kind, what = host_state(case)
     done, t0 = 0, time.perf_counter()
     while done < max(1, max_steps):
         s.Step(1)
@@ -174,6 +189,7 @@ def host_step_sampler(case, max_steps: int, budget_s: float):
         if time.perf_counter() - t0 >= budget_s:
             break
     dt = time.perf_counter() - t0
+    s.close()
     return case.n_cells * done / dt / 1e6, dt, done, cores, kind, what
 
 
@@ -399,21 +415,43 @@ def nonuniform_section(local: int, steps: int, cpu: bool):
 
 
 def run_reference(args):
+    """The reference arm: W untimed and then K timed whole steps of the
+    workload on the host cores (host_state), rank 0 only.  The line reports
+    the steps and warm-up steps it ran; a run that would pass
+    REFERENCE_BUDGET_S stops early and says so."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     case = make_case(args.workload)
-    k = max(1, min(args.steps, 6))
-    v, dt, done, cores, kind, what = host_step_sampler(case, k, 90.0)
+    s, cores, kind, what = host_state(case)
+    t_start = time.perf_counter()
+    warm = 0
+    for _ in range(args.warmup):
+        s.Step(1)
+        warm += 1
+    done, t0 = 0, time.perf_counter()
+    per_step = (t0 - t_start) / warm if warm else 0.0
+    while done < max(1, args.steps):
+        if done and time.perf_counter() - t_start + per_step > REFERENCE_BUDGET_S:
+            break
+        t1 = time.perf_counter()
+        s.Step(1)
+        per_step = time.perf_counter() - t1
+        done += 1
+    dt = time.perf_counter() - t0
+    s.close()
+    v = case.n_cells * done / dt / 1e6
+    cut = "" if done == max(1, args.steps) else f"; stopped after {done} of {args.steps} steps at the " \
+                                                f"{REFERENCE_BUDGET_S:.0f} s budget"
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / done, "higher_is_better": True,
+        "steps": done, "warmup": warm, "ms_per_step": dt * 1e3 / done, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(case),
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": kind,
-                         "sample": f"{done} full steps of {case.name} ({dt:.1f} s, at most {k} steps or 90 s) "
+                         "sample": f"{warm} untimed and {done} timed full steps of {case.name} ({dt:.1f} s timed) "
                                    f"with {what}, {cores} threads; the reference's host (C# under Unity, "
-                                   f"D3D dispatch) cannot run here"},
+                                   f"D3D dispatch) cannot run here{cut}"},
         "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -577,8 +615,41 @@ def run_windfvm(args):
     return 0
 
 
+def run_kernels(args):
+    """A short run of the workload: --steps graph-replayed steps, then the
+    two Jacobi kernels timed alone (CUDA events, cold L2), optionally the
+    objective gradient over --steps steps.  Meant as the program an ncu
+    capture (`ncu -k regex:<kernel> -s <n> -c <m>`) runs."""
+    from unitywindsimulation_b200 import FvmSolverCuda, _lib, cases
+    from unitywindsimulation_b200.adjoint import AdjointSolver, Objective
+
+    case = make_case(args.workload)
+    s = FvmSolverCuda(case.cfg)
+    cases.apply_case(s, case)
+    s.Step(args.steps)
+    out = {"workload": args.workload, "cells": case.n_cells, "step_ms": s.last_step_ms() / max(args.steps, 1)}
+    if case.faces is None:
+        for name, k in (("pres_sweep", _lib.KERNEL_PRES_SWEEP), ("vel_sweep", _lib.KERNEL_VEL_SWEEP)):
+            ms, by, sw = s.time_kernel(k, reps=2, flush_l2=True)
+            out[name] = {"ms_per_launch": ms, "sweeps_per_launch": sw, "alg_gbs": by / (ms / 1e3) / 1e9}
+    s.close()
+    if args.adjoint:
+        s = FvmSolverCuda(case.cfg)
+        cases.apply_case(s, case)
+        nx, nz = case.cfg.nx, case.cfg.nz
+        obj = Objective(x0=nx // 4, x1=3 * nx // 4, z0=nz // 4, z1=3 * nz // 4, y=min(3, case.cfg.ny - 1), window=1)
+        with AdjointSolver(s) as adj:
+            r = adj.gradient(obj, args.steps, args.steps, soft=case.soft)
+        out["adjoint"] = {"gradient_ms": r["ms_total"], "forward_pass_ms": r["ms_forward"], "J": r["J"]}
+        s.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.kernels:
+        return run_kernels(args)
     if args.cpu_table:
         print(json.dumps(cpu_table()), flush=True)
         return 0

@@ -539,8 +539,8 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
  * the host application, a real-time loop that cannot afford cudaMalloc's
  * implicit device synchronisation, a process with a locked-down allocator.
  *
- * Computes the reference's continuity residual, sqrt(sum (Dp*(p'-p'_last))^2
- * / n) (CSComputePresCorrectResidual + host normalisation), of caller-owned
+ * Computes the continuity residual sqrt(sum_i (Dp_i*(p'_i - p'last_i))^2 / n)
+ * (the same norm wf_residuals reports for the pressure loop) of caller-owned
  * device arrays of n_cells floats; d_pc_last may be NULL (all-zero iterate).
  * `stream` is a cudaStream_t (NULL: the legacy default stream); the call
  * returns after that stream has finished the reduction, with the norm in
@@ -551,9 +551,12 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
  * until the process exits.  The call makes no cudaMalloc/cudaFree or other
  * allocating call.  Every call shares that array and overwrites what the
  * previous call left there, so calls that overlap on the GPU (different
- * streams or threads) race and must be serialised by the caller.  The first
- * call on each device looks up the array's device address (with that device
- * current); make that first call before any stream capture.
+ * streams or threads) race and must be serialised by the caller.  Every
+ * call looks up the array's device address in the CUDA context current on
+ * the calling thread (an address is not cached across contexts, so a host
+ * context or a cudaDeviceReset between calls is safe); the first call in a
+ * context also loads the library's device code there, so make that first
+ * call before any stream capture.
  * Returns WF_ERR_INVALID_ARG for NULL inputs or when n_cells is < 1 or larger
  * than WF_NOALLOC_MAX_CELLS, WF_ERR_CUDA when a CUDA call fails. */
 #define WF_NOALLOC_BLOCKS 4096

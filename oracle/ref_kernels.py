@@ -67,6 +67,8 @@ def generate(ref_root: str) -> list[str]:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: ref_kernels.py <reference checkout root>")
+    root = sys.argv[1]
     for p in generate(root):
         print(p)

@@ -80,4 +80,7 @@ def main(reference_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WINDFVM_REFERENCE_ROOT", "/root/reference"))
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WINDFVM_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_nu_golden.py <reference checkout root> (or set WINDFVM_REFERENCE_ROOT)")
+    main(root)

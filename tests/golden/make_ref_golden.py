@@ -104,7 +104,9 @@ def all_outputs(make_solver):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WINDFVM_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_ref_golden.py <reference checkout root> (or set WINDFVM_REFERENCE_ROOT)")
     from oracle.binding import RefSolver, build_ref
     build_ref(root)
     out = all_outputs(RefSolver)

@@ -54,6 +54,28 @@ def test_noalloc_residual_matches_solver_entry_point(built):
     assert seen[0] != seen[1]
 
 
+def test_noalloc_leaves_free_device_memory_unchanged(built):
+    """After a first call (which may load the library's device code into the
+    context), further calls take no device memory: the device's free memory
+    is the same before and after them."""
+    import torch
+
+    lib = _lib.load()
+    n = 1 << 20
+    d_dp = torch.ones(n, device="cuda")
+    d_pc = torch.full((n,), 2.0, device="cuda")
+    torch.cuda.synchronize()
+    assert _noalloc(lib, d_dp.data_ptr(), d_pc.data_ptr(), None, n)[0] == _lib.WF_OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        st, got = _noalloc(lib, d_dp.data_ptr(), d_pc.data_ptr(), None, n)
+        assert st == _lib.WF_OK and got == pytest.approx(2.0, rel=REL_TOL)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_null_last_iterate_and_limits(built):
     import torch
 

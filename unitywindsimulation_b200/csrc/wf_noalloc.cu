@@ -13,24 +13,16 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 #include "wf_common.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
 
 // Block partial sums [0, WF_NOALLOC_BLOCKS) and the final sum at
 // [WF_NOALLOC_BLOCKS].  Shared by every call on a device.
 static __device__ __align__(256) double g_noalloc_scratch[WF_NOALLOC_BLOCKS + 1];
-
-// Device address of g_noalloc_scratch per device ordinal, looked up once.
-// Host code must not pass the symbol itself to a kernel: on the host it
-// names a stand-in, not device memory.
-double* g_scratch_ptr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
 
 __global__ void k_noalloc_partials(const float* __restrict__ dp, const float* __restrict__ pc,
                                    const float* __restrict__ pcl, long long n, double* __restrict__ part) {
@@ -65,19 +57,29 @@ __global__ void k_noalloc_total(double* __restrict__ scratch, int nblocks) {
     if (threadIdx.x == 0) scratch[WF_NOALLOC_BLOCKS] = sh[0];
 }
 
-// Looks up (once per device, with that device current) the device address
-// of the scratch array.
-int scratch_for_current_device(double** out) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WF_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        double* p = nullptr;
-        if (cudaGetSymbolAddress((void**)&p, g_noalloc_scratch) != cudaSuccess || !p) return WF_ERR_CUDA;
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+// The device address of the scratch array in the CUDA context current on
+// the calling thread.  Looked up on every call rather than cached: an address
+// belongs to one context, and a host may call from a context it created
+// itself, or after cudaDeviceReset replaced the primary context.  The lookup
+// allocates nothing; the first one in a context loads the library's device
+// code into it.  Host code must never pass g_noalloc_scratch itself to a
+// kernel: on the host the name is a stand-in, not device memory.
+int scratch_for_current_context(double** out) {
+    double* p = nullptr;
+    if (cudaGetSymbolAddress((void**)&p, g_noalloc_scratch) != cudaSuccess || !p) return WF_ERR_CUDA;
+    *out = p;
     return WF_OK;
+}
+
+// Launches kernel<<<grid, block, 0, st>>>(args...) and returns that launch's
+// own status (not an error left behind by some earlier, unrelated call).
+template <typename... KArgs, typename... Args>
+cudaError_t launch(void (*kernel)(KArgs...), int grid, int block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 }  // namespace
@@ -87,14 +89,15 @@ extern "C" int wf_pres_residual_noalloc(const float* d_dp, const float* d_pc, co
     if (!d_dp || !d_pc || !out) return WF_ERR_INVALID_ARG;
     if (n_cells < 1 || n_cells > (int64_t)WF_NOALLOC_MAX_CELLS) return WF_ERR_INVALID_ARG;
     double* scratch = nullptr;
-    const int s = scratch_for_current_device(&scratch);
+    const int s = scratch_for_current_context(&scratch);
     if (s != WF_OK) return s;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     long long want = (n_cells + kThreads - 1) / kThreads;
     const int nblocks = (int)(want < WF_NOALLOC_BLOCKS ? want : WF_NOALLOC_BLOCKS);
-    k_noalloc_partials<<<nblocks, kThreads, 0, st>>>(d_dp, d_pc, d_pc_last, (long long)n_cells, scratch);
-    k_noalloc_total<<<1, kThreads, 0, st>>>(scratch, nblocks);
-    if (cudaGetLastError() != cudaSuccess) return WF_ERR_CUDA;
+    if (launch(k_noalloc_partials, nblocks, kThreads, st, d_dp, d_pc, d_pc_last, (long long)n_cells, scratch) !=
+        cudaSuccess)
+        return WF_ERR_CUDA;
+    if (launch(k_noalloc_total, 1, kThreads, st, scratch, nblocks) != cudaSuccess) return WF_ERR_CUDA;
     double total = 0.0;
     if (cudaMemcpyAsync(&total, scratch + WF_NOALLOC_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, st) !=
         cudaSuccess)
