@@ -39,6 +39,8 @@ B_ALG_FIXED = 287  # compulsory bytes per cell-step of the non-iterative kernels
 # Wall-clock bound of the reference arm (warm-up and timed steps together):
 # at 9-16 s per urban-block step on 16 host cores, 25 steps fit.
 REFERENCE_BUDGET_S = 900.0
+# Timed steps of each form in the batched sections.
+BATCH_STEPS = 30
 
 
 def b_alg(nv: int, np_: int, nc: int) -> int:
@@ -268,11 +270,14 @@ def batched_section(steps: int, local: int, small: bool = False):
     """Batched form on 16 cases: the direction sweep (uneven grids 96..192 x
     48..80(up) x 96..160, wind rotated by 22.5 degree steps), or with
     small=True 16 small grids (about 0.1 M cells each).  The same cases are
-    stepped one after another (plain form) and together in one graph launch
-    per step (batched form), both after autotuning the blocking depths per
-    grid size and with every step graph captured before timing.  Device
-    time from CUDA events."""
-    from unitywindsimulation_b200 import FvmSolverCuda, autotune, cases
+    stepped one after another (plain form) and together (batched form), both
+    after autotuning the blocking depths and tiles per grid size and with
+    every step graph captured before timing.  The batched form is timed in
+    both modes over `steps` steps: child graphs (one parent graph launch per
+    step, autotuned chain width) and persistent loops (one cooperative launch
+    per Jacobi loop over all cases); the faster is the batched figure.
+    Device time from CUDA events."""
+    from unitywindsimulation_b200 import FvmSolverCuda, _lib, autotune, cases
     from unitywindsimulation_b200.solver import BatchSolver
 
     cs = cases.batch_small() if small else cases.batch_directions()
@@ -293,22 +298,32 @@ def batched_section(steps: int, local: int, small: bool = False):
         s.Step(steps)
         plain_ms += s.last_step_ms()
     b = BatchSolver(solvers)
-    width = autotune.tune_batch(b, steps=2)
-    l0 = b.kernel_launches()
-    b.step(steps)
-    batched_ms = b.last_step_ms()
-    launches = b.kernel_launches() - l0
+    width = autotune.tune_batch(b, steps=2, modes=(_lib.BATCH_GRAPHS,))
+    modes = {}
+    for name, mode in (("graphs", _lib.BATCH_GRAPHS), ("persistent", _lib.BATCH_PERSISTENT)):
+        b.set_mode(mode)
+        if mode == _lib.BATCH_GRAPHS:
+            b.set_width(width["width"])
+        b.step(1)
+        b.prepare_graphs()
+        l0 = b.kernel_launches()
+        b.step(steps)
+        ms = b.last_step_ms()
+        modes[name] = {"mcell_steps_s": cells * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+                       "gpu_launches": b.kernel_launches() - l0}
     b.close()
     for s in solvers:
         s.close()
     plain = cells * steps / (plain_ms / 1e3) / 1e6
-    batched = cells * steps / (batched_ms / 1e3) / 1e6
+    best = max(modes, key=lambda k: modes[k]["mcell_steps_s"])
+    batched = modes[best]["mcell_steps_s"]
     name = "batch_small" if small else "batch_directions"
     return {"workload": f"{name}: {len(cs)} cases, {cells} cells total, grids "
                         f"{min(c.n_cells for c in cs)}..{max(c.n_cells for c in cs)} cells, nV=50 nP=30 nC=2",
             "plain_mcell_steps_s": plain, "batched_mcell_steps_s": batched, "batched_over_plain": batched / plain,
-            "steps": steps, "gpu_launches": launches,
-            "depths": sorted({(t["pres_k"], t["vel_k"]) for t in tuned}), "width": width}
+            "batched_mode": best, "modes": modes, "steps": steps, "gpu_launches": modes[best]["gpu_launches"],
+            "tuned": sorted({(t["pres_k"], t["pres_rows"], t["vel_k"], tuple(t["vel_block"])) for t in tuned}),
+            "width": width}
 
 
 def adjoint_section(local: int):
@@ -579,8 +594,8 @@ def run_windfvm(args):
     solver.close()
     batched = batched_small = None
     if world == 1 and not args.no_batched:
-        batched = batched_section(max(3, min(args.steps, 5)), local)
-        batched_small = batched_section(max(3, min(args.steps, 5)), local, small=True)
+        batched = batched_section(BATCH_STEPS, local)
+        batched_small = batched_section(BATCH_STEPS, local, small=True)
 
     adjoint = None
     if world == 1 and not args.no_adjoint:

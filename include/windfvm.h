@@ -424,6 +424,32 @@ int wf_batch_set_width(wf_batch* b, int width);
  * the replay state (one wf_batch_step after creating the batch or changing
  * its width); otherwise it does nothing. */
 int wf_batch_prepare_graphs(wf_batch* b);
+/* How a batched step runs (no counterpart in the reference).
+ * WF_BATCH_GRAPHS (default): every case's step graph as one branch of a
+ * parent graph, as above.
+ * WF_BATCH_PERSISTENT: every case's step is recorded as five captured
+ * segments (its once-per-step kernels) around its four Jacobi loops
+ * (momentum, SIMPLE pressure, two PISO pressure loops); each loop of all
+ * cases then runs as ONE persistent cooperative launch whose blocks walk a
+ * work queue of (case, tile) items sweep by sweep (pressure: K-sweep passes),
+ * with a grid-wide barrier between sweeps.  Results are identical to the
+ * graph mode.  All cases must have the same step structure (solver type,
+ * correctors, turbulence, iteration counts).  Speed only. */
+enum { WF_BATCH_GRAPHS = 0, WF_BATCH_PERSISTENT = 1 };
+int wf_batch_set_mode(wf_batch* b, int mode);
+int wf_batch_get_mode(const wf_batch* b, int* mode);
+/* Upper bound of one grid-barrier wait in the persistent mode (default 2000
+ * ms).  A wait that runs out sets an error word; every block of the launch
+ * then returns without further waits, later loops of the step return at
+ * once, and wf_batch_step returns WF_ERR_TIMEOUT (the cases' fields are then
+ * not valid).  Nothing in a correct run waits near this long. */
+int wf_batch_set_barrier_timeout(wf_batch* b, double ms);
+/* Self-test of that bounded barrier: one cooperative launch of `blocks`
+ * blocks (<= the device's SM count) that meet at a barrier expecting blocks +
+ * extra arrivals, with the given time limit.  *status = WF_OK when the
+ * barrier released (extra == 0), WF_ERR_TIMEOUT when its wait ran out (extra
+ * > 0: arrivals that never come).  No counterpart in the reference. */
+int wf_grid_barrier_selftest(int device, int blocks, int extra, double timeout_ms, int* status);
 
 /* Temporal-blocking depths of the Jacobi loops: pressure sweeps per pass
  * (1..4) and momentum sweeps per pass (1..2).  Results do not depend on
@@ -432,6 +458,14 @@ int wf_batch_prepare_graphs(wf_batch* b);
  * contain the handle afterwards. */
 int wf_set_blocking(wf_solver* h, int pres_k, int vel_k);
 int wf_get_blocking(const wf_solver* h, int* pres_k, int* vel_k);
+/* Tile shapes of the Jacobi kernels: rows of the pressure multi-sweep tile
+ * (32: 32 x 32 tiles, one block per SM; 16: 32 x 16 tiles, two blocks per
+ * SM, more tiles for small grids) and the block of the four-cell momentum
+ * sweep (vel_bx * vel_by * vel_bz == 256 threads; default 32 x 4 x 2).
+ * Results do not depend on them.  Drops the handle's captured step graphs.
+ * No counterpart in the reference (its kernels are [numthreads(8,8,8)]). */
+int wf_set_tiles(wf_solver* h, int pres_rows, int vel_bx, int vel_by, int vel_bz);
+int wf_get_tiles(const wf_solver* h, int* pres_rows, int* vel_bx, int* vel_by, int* vel_bz);
 
 /* ---- field export ---------------------------------------------------------
  * NcFlowFieldExporter (NcFlowFieldExporter.cs:197-393): velocity and

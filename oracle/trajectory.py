@@ -36,6 +36,19 @@ def step_stats(vel_soa: np.ndarray, pres: np.ndarray, fluid: np.ndarray) -> np.n
     return np.array([np.sqrt(mag2.max()), 0.5 * mag2.mean(), np.abs(p).max()])
 
 
+def save_state(s, path):
+    """Every field the reference's step reads (velocity textures, pressure,
+    eddy and face viscosities, boundary planes), FP32."""
+    from oracle.binding import REF_STATE_FIELDS
+    np.savez_compressed(path, **{str(f): np.asarray(s.get_field(f), dtype=np.float32) for f in REF_STATE_FIELDS})
+
+
+def load_state(s, path):
+    d = np.load(path)
+    for k in d.files:
+        s.set_field(int(k), np.asarray(d[k], dtype=np.float64))
+
+
 def make_solver(case, which: str, threads: int):
     """The workload's set-up state in the chosen host solver."""
     from oracle import OracleSolver
@@ -55,17 +68,16 @@ def make_solver(case, which: str, threads: int):
     return r
 
 
-def run(case, which: str, steps: int, threads: int = 0, blowup: float = 20.0, log=None, start=None):
+def run(case, which: str, steps: int, threads: int = 0, blowup: float = 20.0, log=None, start=None,
+        save_at=None):
     """Steps the workload up to `steps` times; returns (rows, status, u0)
     where rows[k] are the statistics after step k+1 and status is "bounded",
-    "blowup" or "nonfinite".  `start` = (vel, pres) replaces the set-up
-    velocity and pressure (a checkpoint)."""
+    "blowup" or "nonfinite".  `start` = the path of a saved state that
+    replaces the set-up state (load_state); `save_at` = (step, path) writes the
+    state after that step (every field a step reads) to an .npz file."""
     s = make_solver(case, which, threads or (os.cpu_count() or 1))
     if start is not None:
-        from unitywindsimulation_b200 import _lib
-        for f in (_lib.FIELD_VEL, _lib.FIELD_VEL_LAST_TIME, _lib.FIELD_VEL_LAST_ITER):
-            s.set_field(f, np.asarray(start[0], dtype=np.float64).reshape(3, -1))
-        s.set_field(_lib.FIELD_PRES, np.asarray(start[1], dtype=np.float64).reshape(-1))
+        load_state(s, start)
     fluid = np.asarray(case.flags).reshape(-1) == 0
     u0 = step_stats(s.GetVelField(), s.GetPresField(), fluid)[0]
     rows, status = [], "bounded"
@@ -74,6 +86,8 @@ def run(case, which: str, steps: int, threads: int = 0, blowup: float = 20.0, lo
         s.Step(1)
         st = step_stats(s.GetVelField(), s.GetPresField(), fluid)
         rows.append(st)
+        if save_at is not None and k + 1 == save_at[0]:
+            save_state(s, save_at[1])
         if log:
             print(f"{which} step {k + 1}: max|u| {st[0]:.4g} mean ke {st[1]:.4g} max|p| {st[2]:.4g} "
                   f"({time.perf_counter() - t0:.1f} s)", file=log, flush=True)
@@ -97,9 +111,14 @@ def main(argv=None):
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--blowup", type=float, default=20.0)
     ap.add_argument("--out", required=True)
+    ap.add_argument("--start", help="state file (save_state) to start from instead of the set-up state")
+    ap.add_argument("--save-step", type=int, help="write the state after this step to --save-path")
+    ap.add_argument("--save-path")
     a = ap.parse_args(argv)
     case = cases.WORKLOADS[a.workload]()
-    rows, status, u0 = run(case, a.solver, a.steps, a.threads, a.blowup, log=sys.stdout)
+    save_at = (a.save_step, a.save_path) if a.save_step else None
+    rows, status, u0 = run(case, a.solver, a.steps, a.threads, a.blowup, log=sys.stdout, start=a.start,
+                           save_at=save_at)
     np.savez_compressed(a.out, rows=rows, status=status, u0=u0, solver=a.solver, workload=a.workload,
                         stat_names=np.array(STAT_NAMES))
     print(f"{a.solver} {a.workload}: {len(rows)} steps, {status}")

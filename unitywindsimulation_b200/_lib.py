@@ -26,6 +26,10 @@ WF_NOT_FINISHED = 7
 WF_ERR_STATE = 8
 WF_ERR_IO = 9
 
+# batch modes (wf_batch_set_mode)
+BATCH_GRAPHS = 0
+BATCH_PERSISTENT = 1
+
 # ---- enums ----
 CELL_FLUID, CELL_SOLID = 0, 1
 BND_FIXED_VALUE, BND_ZERO_GRAD, BND_SYMMETRY = 0, 1, 2
@@ -189,6 +193,12 @@ _SIGNATURES = {
     "wf_batch_set_width": (c_int, [c_void_p, c_int]),
     "wf_batch_prepare_graphs": (c_int, [c_void_p]),
     "wf_prepare_graphs": (c_int, [c_void_p]),
+    "wf_batch_set_mode": (c_int, [c_void_p, c_int]),
+    "wf_batch_get_mode": (c_int, [c_void_p, POINTER(c_int)]),
+    "wf_batch_set_barrier_timeout": (c_int, [c_void_p, c_double]),
+    "wf_grid_barrier_selftest": (c_int, [c_int, c_int, c_int, c_double, POINTER(c_int)]),
+    "wf_set_tiles": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "wf_get_tiles": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "wf_set_blocking": (c_int, [c_void_p, c_int, c_int]),
     "wf_get_blocking": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
     "wf_export_open": (c_int, [c_void_p, c_char_p, c_int, c_int, c_int, POINTER(c_void_p)]),

@@ -483,6 +483,49 @@ int ensure_step_graph(wf_solver* h, const wf_solver::GraphEntry** out) {
     return WF_OK;
 }
 
+int LoopRecorder::cut(wf_solver* h) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->st, &g);
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+        return WF_ERR_CUDA;
+    }
+    segments.push_back(g);
+    e = cudaStreamBeginCapture(h->st, mode);
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e);
+        return WF_ERR_CUDA;
+    }
+    return WF_OK;
+}
+
+int capture_step_segments(wf_solver* h, LoopRecorder* rec, wf_solver::RoleKey* after, long long* kernels) {
+    const auto key = role_key(h);
+    const int64_t step0 = h->step;
+    const long long l0 = g_launches;
+    WF_CUDA(cudaStreamBeginCapture(h->st, rec->mode));
+    h->rec = rec;
+    const int s = enqueue_step(h);
+    h->rec = nullptr;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->st, &g);
+    if (g) rec->segments.push_back(g);
+    *kernels = g_launches - l0;
+    *after = role_key(h);
+    // the capture only recorded the work: restore the roles it rotated
+    set_roles(h, key);
+    h->iter_alias = true;
+    h->pc_zero = true;
+    h->step = step0;
+    g_launches = l0;
+    if (s != WF_OK) return s;
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+        return WF_ERR_CUDA;
+    }
+    return WF_OK;
+}
+
 void commit_graph_step(wf_solver* h, const wf_solver::GraphEntry& e) {
     set_roles(h, e.after);
     h->iter_alias = true;

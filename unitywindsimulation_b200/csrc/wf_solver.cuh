@@ -8,6 +8,10 @@
 
 #include "wf_common.cuh"
 
+namespace wf {
+struct LoopRecorder;
+}
+
 struct wf_solver {
     wf_config cfg{};
     wf::Params P{};
@@ -83,12 +87,15 @@ struct wf_solver {
     int fast = 1;             // use the fast Jacobi kernels (wf_sweeps.cu)
     int pres_k = 4;           // pressure sweeps per multi-sweep pass (1..4)
     int vel_k = 1;            // momentum sweeps per multi-sweep pass (1..2)
+    int pres_ty = 32;         // tile rows of the pressure multi-sweep kernel (32 or 16)
+    int vel_blk[3] = {32, 4, 2};  // block of the four-cell momentum sweep (256 threads)
     int num_sms = 148;        // multiprocessors of the device
     int pdl = 1;              // programmatic dependent launch in the non-uniform grid's sweep chains
                               // (WF_PDL=0: plain stream order)
     int vec4 = 1;             // 4-cell vector momentum sweep when nx % 4 == 0 and the
                               // planes are 16-byte aligned (WF_VEC4=0: one cell per thread)
     bool in_step = false;     // inside wf_step: skip iterates no later kernel reads
+    wf::LoopRecorder* rec = nullptr;  // set while a batch records the step in segments
     long long launches = 0;   // kernels launched by wf_step
     std::string err;
 
@@ -113,5 +120,9 @@ int ensure_step_graph(wf_solver* h, const wf_solver::GraphEntry** out);
 void commit_graph_step(wf_solver* h, const wf_solver::GraphEntry& e);
 // One step launched kernel by kernel on the handle's stream.
 int run_step_eager(wf_solver* h);
+// Captures one step from the handle's current state as segments around its
+// Jacobi loops (rec), without running it; *after receives the roles after
+// the step and *kernels the kernels in the segments.
+int capture_step_segments(wf_solver* h, LoopRecorder* rec, wf_solver::RoleKey* after, long long* kernels);
 void drop_graphs(wf_solver* h);
 }  // namespace wf

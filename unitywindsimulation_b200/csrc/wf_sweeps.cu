@@ -25,6 +25,12 @@
 
 namespace wf {
 
+#define WF_TRY_REC(x)             \
+    do {                          \
+        const int s_ = (x);       \
+        if (s_ != WF_OK) return s_; \
+    } while (0)
+
 namespace {
 
 __device__ __forceinline__ float ld(const float* p, size_t i) { return __ldg(p + i); }
@@ -113,13 +119,11 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
 // not once for 1/D and again for the rest (76 -> 63 us per sweep on the
 // urban block; indices are clamped in-domain, so the loads of non-fluid cells
 // are harmless and their results unused).
-template <bool kCopyAll = false>
-__global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Params P, const float* __restrict__ A,
-                                                    const float* __restrict__ iD, const float* __restrict__ bv,
-                                                    const float* __restrict__ ui, float* __restrict__ uo) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+template <bool kCopyAll>
+__device__ __forceinline__ void vel_sweep1_at(const Params& P, const float* __restrict__ A,
+                                              const float* __restrict__ iD, const float* __restrict__ bv,
+                                              const float* __restrict__ ui, float* __restrict__ uo, int x, int y,
+                                              int z) {
     if (x >= P.nx || y >= P.ny || z >= P.nz) return;
     const int i = cidx(P, x, y, z);
     const size_t N = P.N;
@@ -156,6 +160,14 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
     uo[2 * N + i] = d2 * r[2];
 }
 
+template <bool kCopyAll = false>
+__global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Params P, const float* __restrict__ A,
+                                                    const float* __restrict__ iD, const float* __restrict__ bv,
+                                                    const float* __restrict__ ui, float* __restrict__ uo) {
+    vel_sweep1_at<kCopyAll>(P, A, iD, bv, ui, uo, blockIdx.x * blockDim.x + threadIdx.x,
+                            blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z * blockDim.z + threadIdx.z);
+}
+
 // One momentum sweep, four consecutive x cells per thread (nx % 4 == 0 and
 // 16-byte aligned planes): every plane is read with 128-bit loads (A_E..A_D,
 // 1/D, b, the own and the y/z-neighbour iterates), the x neighbours beyond
@@ -167,15 +179,11 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
 __device__ __forceinline__ float4 ld4(const float* p, size_t i) { return __ldg(reinterpret_cast<const float4*>(p + i)); }
 __device__ __forceinline__ float f4(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
 
-template <bool kCopyAll = false>
-__global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Params P, const float* __restrict__ A,
-                                                    const float* __restrict__ iD, const float* __restrict__ bv,
-                                                    const float* __restrict__ ui, float* __restrict__ uo) {
-    chain_wait();
-    chain_release();
-    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z * blockDim.z + threadIdx.z;
+template <bool kCopyAll>
+__device__ __forceinline__ void vel_sweep4_at(const Params& P, const float* __restrict__ A,
+                                              const float* __restrict__ iD, const float* __restrict__ bv,
+                                              const float* __restrict__ ui, float* __restrict__ uo, int x0, int y,
+                                              int z) {
     if (x0 >= P.nx || y >= P.ny || z >= P.nz) return;
     const int i = cidx(P, x0, y, z);
     const size_t N = P.N;
@@ -238,6 +246,16 @@ __global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Para
                 if (fl[j]) o[j] = r[k][j];
         }
     }
+}
+
+template <bool kCopyAll = false>
+__global__ void __launch_bounds__(256) k_vel_sweep4(const __grid_constant__ Params P, const float* __restrict__ A,
+                                                    const float* __restrict__ iD, const float* __restrict__ bv,
+                                                    const float* __restrict__ ui, float* __restrict__ uo) {
+    chain_wait();
+    chain_release();
+    vel_sweep4_at<kCopyAll>(P, A, iD, bv, ui, uo, 4 * (blockIdx.x * blockDim.x + threadIdx.x),
+                            blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z * blockDim.z + threadIdx.z);
 }
 
 // The four-cell sweep applies: the switch on, x extent a multiple of 4 and
@@ -401,10 +419,12 @@ __global__ void __launch_bounds__(256) k_pres_sweep1(const __grid_constant__ Par
 // DRAM traffic per pass and cell: coefficients (c_E, c_N, c_U, 1/Dp, rhs:
 // 20 B) and the input iterate (4 B) once, the output iterate (4 B) once,
 // against 28 B per sweep for one sweep per launch.
-constexpr int MS_TX = 32, MS_TY = 32;
-constexpr size_t pres_msweep_smem(int K) { return sizeof(float) * MS_TX * MS_TY * (2 * K + 2 * 6); }
+constexpr int MS_TX = 32;
+// Tile height (rows) of the wavefront: 32 (1024 threads, one block per SM)
+// or 16 (512 threads, two blocks per SM; more tiles for small grids).
+constexpr size_t pres_msweep_smem(int K, int TY = 32) { return sizeof(float) * MS_TX * TY * (2 * K + 2 * 6); }
 
-template <int K>
+template <int K, int MS_TY>
 struct PresWave {
     static_assert(K >= 1 && K <= 4, "ring of 6 planes holds K <= 4");
     static constexpr int R = 6;  // ring period: unrolled z steps per loop trip
@@ -487,24 +507,26 @@ struct PresWave {
     }
 };
 
-template <int K>
-__global__ void __launch_bounds__(MS_TX* MS_TY, 1)
-    k_pres_msweep(const __grid_constant__ Params P, const float* __restrict__ c3, const float* __restrict__ ainv,
-                  const float* __restrict__ rhs, const float* __restrict__ pin, float* __restrict__ pout,
-                  float* __restrict__ pprev, int zchunk, float* __restrict__ stack) {
-    // dynamic shared memory: V[K][2][TY][TX] level planes, CE/CN[6][TY][TX]
+// One tile (bx, by) and z chunk bz of a K-sweep pass, run by a block of
+// MS_TX x MS_TY threads over the shared memory at msm (pres_msweep_smem).
+template <int K, int MS_TY>
+__device__ __forceinline__ void pres_wave_tile(const Params& P, const float* __restrict__ c3,
+                                               const float* __restrict__ ainv, const float* __restrict__ rhs,
+                                               const float* __restrict__ pin, float* __restrict__ pout,
+                                               float* __restrict__ pprev, int zchunk, float* __restrict__ stack,
+                                               int bx, int by, int bz, float* msm) {
+    // shared memory: V[K][2][TY][TX] level planes, CE/CN[6][TY][TX]
     // coefficient rings
-    extern __shared__ float msm[];
-    PresWave<K> w;
+    PresWave<K, MS_TY> w;
     w.V = reinterpret_cast<float(*)[2][MS_TY][MS_TX]>(msm);
     w.CE = reinterpret_cast<float(*)[MS_TY][MS_TX]>(msm + K * 2 * MS_TY * MS_TX);
-    w.CN = w.CE + PresWave<K>::R;
+    w.CN = w.CE + PresWave<K, MS_TY>::R;
     w.tx = threadIdx.x;
     w.ty = threadIdx.y;
     constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
-    const int x = blockIdx.x * OX - K + w.tx;
-    const int y = blockIdx.y * OY - K + w.ty;
-    w.z0 = blockIdx.z * zchunk;
+    const int x = bx * OX - K + w.tx;
+    const int y = by * OY - K + w.ty;
+    w.z0 = bz * zchunk;
     w.z1 = min(w.z0 + zchunk, P.nz);
     w.nz = P.nz;
     w.inxy = x >= 0 && x < P.nx && y >= 0 && y < P.ny;
@@ -528,7 +550,7 @@ __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
 #pragma unroll
     for (int s = 0; s < K; ++s) w.V[s][0][w.ty][w.tx] = w.V[s][1][w.ty][w.tx] = 0.f;
 #pragma unroll
-    for (int r = 0; r < PresWave<K>::R; ++r) {
+    for (int r = 0; r < PresWave<K, MS_TY>::R; ++r) {
         w.CE[r][w.ty][w.tx] = w.CN[r][w.ty][w.tx] = 0.f;
         w.qa[r] = w.qr[r] = w.qu[r] = 0.f;
     }
@@ -538,7 +560,7 @@ __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
     w.T = (w.z1 - w.z0) + 2 * K;
     w.fetch(w.zs, w.qa[0], w.qr[0]);
     __syncthreads();
-    for (int t = 0; t < w.T; t += PresWave<K>::R) {
+    for (int t = 0; t < w.T; t += PresWave<K, MS_TY>::R) {
         w.template step<0>(t);
         w.template step<1>(t + 1);
         w.template step<2>(t + 2);
@@ -546,6 +568,16 @@ __global__ void __launch_bounds__(MS_TX* MS_TY, 1)
         w.template step<4>(t + 4);
         w.template step<5>(t + 5);
     }
+}
+
+template <int K, int TY = 32>
+__global__ void __launch_bounds__(MS_TX* TY, TY == 32 ? 1 : 2)
+    k_pres_msweep(const __grid_constant__ Params P, const float* __restrict__ c3, const float* __restrict__ ainv,
+                  const float* __restrict__ rhs, const float* __restrict__ pin, float* __restrict__ pout,
+                  float* __restrict__ pprev, int zchunk, float* __restrict__ stack) {
+    extern __shared__ float msm[];
+    pres_wave_tile<K, TY>(P, c3, ainv, rhs, pin, pout, pprev, zchunk, stack, blockIdx.x, blockIdx.y, blockIdx.z,
+                          msm);
 }
 
 // K momentum sweeps per pass: the same wavefront for the three velocity
@@ -739,6 +771,13 @@ void vel_coef(wf_solver* h) {
     h->id_gen = h->d_gen;  // vcoef + 6N now holds 1/D of the current D
 }
 
+// Block of the four-cell momentum sweep: the handle's tile shape (256
+// threads, x threads cover four cells each).
+dim3 vblk(const wf_solver* h) { return dim3(h->vel_blk[0], h->vel_blk[1], h->vel_blk[2]); }
+dim3 grd4(const Params& P, dim3 b) {
+    return dim3((P.nx / 4 + b.x - 1) / b.x, (P.ny + b.y - 1) / b.y, (P.nz + b.z - 1) / b.z);
+}
+
 void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
     const Params& P = h->P;
     const size_t N = P.N;
@@ -746,7 +785,7 @@ void launch_vel_sweep_fast(wf_solver* h, const float* src, float* dst) {
     if (vec4_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst)) {
         // consecutive sweeps chain as programmatic dependent launches
         // (chain_wait / chain_release)
-        launch_chained(k_vel_sweep4<false>, grd4(P), blk(), h->st, h->pdl != 0, P,
+        launch_chained(k_vel_sweep4<false>, grd4(P, vblk(h)), vblk(h), h->st, h->pdl != 0, P,
                        (const float*)h->vcoef, (const float*)(h->vcoef + 6 * N), (const float*)h->bv, src, dst);
     } else {
         k_vel_sweep1<false><<<grd(P), blk(), 0, h->st>>>(P, h->vcoef, h->vcoef + 6 * N, h->bv, src, dst);
@@ -825,13 +864,17 @@ void launch_vmsweep(wf_solver* h, int k, const float* in, float* out, float* pre
 int sweeps_setup() {
     // dynamic shared memory above 48 KB needs the opt-in, per device
     cudaError_t e = cudaSuccess;
-    e = cudaFuncSetAttribute(k_pres_msweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(1));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_pres_msweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(2));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_pres_msweep<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(3));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_pres_msweep<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_msweep_smem(4));
+    auto opt_in = [&](auto kernel, size_t bytes) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
+    opt_in(k_pres_msweep<1, 32>, pres_msweep_smem(1, 32));
+    opt_in(k_pres_msweep<2, 32>, pres_msweep_smem(2, 32));
+    opt_in(k_pres_msweep<3, 32>, pres_msweep_smem(3, 32));
+    opt_in(k_pres_msweep<4, 32>, pres_msweep_smem(4, 32));
+    opt_in(k_pres_msweep<1, 16>, pres_msweep_smem(1, 16));
+    opt_in(k_pres_msweep<2, 16>, pres_msweep_smem(2, 16));
+    opt_in(k_pres_msweep<3, 16>, pres_msweep_smem(3, 16));
+    opt_in(k_pres_msweep<4, 16>, pres_msweep_smem(4, 16));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_vel_msweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_msweep_smem(1));
     if (e == cudaSuccess)
@@ -839,8 +882,37 @@ int sweeps_setup() {
     return e == cudaSuccess ? WF_OK : WF_ERR_CUDA;
 }
 
+namespace {
+
+// The one-sweep-per-launch rotation of vel_sweeps_fast, recorded instead of
+// launched: sweep 0 reads velFieldLastTime, the iterates ping-pong between
+// the velField and velFieldLastIter buffers.
+int record_vel_loop(wf_solver* h, int n) {
+    WF_TRY_REC(h->rec->cut(h));
+    const Params& P = h->P;
+    const size_t N = P.N;
+    VelLoopRec L;
+    L.A = h->vcoef;
+    L.iD = h->vcoef + 6 * N;
+    L.bv = h->bv;
+    L.vec4 = quad_ok(P, {L.A, L.iD, L.bv, h->vb[0], h->vb[1], h->vb[2], h->vb[3]});
+    for (int k = 0; k < n; ++k) {
+        L.src.push_back(h->iter_alias ? h->vb[h->iT] : h->vb[h->iI]);
+        L.dst.push_back(h->vb[h->iF]);
+        std::swap(h->iI, h->iF);
+        h->iter_alias = false;
+    }
+    std::swap(h->iI, h->iF);
+    h->rec->kinds.push_back(0);
+    h->rec->vel.push_back(std::move(L));
+    return WF_OK;
+}
+
+}  // namespace
+
 int vel_sweeps_fast(wf_solver* h, int n) {
     vel_coef(h);
+    if (h->rec) return record_vel_loop(h, n);
     const int kmax = std::min(std::max(h->vel_k, 1), 2);
     if (kmax > 1) {
         // Passes of up to kmax sweeps over buffers other than velFieldLastTime;
@@ -894,33 +966,81 @@ int vel_sweeps_fast(wf_solver* h, int n) {
 
 namespace {
 
-template <int K>
+// One K-sweep pass with tiles of TY rows: 32 (one block per SM) or 16
+// (two per SM); the z chunks fill one wave of resident blocks.
+template <int K, int TY>
 void launch_msweep_k(wf_solver* h, const float* rhs, const float* in, float* out, float* prev) {
     const Params& P = h->P;
     const size_t N = P.N;
-    constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
+    constexpr int OX = MS_TX - 2 * K, OY = TY - 2 * K;
     const int gx = (P.nx + OX - 1) / OX, gy = (P.ny + OY - 1) / OY;
     int zchunk = 0, nchunk = 0;
-    wave_chunks(h, gx * gy, K, zchunk, nchunk);
-    const size_t smem = pres_msweep_smem(K);
+    wave_chunks_n(h->num_sms * (TY == 32 ? 1 : 2), P.nz, gx * gy, K, zchunk, nchunk);
+    const size_t smem = pres_msweep_smem(K, TY);
     WF_COUNT_LAUNCH();
-    k_pres_msweep<K><<<dim3(gx, gy, nchunk), dim3(MS_TX, MS_TY), smem, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
-                                                                              in, out, prev, zchunk, nullptr);
+    k_pres_msweep<K, TY><<<dim3(gx, gy, nchunk), dim3(MS_TX, TY), smem, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
+                                                                               in, out, prev, zchunk, nullptr);
 }
 
 void launch_msweep(wf_solver* h, int k, const float* rhs, const float* in, float* out, float* prev) {
-    switch (k) {
-        case 1: launch_msweep_k<1>(h, rhs, in, out, prev); break;
-        case 2: launch_msweep_k<2>(h, rhs, in, out, prev); break;
-        case 3: launch_msweep_k<3>(h, rhs, in, out, prev); break;
-        default: launch_msweep_k<4>(h, rhs, in, out, prev); break;
+    if (h->pres_ty == 16) {
+        switch (k) {
+            case 1: launch_msweep_k<1, 16>(h, rhs, in, out, prev); break;
+            case 2: launch_msweep_k<2, 16>(h, rhs, in, out, prev); break;
+            case 3: launch_msweep_k<3, 16>(h, rhs, in, out, prev); break;
+            default: launch_msweep_k<4, 16>(h, rhs, in, out, prev); break;
+        }
+        return;
     }
+    switch (k) {
+        case 1: launch_msweep_k<1, 32>(h, rhs, in, out, prev); break;
+        case 2: launch_msweep_k<2, 32>(h, rhs, in, out, prev); break;
+        case 3: launch_msweep_k<3, 32>(h, rhs, in, out, prev); break;
+        default: launch_msweep_k<4, 32>(h, rhs, in, out, prev); break;
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// The multi-sweep rotation of pres_sweeps_fast inside a step, recorded
+// instead of launched.
+int record_pres_loop(wf_solver* h, int n, const float* rhs) {
+    WF_TRY_REC(h->rec->cut(h));
+    const size_t N = h->P.N;
+    PresLoopRec L;
+    L.c3 = h->pcoef;
+    L.ainv = h->pcoef + 3 * N;
+    L.rhs = rhs;
+    const int kmax = std::min(std::max(h->pres_k, 1), 4);
+    int in_idx = h->pc_zero ? -1 : h->iPCL;
+    int out_idx = -1, prev_idx = -1;
+    int remaining = n;
+    while (remaining > 0) {
+        const int k = std::min(kmax, remaining);
+        const bool last = remaining == k;
+        out_idx = in_idx == 0 ? 1 : 0;
+        if (last && k >= 2) prev_idx = in_idx < 0 ? (out_idx == 0 ? 1 : 0) : 3 - in_idx - out_idx;
+        else if (last) prev_idx = in_idx;
+        L.passes.push_back({k, in_idx < 0 ? nullptr : h->pcb[in_idx], h->pcb[out_idx]});
+        remaining -= k;
+        if (!last) in_idx = out_idx;
+    }
+    h->pc_zero = false;
+    h->iPC = out_idx;
+    if (prev_idx < 0) prev_idx = out_idx == 0 ? 1 : 0;
+    h->iPCL = prev_idx;
+    h->rec->kinds.push_back(1);
+    h->rec->pres.push_back(std::move(L));
+    return WF_OK;
 }
 
 }  // namespace
 
 int pres_sweeps_fast(wf_solver* h, int n, bool piso) {
     const float* rhs = pres_coef(h, piso);
+    if (h->rec) return record_pres_loop(h, n, rhs);
     const int kmax = std::min(std::max(h->pres_k, 1), 4);
     if (kmax == 1) {
         for (int k = 0; k < n; ++k) {
@@ -1035,12 +1155,12 @@ int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double
 template <int K>
 void launch_stack_pass(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
                        const float* rhs, const float* in, float* slots) {
-    constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
+    constexpr int OX = MS_TX - 2 * K, OY = 32 - 2 * K;
     const int gx = (P.nx + OX - 1) / OX, gy = (P.ny + OY - 1) / OY;
     int zchunk = 0, nchunk = 0;
     wave_chunks_n(sms, P.nz, gx * gy, K, zchunk, nchunk);
     WF_COUNT_LAUNCH();
-    k_pres_msweep<K><<<dim3(gx, gy, nchunk), dim3(MS_TX, MS_TY), pres_msweep_smem(K), st>>>(
+    k_pres_msweep<K, 32><<<dim3(gx, gy, nchunk), dim3(MS_TX, 32), pres_msweep_smem(K, 32), st>>>(
         P, c3, ainv, rhs, in, nullptr, nullptr, zchunk, slots);
 }
 void launch_pres_stack(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
@@ -1087,6 +1207,194 @@ void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, co
                          const float* aodu, float* ainv, float* rhs) {
     WF_COUNT_LAUNCH();
     k_piso_pre<<<grd(P), blk(), 0, st>>>(P, fl, Dv, iD, aodu, ainv, rhs);
+}
+
+
+// ------------------------------------------------------------------------
+// Persistent multi-case Jacobi loops.
+//
+// One cooperative launch runs a whole loop (every sweep or pass) of every
+// case of a batch: the blocks walk a work queue of (case, tile) items, then
+// meet at a grid-wide barrier before the next sweep reads what this one
+// wrote.  A cooperative launch guarantees that all blocks are resident, so
+// the barrier cannot wait on a block that never runs; its wait is still
+// bounded by a time limit, after which the block sets the sticky error word
+// and returns, and every later barrier returns at once.
+
+namespace {
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier for `expected` arriving blocks.  Returns false (on every
+// thread of the block) when the barrier's error word is or becomes set, or
+// when this block waited longer than timeout_ns.
+__device__ bool grid_barrier(GridBar* bar, unsigned expected, unsigned long long timeout_ns) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+        volatile GridBar* vb = bar;
+        int good = vb->err == 0;
+        if (good) {
+            const unsigned gen = vb->gen;
+            __threadfence();
+            const unsigned arrived = atomicAdd(&bar->count, 1u) + 1u;
+            if (arrived == expected) {
+                bar->count = 0;
+                __threadfence();
+                atomicAdd(&bar->gen, 1u);
+            } else {
+                const unsigned long long t0 = global_ns();
+                while (vb->gen == gen) {
+                    if (vb->err != 0) {
+                        good = 0;
+                        break;
+                    }
+                    if (global_ns() - t0 > timeout_ns) {
+                        atomicExch(&bar->err, 1);
+                        good = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The momentum loop: nsweeps sweeps of every case, items = the blocks of
+// each case's sweep grid (32 x 4 x 2 threads; the four-cell form covers 128
+// x cells per block row).
+__global__ void __launch_bounds__(256) k_fused_vel_loop(const FusedVelCase* __restrict__ cases, int ncases,
+                                                        int nitems, int nsweeps, GridBar* bar,
+                                                        unsigned long long timeout_ns) {
+    for (int s = 0; s < nsweeps; ++s) {
+        for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+            int c = 0;
+            while (c + 1 < ncases && cases[c + 1].item0 <= it) ++c;
+            const FusedVelCase& q = cases[c];
+            const int local = it - q.item0;
+            const int bx = local % q.gx, by = (local / q.gx) % q.gy, bz = local / (q.gx * q.gy);
+            const int x = bx * 32 + threadIdx.x, y = by * 4 + threadIdx.y, z = bz * 2 + threadIdx.z;
+            if (q.vec4)
+                vel_sweep4_at<false>(q.P, q.A, q.iD, q.bv, q.src[s], q.dst[s], 4 * x, y, z);
+            else
+                vel_sweep1_at<false>(q.P, q.A, q.iD, q.bv, q.src[s], q.dst[s], x, y, z);
+        }
+        if (s + 1 < nsweeps && !grid_barrier(bar, gridDim.x, timeout_ns)) return;
+    }
+}
+
+// The pressure loop: round r runs pass r of every case (a multi-sweep pass
+// of k sweeps per tile and z chunk); items of a round are the (case, tile,
+// chunk) triples, round_items[r] of them.
+__global__ void __launch_bounds__(1024, 1) k_fused_pres_loop(const FusedPresCase* __restrict__ cases, int ncases,
+                                                             const FusedPresPass* __restrict__ passes,
+                                                             const int* __restrict__ round_items, int nrounds,
+                                                             GridBar* bar, unsigned long long timeout_ns) {
+    extern __shared__ float fsm[];
+    for (int r = 0; r < nrounds; ++r) {
+        const int nitems = round_items[r];
+        for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+            // item0 is the prefix count of items (a case without a pass in
+            // this round owns an empty range): the last case starting at or
+            // before the item owns it
+            int c = 0;
+            while (c + 1 < ncases && passes[(c + 1) * nrounds + r].item0 <= it) ++c;
+            const FusedPresCase& q = cases[c];
+            const FusedPresPass& ps = passes[c * nrounds + r];
+            const int local = it - ps.item0;
+            const int bx = local % ps.gx, by = (local / ps.gx) % ps.gy, bz = local / (ps.gx * ps.gy);
+            switch (ps.k) {
+                case 1:
+                    pres_wave_tile<1, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                                          bz, fsm);
+                    break;
+                case 2:
+                    pres_wave_tile<2, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                                          bz, fsm);
+                    break;
+                case 3:
+                    pres_wave_tile<3, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                                          bz, fsm);
+                    break;
+                default:
+                    pres_wave_tile<4, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                                          bz, fsm);
+                    break;
+            }
+            __syncthreads();  // the next item reuses the shared memory
+        }
+        if (r + 1 < nrounds && !grid_barrier(bar, gridDim.x, timeout_ns)) return;
+    }
+}
+
+__global__ void k_barrier_selftest(int extra, GridBar* bar, unsigned long long timeout_ns) {
+    grid_barrier(bar, gridDim.x + (unsigned)extra, timeout_ns);
+}
+
+cudaError_t launch_coop(const void* fn, int blocks, dim3 block, size_t smem, cudaStream_t st, void** args) {
+    return cudaLaunchCooperativeKernel(fn, dim3(blocks), block, args, smem, st);
+}
+
+}  // namespace
+
+const void* fused_vel_kernel() { return (const void*)k_fused_vel_loop; }
+const void* fused_pres_kernel() { return (const void*)k_fused_pres_loop; }
+size_t fused_pres_smem() { return pres_msweep_smem(4, 32); }
+
+int fused_vel_blocks_per_sm(int* out) {
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_fused_vel_loop, 256, 0);
+    return e == cudaSuccess ? WF_OK : WF_ERR_CUDA;
+}
+
+int fused_pres_blocks_per_sm(int* out) {
+    cudaError_t e = cudaFuncSetAttribute(k_fused_pres_loop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pres_msweep_smem(4, 32));
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_fused_pres_loop, 1024, pres_msweep_smem(4, 32));
+    return e == cudaSuccess ? WF_OK : WF_ERR_CUDA;
+}
+
+void fused_pres_geometry(const Params& P, int k, int* gx, int* gy, int* nchunk, int* zchunk) {
+    const int OX = MS_TX - 2 * k, OY = 32 - 2 * k;
+    *gx = (P.nx + OX - 1) / OX;
+    *gy = (P.ny + OY - 1) / OY;
+    // chunks of about 48 planes: the halo ramp (2k planes) stays a small
+    // share, and the items of all cases balance over the resident blocks
+    const int n = std::max(1, (P.nz + 24) / 48);
+    *zchunk = std::max(2 * k + 2, (P.nz + n - 1) / n);
+    *nchunk = (P.nz + *zchunk - 1) / *zchunk;
+}
+
+cudaError_t launch_fused_vel_loop(cudaStream_t st, int blocks, const FusedVelCase* cases, int ncases, int nitems,
+                                  int nsweeps, GridBar* bar, unsigned long long timeout_ns) {
+    void* args[] = {(void*)&cases, (void*)&ncases, (void*)&nitems, (void*)&nsweeps, (void*)&bar, (void*)&timeout_ns};
+    WF_COUNT_LAUNCH();
+    return launch_coop((const void*)k_fused_vel_loop, blocks, dim3(32, 4, 2), 0, st, args);
+}
+
+cudaError_t launch_fused_pres_loop(cudaStream_t st, int blocks, const FusedPresCase* cases, int ncases,
+                                   const FusedPresPass* passes, const int* round_items, int nrounds, GridBar* bar,
+                                   unsigned long long timeout_ns) {
+    void* args[] = {(void*)&cases, (void*)&ncases, (void*)&passes, (void*)&round_items, (void*)&nrounds,
+                    (void*)&bar, (void*)&timeout_ns};
+    WF_COUNT_LAUNCH();
+    return launch_coop((const void*)k_fused_pres_loop, blocks, dim3(MS_TX, 32), pres_msweep_smem(4, 32), st, args);
+}
+
+cudaError_t launch_barrier_selftest(cudaStream_t st, int blocks, int extra, GridBar* bar,
+                                    unsigned long long timeout_ns) {
+    void* args[] = {(void*)&extra, (void*)&bar, (void*)&timeout_ns};
+    WF_COUNT_LAUNCH();
+    return launch_coop((const void*)k_barrier_selftest, blocks, dim3(32), 0, st, args);
 }
 
 }  // namespace wf

@@ -287,6 +287,17 @@ class FvmSolverCuda:
         self._check(self._lib.wf_get_blocking(self._h, byref(p), byref(v)))
         return p.value, v.value
 
+    def set_tiles(self, pres_rows: int, vel_block=(32, 4, 2)) -> None:
+        """Tile shapes of the Jacobi kernels (wf_set_tiles): pressure
+        multi-sweep tile rows (32 or 16) and the momentum sweep's block."""
+        bx, by, bz = (int(v) for v in vel_block)
+        self._check(self._lib.wf_set_tiles(self._h, int(pres_rows), bx, by, bz))
+
+    def get_tiles(self):
+        p, x, y, z = c_int(0), c_int(0), c_int(0), c_int(0)
+        self._check(self._lib.wf_get_tiles(self._h, byref(p), byref(x), byref(y), byref(z)))
+        return p.value, (x.value, y.value, z.value)
+
     # ---- per-kernel operations ----
     def op(self, name: str, *args) -> None:
         fn = getattr(self._lib, f"wf_op_{name}")
@@ -377,6 +388,19 @@ class BatchSolver:
 
     def set_width(self, width: int) -> None:
         self._check(self._lib.wf_batch_set_width(self._b, int(width)))
+
+    def set_mode(self, mode: int) -> None:
+        """_lib.BATCH_GRAPHS (child graphs) or _lib.BATCH_PERSISTENT (one
+        persistent launch per Jacobi loop over all cases)."""
+        self._check(self._lib.wf_batch_set_mode(self._b, int(mode)))
+
+    def get_mode(self) -> int:
+        m = c_int(0)
+        self._check(self._lib.wf_batch_get_mode(self._b, byref(m)))
+        return m.value
+
+    def set_barrier_timeout(self, ms: float) -> None:
+        self._check(self._lib.wf_batch_set_barrier_timeout(self._b, float(ms)))
 
     def prepare_graphs(self) -> None:
         """Captures the batch graphs of every buffer-role state ahead of time
