@@ -167,9 +167,13 @@ int wf_change_phys_field_pos(wf_solver* h);
  * call them after this, as the reference's constructor builds the mesh
  * before the fields.  The face-flux texture starts at zero and is bound
  * for the momentum kernels, which the reference leaves out (:1160,1196
- * are commented out).  SIMPLE without a turbulence model only
- * (WF_ERR_UNSUPPORTED otherwise); batches and the adjoint take uniform
- * grids only.  All three NULL: back to the uniform grid. */
+ * are commented out).  SIMPLE, with or without the Smagorinsky model
+ * (the wall function and LES kernels use the constant dx, as the
+ * reference's WallFunc and Les shaders do; the momentum kernels interpolate
+ * the eddy viscosity to the faces, useLES); PISO returns WF_ERR_UNSUPPORTED,
+ * as the reference has no PISO shader for this grid (:493-496 throws);
+ * batches and the adjoint take uniform grids only.  All three NULL: back to
+ * the uniform grid. */
 int wf_set_face_positions(wf_solver* h, const float* face_x, const float* face_y, const float* face_z);
 /* The face-flux texture of the non-uniform grid (velFaceFluxField,
  * FvmSolverGpu.cs:275, written by CSPresCorrectRhieChowPreCompute,

@@ -486,8 +486,12 @@ void pres_correct_nu(wfr_solver& s) {
     }
 }
 
-void step_once_nu(wfr_solver& s) {
+void step_once_nu(wfr_solver& s) {  // Step, :1050-1121, on the non-uniform grid
     set_uniforms(s);
+    if (s.cfg.turbulence == WF_TURB_SMAGORINSKY) {  // the Les and WallFunc shaders, constant dx
+        cal_wall_func(s);
+        cal_les_terms(s);
+    }
     vel_predict_nu(s);
     pres_correct_nu(s);
     bind_all(s);
@@ -815,9 +819,10 @@ int wfr_step(wfr_solver* s, int n_steps) {
  * it (FvmCollNonUniform.compute:204-335, 799-841) have their SetTexture calls
  * commented out (:1160, :1196).  Here the texture is bound for them too, so
  * that the momentum equation sees the face fluxes of the last pressure
- * pre-compute, the intended data flow.  Only SIMPLE without turbulence is
- * replayed: the reference pairs PISO and LES with the uniform-grid shaders'
- * constant dx. */
+ * pre-compute, the intended data flow.  SIMPLE is replayed with or without
+ * the Smagorinsky model (its Les and WallFunc shaders take the constant dx on
+ * every grid); PISO is refused, as InitPisoShader throws for this grid type
+ * (:493-496). */
 int wfr_set_face_positions(wfr_solver* s, const float* fx, const float* fy, const float* fz) {
     if (!s) return WF_ERR_INVALID_ARG;
     if (!fx && !fy && !fz) {
@@ -825,7 +830,7 @@ int wfr_set_face_positions(wfr_solver* s, const float* fx, const float* fy, cons
         return WF_OK;
     }
     if (!fx || !fy || !fz) return WF_ERR_INVALID_ARG;
-    if (s->cfg.solver_type != WF_SOLVER_SIMPLE || s->cfg.turbulence != WF_TURB_NONE) return WF_ERR_UNSUPPORTED;
+    if (s->cfg.solver_type != WF_SOLVER_SIMPLE) return WF_ERR_UNSUPPORTED;
     auto ok = [](const float* f, int n) {
         for (int i = 0; i < n; ++i)
             if (!(f[i + 1] > f[i])) return false;

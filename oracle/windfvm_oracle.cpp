@@ -466,7 +466,25 @@ template <class R> struct Oracle {
         return flux[t].c[F.axis];
     }
 
-    // CSVelPredictPreCompute, FvmCollNonUniform.compute:111-721 (useLES off).
+    // Face viscosities of the non-uniform momentum kernels (FvmCollNonUniform.
+    // compute:483-505, same block in CSVelPredict :846-868): nu without LES;
+    // with useLES nu + nu_t,P, and nu + wP nu_t,P + wQ nu_t,Q across a face to
+    // a fluid neighbour, with the linear interpolation weights of the mesh.
+    void nu_face_vis(int x, int y, int z, const Geo& g, R vis[6]) const {
+        for (int f = 0; f < 6; ++f) vis[f] = nu;
+        if (!les) return;
+        const size_t P = idx(x, y, z);
+        for (int f = 0; f < 6; ++f) vis[f] = nu + eddy[P];
+        for (int f = 0; f < 6; ++f) {
+            const Face& F = kFaces[f];
+            const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
+            if (!in_fluid(X, Y, Z)) continue;
+            const R wP = w_self(g, f), wQ = R(1.0f) - wP;
+            vis[f] = nu + wP * eddy[P] + wQ * eddy[idx(X, Y, Z)];
+        }
+    }
+
+    // CSVelPredictPreCompute, FvmCollNonUniform.compute:111-721.
     void nu_vel_precompute() {
         for_cells([&](int x, int y, int z) {
             if (!fluid(x, y, z)) return;
@@ -515,10 +533,12 @@ template <class R> struct Oracle {
             }
             for (int a = 0; a < 3; ++a) b[a] += -(R(1.0) / den) * g.ds[a] * (pf[2 * a] - pf[2 * a + 1]);
             // diffusion, :468-697
-            const R vis = nu;
+            R visf[6];
+            nu_face_vis(x, y, z, g, visf);
             for (int f = 0; f < 6; ++f) {
                 const Face& F = kFaces[f];
                 const int a = F.axis;
+                const R vis = visf[f];
                 const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
                 if (in_region(X, Y, Z)) {
                     const R t = fluid(X, Y, Z) ? vis * g.ds[a] / h_face(g, f)
@@ -538,11 +558,14 @@ template <class R> struct Oracle {
             // time and force, :699-710
             for (int k = 0; k < 3; ++k) b[k] += g.dv / dt * velT[P].c[k];
             for (int k = 0; k < 3; ++k) b[k] += g.dv * force[k];
+            // LES deferred-correction term, :712-717
+            if (les)
+                for (int k = 0; k < 3; ++k) b[k] += bv[P].c[k];
             Dv[P] = V3<R>{{D[0], D[1], D[2]}};
             bv[P] = V3<R>{{b[0], b[1], b[2]}};
         });
     }
-    // CSVelPredict, FvmCollNonUniform.compute:725-917 (useLES off).
+    // CSVelPredict, FvmCollNonUniform.compute:725-917.
     void nu_vel_sweep() {
         for_cells([&](int x, int y, int z) {
             if (!fluid(x, y, z)) return;
@@ -561,13 +584,14 @@ template <class R> struct Oracle {
                     adv[k] = F.sign > 0 ? adv[k] - t : adv[k] + t;
                 }
             }
-            const R vis = nu;
+            R visf[6];
+            nu_face_vis(x, y, z, g, visf);
             for (int f = 0; f < 6; ++f) {  // :844-907
                 const Face& F = kFaces[f];
                 const int X = x + F.ox, Y = y + F.oy, Z = z + F.oz;
                 if (!in_fluid(X, Y, Z)) continue;
                 const V3<R>& uQ = velI[idx(X, Y, Z)];
-                for (int k = 0; k < 3; ++k) dif[k] += vis * g.ds[F.axis] / h_face(g, f) * uQ.c[k];
+                for (int k = 0; k < 3; ++k) dif[k] += visf[f] * g.ds[F.axis] / h_face(g, f) * uQ.c[k];
             }
             V3<R> u;
             for (int k = 0; k < 3; ++k) u.c[k] = R(1.0) / Dv[P].c[k] * (adv[k] + dif[k] + bv[P].c[k]);
@@ -1308,7 +1332,8 @@ int wfo_set_face_positions(wfo_solver* h, const float* fx, const float* fy, cons
             return int(WF_OK);
         }
         if (!fx || !fy || !fz) return int(WF_ERR_INVALID_ARG);
-        if (o.cf.solver_type != WF_SOLVER_SIMPLE || o.cf.turbulence != WF_TURB_NONE) return int(WF_ERR_UNSUPPORTED);
+        // the reference has no PISO shader for this grid (FvmSolverGpu.cs:493-496)
+        if (o.cf.solver_type != WF_SOLVER_SIMPLE) return int(WF_ERR_UNSUPPORTED);
         const float* f[3] = {fx, fy, fz};
         const int n[3] = {o.nx, o.ny, o.nz};
         for (int a = 0; a < 3; ++a)

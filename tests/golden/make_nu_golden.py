@@ -36,6 +36,11 @@ CASES = {
     "log_urban_normalised": dict(log_inflow=True, seed=1),
     # nx = 15: the one-cell-per-thread sweeps (no four-cell quads in a row)
     "const_tunnel_odd_nx": dict(log_inflow=False, seed=2, nx=15, x_split=(7, 4)),
+    # Smagorinsky LES on the non-uniform grid: wall function and LES terms
+    # with the constant dx, face eddy viscosities interpolated with the mesh
+    # weights in the momentum kernels (useLES)
+    "log_urban_les": dict(log_inflow=True, seed=3, les=True),
+    "const_tunnel_les": dict(log_inflow=False, seed=4, les=True),
 }
 # Fields recorded after each step, and after the last one: (name, field id).
 STEP_FIELDS = (("vel", _lib.FIELD_VEL_LAST_TIME), ("pres", _lib.FIELD_PRES))

@@ -69,10 +69,10 @@ def test_fixture_covers_cases():
             assert np.isfinite(FIXTURE[f"{name}/{G.STEPS}/{key}"]).all()
 
 
-def _oracle_outputs(precision):
+def _oracle_outputs(precision, names=None):
     from oracle import OracleSolver
     out = {}
-    for name in G.CASES:
+    for name in (names or G.CASES):
         def rec(step, key, a, name=name):
             out[f"{name}/{step}/{key}"] = np.asarray(a)
         G.run_case(lambda cfg: OracleSolver(cfg, precision), name, rec)
@@ -88,10 +88,21 @@ def test_oracle_fp32_bit_identical_to_reference_kernels(built):
         assert np.array_equal(a.astype(np.float32), FIXTURE[k]), (k, float(np.abs(a - FIXTURE[k]).max()))
 
 
+# Recorded fields that are small differences of large terms: bp (the
+# divergence of the predicted velocity) and the velocity correction.  The
+# reference's own FP32 arithmetic departs from FP64 by up to about 2e-5
+# there (LES cases); other fields by less than 1e-5.
+CANCELLING = ("/bp", "/vel_correct")
+
+
+def _fp64_bound(k):
+    return 5e-5 if k.endswith(CANCELLING) else 1e-5
+
+
 def test_oracle_fp64_within_fp32_rounding_of_reference_kernels(built):
     out = _oracle_outputs(64)
     for k, a in out.items():
-        assert rel_l2(a, FIXTURE[k]) <= 1e-5, k
+        assert rel_l2(a, FIXTURE[k]) <= _fp64_bound(k), (k, rel_l2(a, FIXTURE[k]))
 
 
 def test_reference_kernels_reproduce_fixture():
@@ -110,7 +121,7 @@ def test_reference_kernels_reproduce_fixture():
             assert np.array_equal(a, FIXTURE[k]), k
 
 
-def test_reference_kernels_reject_piso_and_les():
+def test_reference_kernels_reject_piso():
     from oracle.binding import RefSolver, ref_available
     if not ref_available():
         pytest.skip("reference kernels not built (oracle/_ref)")
@@ -144,9 +155,15 @@ def test_cuda_matches_reference_kernels(name):
         got[f"{name}/{step}/{key}"] = a
     G.run_case(_cuda(), name, rec)
     assert set(got) == {k for k in FIXTURE.files if k.startswith(name + "/")}
+    # the cancelling fields: held to max(REL_TOL, 2 x the reference's own
+    # FP32 departure from FP64 on the same field)
+    ref64 = _oracle_outputs(64, names=[name]) if any(k.endswith(CANCELLING) for k in got) else {}
     for k, a in got.items():
         err = rel_l2(a, FIXTURE[k])
-        assert err <= REL_TOL, (k, err)
+        tol = REL_TOL
+        if k.endswith(CANCELLING):
+            tol = max(REL_TOL, 2.0 * rel_l2(FIXTURE[k], ref64[k]))
+        assert err <= tol, (k, err, tol)
 
 
 @pytest.mark.gpu
@@ -189,13 +206,17 @@ def test_unsupported_combinations_are_refused():
     from unitywindsimulation_b200.solver import FvmSolverCuda
     from unitywindsimulation_b200._lib import WindFvmError
     case = cases.small_nonuniform_case()
-    for over in (dict(solver_type=_lib.SOLVER_PISO), dict(turbulence=_lib.TURB_SMAGORINSKY)):
-        cfg = case.cfg.copy()
-        for k, v in over.items():
-            setattr(cfg, k, v)
-        s = FvmSolverCuda(cfg)
-        with pytest.raises(WindFvmError):
-            s.set_face_positions(*case.faces)
+    # PISO: the reference has no PISO shader for this grid (FvmSolverGpu.cs:493-496)
+    cfg = case.cfg.copy()
+    cfg.solver_type = _lib.SOLVER_PISO
+    s = FvmSolverCuda(cfg)
+    with pytest.raises(WindFvmError) as e:
+        s.set_face_positions(*case.faces)
+    assert e.value.status == _lib.WF_ERR_UNSUPPORTED
+    # LES runs on this grid, as in the reference
+    cfg = case.cfg.copy()
+    cfg.turbulence = _lib.TURB_SMAGORINSKY
+    FvmSolverCuda(cfg).set_face_positions(*case.faces)
     s = FvmSolverCuda(case.cfg)
     with pytest.raises(WindFvmError):
         s.set_face_positions(case.faces[0][::-1].copy(), case.faces[1], case.faces[2])  # decreasing

@@ -437,18 +437,23 @@ def wind_tunnel(nv: int = 800, np_: int = 2000, steps: int = 1) -> Case:
 
 
 def small_nonuniform_case(nx=16, ny=10, nz=12, log_inflow=False, seed=0, nv=8, np_=12,
-                          x_split=(8, 4)) -> Case:
+                          x_split=(8, 4), les=False) -> Case:
     """Small non-uniform case for parity tests: stretched x (x_split =
     (uniform, per side) cells: 4 + 8 + 4 by default), y (2 + 6 + 2) and z
     (3 + 6 + 3) axes of 0.5 m cores, one box.
     log_inflow=False: the wind-tunnel boundary set with a constant 3 m/s
     inflow; True: the urban set (no-slip ground, symmetry top and sides)
     with a log inflow and no fixed-pressure face (the pressure is
-    normalised)."""
+    normalised).  les=True adds the Smagorinsky model (Cs = 0.15), whose
+    wall function and LES kernels run with the constant dx, as in the
+    reference."""
     rng = np.random.default_rng(seed)
     dx = 0.5
     cfg = default_config(nx=nx, ny=ny, nz=nz, dx=dx, mu=0.01, den=1.0, solver_type=_lib.SOLVER_SIMPLE,
-                         turbulence=_lib.TURB_NONE, vel_iters=nv, pres_iters=np_)
+                         turbulence=_lib.TURB_SMAGORINSKY if les else _lib.TURB_NONE, vel_iters=nv,
+                         pres_iters=np_)
+    if les:
+        cfg.cs = 0.15
     if log_inflow:
         cfg.inflow_type = _lib.INFLOW_LOG
         cfg.wind_speed = 4.0
@@ -469,7 +474,7 @@ def small_nonuniform_case(nx=16, ny=10, nz=12, log_inflow=False, seed=0, nv=8, n
     h = int(rng.integers(2, 5))
     flags[z0_:z0_ + 3, 0:h, x0:x0 + 2] = 1
     faces = (stretched_faces(nx, dx, *x_split), stretched_faces(ny, dx, 6, 2), stretched_faces(nz, dx, 6, 3))
-    name = f"small_nu_{nx}x{ny}x{nz}_{'log' if log_inflow else 'const'}_s{seed}"
+    name = f"small_nu_{nx}x{ny}x{nz}_{'log' if log_inflow else 'const'}{'_les' if les else ''}_s{seed}"
     return Case(name, cfg, flags, None, 1, seed, [(x0, x0 + 2, z0_, z0_ + 3, h)], None, faces)
 
 

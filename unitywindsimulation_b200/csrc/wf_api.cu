@@ -758,8 +758,9 @@ int wf_set_face_positions(wf_solver* h, const float* fx, const float* fy, const 
         return WF_OK;
     }
     if (!fx || !fy || !fz) return set_err(h, WF_ERR_INVALID_ARG, "face positions: all three axes or none");
-    if (h->cfg.solver_type != WF_SOLVER_SIMPLE || h->cfg.turbulence != WF_TURB_NONE)
-        return set_err(h, WF_ERR_UNSUPPORTED, "the non-uniform grid runs SIMPLE without a turbulence model");
+    // the reference has no PISO shader for this grid (FvmSolverGpu.cs:493-496)
+    if (h->cfg.solver_type != WF_SOLVER_SIMPLE)
+        return set_err(h, WF_ERR_UNSUPPORTED, "the non-uniform grid runs SIMPLE (the reference has no PISO for it)");
     const int n[3] = {P.nx, P.ny, P.nz};
     const float* f[3] = {fx, fy, fz};
     for (int a = 0; a < 3; ++a)

@@ -12,8 +12,12 @@
 // three SoA planes here) feed the next momentum pre-compute and sweeps: the
 // reference leaves that texture unbound for those two kernels
 // (FvmSolverGpu.cs:1160,1196 are commented out); this library binds it, the
-// intended data flow.  Only SIMPLE without turbulence runs on this grid: the
-// reference pairs PISO and LES with the uniform shaders' constant dx.
+// intended data flow.  SIMPLE runs on this grid, with or without the
+// Smagorinsky model: as in the reference, the wall function and the LES
+// kernels run with the constant dx (Les and WallFunc have no non-uniform
+// form) and the momentum kernels interpolate the eddy viscosity to the faces
+// with the mesh weights (useLES).  The reference has no PISO shader for this
+// grid (FvmSolverGpu.cs:493-496 throws), so PISO is refused here too.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -112,7 +116,29 @@ __device__ __forceinline__ bool fluid_far(const Params& P, const uint8_t* fl, in
     return in_region(P, X, Y, Z) && fluid_cell(fl, cidx(P, X, Y, Z));
 }
 
-// CSVelPredictPreCompute, FvmCollNonUniform.compute:111-721 (useLES off).
+// Face viscosities of the non-uniform momentum kernels (FvmCollNonUniform.
+// compute:483-505 and 846-868): nu without LES (eddy == nullptr); with LES
+// nu + nu_t,P, and across a face to a fluid neighbour nu + wP nu_t,P + wQ
+// nu_t,Q with the mesh's interpolation weights (wQ = 1 - wP).
+__device__ __forceinline__ void nu_face_vis(const Params& P, const Geo& g, unsigned m, const float* eddy, int i,
+                                            float vis[6]) {
+    if (!eddy) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) vis[f] = P.nu;
+        return;
+    }
+    const float eP = ldn(eddy, i);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        vis[f] = P.nu + eP;
+        if (nb_fluid(m, f)) {
+            const float wP = w_self(g, f), wQ = 1.0f - wP;
+            vis[f] = P.nu + wP * eP + wQ * ldn(eddy, i + face_off(P, f));
+        }
+    }
+}
+
+// CSVelPredictPreCompute, FvmCollNonUniform.compute:111-721.
 // Besides D and b it stores the sweep's coefficients for the step: per
 // fluid-neighbour face A_f = (nu ds) / h -+ (ds w_neighbour) F_f (the
 // diffusion and advection factors CSVelPredict multiplies u_neighbour by,
@@ -125,8 +151,8 @@ __global__ void k_nu_vel_precompute(const __grid_constant__ Params P, const Bnd 
                                     const float* __restrict__ fy, const float* __restrict__ fz,
                                     const uint8_t* __restrict__ fl, const float* __restrict__ uT,
                                     const float* __restrict__ pr, const float* __restrict__ flux,
-                                    float* __restrict__ Dv, float* __restrict__ bv, float* __restrict__ A,
-                                    float* __restrict__ iD) {
+                                    const float* __restrict__ eddy, float* __restrict__ Dv,
+                                    float* __restrict__ bv, float* __restrict__ A, float* __restrict__ iD) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -189,11 +215,13 @@ __global__ void k_nu_vel_precompute(const __grid_constant__ Params P, const Bnd 
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) b[a] += -(1.0f / P.den) * g.ds[a] * (pf[2 * a] - pf[2 * a + 1]);
-    // diffusion with vis = nu, :468-697
-    const float vis = P.nu;
+    // diffusion with the face viscosities, :468-697
+    float visf[6];
+    nu_face_vis(P, g, m, eddy, i, visf);
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f);
+        const float vis = visf[f];
         if (face_in(P, x, y, z, f)) {
             const float t = nb_fluid(m, f) ? vis * g.ds[a] / h_face(g, f) : vis * g.ds[a] / (0.5f * g.a[a].d);
 #pragma unroll
@@ -216,6 +244,11 @@ __global__ void k_nu_vel_precompute(const __grid_constant__ Params P, const Bnd 
     for (int k = 0; k < 3; ++k) b[k] += g.dv / P.dt * ldn(uT, k * N + i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) b[k] += g.dv * P.force[k];
+    // LES deferred-correction term the LES kernel left in bField, :712-717
+    if (eddy) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) b[k] += ldn(bv, k * N + i);
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         Dv[k * N + i] = D[k];
@@ -229,7 +262,7 @@ __global__ void k_nu_vel_precompute(const __grid_constant__ Params P, const Bnd 
         if (nb_fluid(m, f)) {
             const int a = face_axis(f);
             const float adv = g.ds[a] * (1.0f - w_self(g, f)) * face_flux(F, x, y, z, f);
-            const float dif = vis * g.ds[a] / h_face(g, f);
+            const float dif = visf[f] * g.ds[a] / h_face(g, f);
             c = face_sign(f) > 0 ? dif - adv : dif + adv;
         }
         A[f * N + i] = c;
@@ -583,7 +616,8 @@ void launch_nu_vel_precompute(const wf_solver* h) {
     const float* fz = fy + P.ny + 1;
     WF_COUNT_LAUNCH();
     k_nu_vel_precompute<<<nu_grid(P), nu_block(), 0, h->st>>>(P, h->B, fx, fy, fz, h->fl, h->vb[h->iT], h->pr,
-                                                               h->flux, h->Dv, h->bv, h->vcoef, h->vcoef + 6 * (size_t)P.N);
+                                                               h->flux, P.les ? h->eddy : nullptr, h->Dv, h->bv,
+                                                               h->vcoef, h->vcoef + 6 * (size_t)P.N);
 }
 
 void launch_nu_pres_precompute(wf_solver* h, const float* u) {
