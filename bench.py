@@ -359,6 +359,43 @@ def adjoint_section(local: int):
             "dJ_dz0": r["dJ_dz0"], "dJ_dheights": [float(x) for x in r["dJ_dheights"]]}
 
 
+def adjoint_scale_section(local: int, directions: int = 1):
+    """Adjoint at scale on the batched-adjoint workload (256 x 96(up) x 256
+    cells, 64 soft buildings, nP = 40, 400-step window, checkpoints every
+    25 steps): the gradient of `directions` of its wind directions (a bounded
+    sample of the 8; each direction is an independent case), each against
+    its own plain forward over the same 400 steps (device time, CUDA
+    events)."""
+    from unitywindsimulation_b200 import FvmSolverCuda, cases
+    from unitywindsimulation_b200.adjoint import AdjointSolver, Objective
+
+    cs = cases.adjoint_batch()[:directions]
+    obj = Objective(**cases.ADJOINT_BATCH_OBJECTIVE)
+    rows = []
+    for c in cs:
+        g = FvmSolverCuda(c.cfg, device=local)
+        cases.apply_case(g, c)
+        g.Step(3)
+        g.prepare_graphs()
+        g.Step(c.steps)
+        fwd = g.last_step_ms()
+        g.close()
+        g = FvmSolverCuda(c.cfg, device=local)
+        cases.apply_case(g, c)
+        with AdjointSolver(g) as adj:
+            r = adj.gradient(obj, c.steps, cases.ADJOINT_BATCH_CHECKPOINT, soft=c.soft)
+        g.close()
+        rows.append({"case": c.name, "forward_ms": fwd, "gradient_ms": r["ms_total"],
+                     "adjoint_over_forward": r["ms_total"] / fwd, "J": r["J"]})
+    c = cs[0]
+    return {"workload": f"adjoint_batch: {directions} of 8 directions, {c.cfg.nx}x{c.cfg.ny}(up)x{c.cfg.nz} "
+                        f"cells each, 64 soft buildings, PISO laminar with viscosity {c.cfg.mu} m^2/s, "
+                        f"nV={c.cfg.vel_iters} nP={c.cfg.pres_iters} nC={c.cfg.piso_correctors}, {c.steps}-step window, "
+                        f"checkpoints every {cases.ADJOINT_BATCH_CHECKPOINT}",
+            "directions": rows,
+            "adjoint_over_forward": sum(r["gradient_ms"] for r in rows) / sum(r["forward_ms"] for r in rows)}
+
+
 def b_alg_nonuniform(nv: int, np_: int) -> int:
     """Compulsory bytes per cell-step of the non-uniform SIMPLE step
     (FvmCollNonUniform.compute; vector 12 B, scalar 4 B, flag 1 B): momentum
@@ -597,9 +634,10 @@ def run_windfvm(args):
         batched = batched_section(BATCH_STEPS, local)
         batched_small = batched_section(BATCH_STEPS, local, small=True)
 
-    adjoint = None
+    adjoint = adjoint_scale = None
     if world == 1 and not args.no_adjoint:
         adjoint = adjoint_section(local)
+        adjoint_scale = adjoint_scale_section(local)
 
     nonuniform = None
     if world == 1 and not args.no_nonuniform:
@@ -623,6 +661,7 @@ def run_windfvm(args):
             "batched": batched,
             "batched_small_cases": batched_small,
             "adjoint": adjoint,
+            "adjoint_scale": adjoint_scale,
             "nonuniform": nonuniform,
         }
         print(json.dumps(line), flush=True)
