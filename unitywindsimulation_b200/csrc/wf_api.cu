@@ -632,6 +632,10 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     P.dt = cfg->dt;
     P.nu = cfg->mu / cfg->den;            // :339
     P.den = cfg->den;
+    P.rdx = 1.0f / P.dx;
+    P.rdx2 = 1.0f / (2.f * P.dx);
+    P.rden = 1.0f / P.den;
+    P.dvden = P.dv / P.den;
     P.cs = cfg->cs;
     for (int i = 0; i < 3; ++i) P.force[i] = cfg->ext_force[i];
     for (int f = 0; f < 6; ++f) { P.vbc[f] = cfg->vel_bc[f]; P.pbc[f] = cfg->pres_bc[f]; }

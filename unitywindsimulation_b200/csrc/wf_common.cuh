@@ -27,6 +27,12 @@ struct Params {
     int N;          // nx*ny*nz (checked < 2^31 / 4 at create)
     int plane[6];   // point count of each boundary plane
     float dx, ds, dv, dt, nu, den, cs;
+    // Reciprocals computed once on the host: x * rdx in place of x / dx (and
+    // the like) saves an IEEE division per use.  Exact where dx and den are
+    // powers of two (every BASELINE workload: dx = 0.5, den = 1); within one
+    // rounding of the quotient otherwise.  dvden = dv / den is the quotient
+    // itself.
+    float rdx, rdx2, rden, dvden;
     float force[3];
     int vbc[6], pbc[6];
     int les;

@@ -161,7 +161,7 @@ __device__ __forceinline__ void cell_grad(const Params& P, const Bnd& B, const u
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) / P.dx;
+        for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) * P.rdx;
 }
 
 // cell_grad from the neighbour mask and loaded values: uP = own velocity,
@@ -192,7 +192,7 @@ __device__ __forceinline__ void cell_grad_v(const Params& P, const Bnd& B, unsig
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) / P.dx;
+        for (int j = 0; j < 3; ++j) g[i][j] = (fv[2 * j][i] - fv[2 * j + 1][i]) * P.rdx;
 }
 
 // ------------------------------------------------------------ wall function
@@ -331,7 +331,7 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
                     for (int j = 0; j < 3; ++j) fg[f][j] = 0.5f * (g[a][j] + gn[a][j]);
                 }
             } else {
-                const float v = uP[a] / (0.5f * P.dx);
+                const float v = uP[a] * (2.f * P.rdx);
                 fg[f][a] = face_sign(f) > 0 ? -v : v;
             }
         } else {
@@ -339,7 +339,7 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
             if (bt == WF_BND_FIXED_VALUE) {
                 const float b = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
                 const float u = uP[a];
-                fg[f][a] = face_sign(f) > 0 ? (b - u) / (0.5f * P.dx) : (u - b) / (0.5f * P.dx);
+                fg[f][a] = face_sign(f) > 0 ? (b - u) * (2.f * P.rdx) : (u - b) * (2.f * P.rdx);
             } else {
 #pragma unroll
                 for (int j = 0; j < 3; ++j)
@@ -430,18 +430,18 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
         }
     }
 #pragma unroll
-    for (int a = 0; a < 3; ++a) b[a] += -(1.0f / P.den) * P.ds * (pf[2 * a] - pf[2 * a + 1]);
+    for (int a = 0; a < 3; ++a) b[a] += -P.rden * P.ds * (pf[2 * a] - pf[2 * a + 1]);
     // diffusion, :1593-1836
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const float vis = vis_face_v(P, m, face, c, f, eP, eq[f]);
         if (face_in(P, c.x, c.y, c.z, f)) {
-            const float t = nb_fluid(m, f) ? vis * P.ds / P.dx : 2.f * vis * P.ds / P.dx;
+            const float t = nb_fluid(m, f) ? vis * P.ds * P.rdx : 2.f * vis * P.ds * P.rdx;
 #pragma unroll
             for (int k = 0; k < 3; ++k) D[k] += t;
         } else {
             const int bc = face_bc(f), bt = P.vbc[bc];
-            const float t = 2.f * vis * P.ds / P.dx;
+            const float t = 2.f * vis * P.ds * P.rdx;
             if (bt == WF_BND_FIXED_VALUE) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) b[k] += t * bnd_comp(P, B, bc, c.x, c.y, c.z, k);
@@ -507,7 +507,7 @@ __global__ void k_vel_sweep(const __grid_constant__ Params P, const uint8_t* __r
         if (!fluid_at(fl, q)) continue;
         const float vis = vis_face(P, fl, eddy, face, c, f);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) dif[k] += vis * P.ds / P.dx * ld(uI, k * N + q);
+        for (int k = 0; k < 3; ++k) dif[k] += vis * P.ds * P.rdx * ld(uI, k * N + q);
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) uo[k * N + c.i] = 1.0f / ld(Dv, k * N + c.i) * (adv[k] + dif[k] + ld(bv, k * N + c.i));
@@ -550,7 +550,6 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
         pq2[f] = ld(pr, q2);
     }
     if (!(m & 64u)) return;
-    const float dx2 = 2.f * P.dx;
     float DP = 0.f, bP = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -558,7 +557,7 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
         if (face_in(P, c.x, c.y, c.z, f)) {
             if (!nb_fluid(m, f)) continue;
             const float DInv = 0.5f * (dP[a] + dq[f]);
-            DP -= (P.dv / P.den) * DInv / P.dx;
+            DP -= P.dvden * DInv * P.rdx;
             const float fl_ = 0.5f * (uP[a] + uq[f]);
             bP = s > 0 ? bP + fl_ : bP - fl_;
             // Rhie-Chow over the face between low cell L and high cell H: the
@@ -568,14 +567,14 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
             const bool ll = s > 0 ? behindP : beyondQ;
             const float pL = s > 0 ? pP : pq[f], pH = s > 0 ? pq[f] : pP;
             const float pHH = s > 0 ? pq2[f] : pq[f ^ 1], pLL = s > 0 ? pq[f ^ 1] : pq2[f];
-            const float presGrad = (pH - pL) / P.dx;
+            const float presGrad = (pH - pL) * P.rdx;
             float ave = presGrad;
             if (hh || ll) {
-                const float gH = hh ? (pHH - pL) / dx2 : (pH - pL) / dx2;
-                const float gL = ll ? (pH - pLL) / dx2 : (pH - pL) / dx2;
+                const float gH = hh ? (pHH - pL) * P.rdx2 : (pH - pL) * P.rdx2;
+                const float gL = ll ? (pH - pLL) * P.rdx2 : (pH - pL) * P.rdx2;
                 ave = 0.5f * (gH + gL);
             }
-            const float vct = -(P.dv * DInv) / P.den * (presGrad - ave);
+            const float vct = -(P.dv * DInv) * P.rden * (presGrad - ave);
             bP = s > 0 ? bP + vct : bP - vct;
         } else {
             const int bc = face_bc(f), vb = P.vbc[bc];
@@ -586,7 +585,7 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
                 const float t = uP[a];
                 bP = s > 0 ? bP + t : bP - t;
             }
-            if (P.pbc[bc] == WF_BND_FIXED_VALUE) DP -= 2.f * (P.dv / P.den) * dP[a] / P.dx;
+            if (P.pbc[bc] == WF_BND_FIXED_VALUE) DP -= 2.f * P.dvden * dP[a] * P.rdx;
         }
     }
     Dp[c.i] = DP;
@@ -612,7 +611,7 @@ __global__ void k_pres_sweep(const __grid_constant__ Params P, const uint8_t* __
             const int q = cidx(P, X, Y, Z);
             if (!fluid_at(fl, q)) continue;
             const float DInv = 0.5f * (1.f / ld(Dv, a * N + c.i) + 1.f / ld(Dv, a * N + q));
-            t -= (P.dv / P.den) * DInv / P.dx * ld(pin, q);
+            t -= P.dvden * DInv * P.rdx * ld(pin, q);
         }
     }
     pout[c.i] = (1.f / ld(Dp, c.i)) * (t + ld(bp, c.i));
@@ -690,7 +689,7 @@ __global__ void k_apply_vel(const __grid_constant__ Params P, const uint8_t* __r
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float corr = -(P.dv / P.den) * di[a] * (pf[2 * a] - pf[2 * a + 1]) / P.dx;
+        const float corr = -P.dvden * di[a] * (pf[2 * a] - pf[2 * a + 1]) * P.rdx;
         uc[a * N + c.i] = corr;
         u[a * N + c.i] = uo[a] + corr;
     }
@@ -733,7 +732,7 @@ __global__ void k_piso_aodu(const __grid_constant__ Params P, const uint8_t* __r
             const float uq = ucq[f][k];
             const float t = P.ds * 0.25f * uq * sum;
             adv[k] = face_sign(f) > 0 ? adv[k] + t : adv[k] - t;
-            dif[k] -= vis * P.ds / P.dx * uq;
+            dif[k] -= vis * P.ds * P.rdx * uq;
         }
     }
 #pragma unroll
@@ -757,7 +756,7 @@ __global__ void k_piso_pres_sweep(const __grid_constant__ Params P, const uint8_
         if (!in_region(P, X, Y, Z)) {
             if (consistent && P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE) {
                 const float DInv = 1.f / ld(Dv, a * N + c.i);
-                coeff -= 2.f * (P.dv / P.den) * DInv / P.dx;
+                coeff -= 2.f * P.dvden * DInv * P.rdx;
             }
             continue;
         }
@@ -767,11 +766,11 @@ __global__ void k_piso_pres_sweep(const __grid_constant__ Params P, const uint8_
         const float Aod = 0.5f * (ld(aodu, a * N + c.i) + ld(aodu, a * N + q));
         const float pq = pin ? ld(pin, q) : 0.f;
         if (a == 0) {
-            coeff -= (P.dv / P.den) * (AdInv / P.dx);
-            pt -= (P.dv / P.den) * (AdInv / P.dx) * pq;
+            coeff -= P.dvden * (AdInv * P.rdx);
+            pt -= P.dvden * (AdInv * P.rdx) * pq;
         } else {
-            coeff -= (P.dv / P.den) * AdInv / P.dx;
-            pt -= (P.dv / P.den) * AdInv / P.dx * pq;
+            coeff -= P.dvden * AdInv * P.rdx;
+            pt -= P.dvden * AdInv * P.rdx * pq;
         }
         vt = face_sign(f) > 0 ? vt - AdInv * Aod : vt + AdInv * Aod;
     }
@@ -806,8 +805,8 @@ __global__ void k_piso_vel(const __grid_constant__ Params P, const uint8_t* __re
     for (int f = 0; f < 6; ++f) pf[f] = nb_fluid(m, f) ? 0.5f * (pP + pn[f]) : pP;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float grad = (pf[2 * a] - pf[2 * a + 1]) / P.dx;
-        const float corr = -di[a] * (ao[a] + P.dv / P.den * grad);
+        const float grad = (pf[2 * a] - pf[2 * a + 1]) * P.rdx;
+        const float corr = -di[a] * (ao[a] + P.dvden * grad);
         uc[a * N + c.i] = corr;
         u[a * N + c.i] = uo[a] + corr;
     }

@@ -104,7 +104,7 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
         if (nb_fluid(m, f)) {
             const float conv = P.ds * 0.25f * (uTP[face_axis(f)] + uTq[f]);
             const float vis = P.les ? P.nu + 0.5f * (eP + eq[f]) : P.nu;
-            const float dif = vis * P.ds / P.dx;
+            const float dif = vis * P.ds * P.rdx;
             c = face_sign(f) > 0 ? dif - conv : dif + conv;
         }
         A[f * N + i] = c;
@@ -283,7 +283,7 @@ __global__ void k_pres_coef(const __grid_constant__ Params P, const uint8_t* __r
         if (me && nb_fluid(m, f)) {
             const int q = i + face_off(P, f);
             const float DInv = 0.5f * (inv_d(iDc, Dv, N, a, i) + inv_d(iDc, Dv, N, a, q));
-            c = (P.dv / P.den) * DInv / P.dx;
+            c = P.dvden * DInv * P.rdx;
         }
         c3[a * N + i] = c;
     }
@@ -353,14 +353,14 @@ __global__ void k_piso_pre(const __grid_constant__ Params P, const uint8_t* __re
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f);
         if (!face_in(P, x, y, z, f)) {
-            if (consistent && P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE) coeff -= 2.f * (P.dv / P.den) * dP[a] / P.dx;
+            if (consistent && P.pbc[face_bc(f)] == WF_BND_FIXED_VALUE) coeff -= 2.f * P.dvden * dP[a] * P.rdx;
             continue;
         }
         if (!nb_fluid(m, f)) continue;
         const float AdInv = 0.5f * (dP[a] + dq[f]);
         const float Aod = 0.5f * (aP[a] + aq[f]);
-        if (a == 0) coeff -= (P.dv / P.den) * (AdInv / P.dx);
-        else coeff -= (P.dv / P.den) * AdInv / P.dx;
+        if (a == 0) coeff -= P.dvden * (AdInv * P.rdx);
+        else coeff -= P.dvden * AdInv * P.rdx;
         vt = face_sign(f) > 0 ? vt - AdInv * Aod : vt + AdInv * Aod;
     }
     ainv[i] = 1.f / coeff;
