@@ -181,9 +181,16 @@ int do_vel_precompute(wf_solver* h) {
         WF_CHECK_LAUNCH();
         return WF_OK;
     }
+    // inside a step the fast momentum sweeps' coefficients (A, 1/D) come out
+    // of the same pass; nothing between here and the sweeps changes their
+    // inputs (velFieldLastTime, the eddy viscosity, D)
+    const bool coef = h->in_step && h->fast;
+    float* A = coef ? h->vcoef : nullptr;
+    float* iD = coef ? h->vcoef + 6 * (size_t)h->P.N : nullptr;
     wf::launch_vel_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iT], h->pr, h->eddy, h->face,
-                              h->P.les ? h->bv : nullptr, h->drag, h->Dv, h->bv);
+                              h->P.les ? h->bv : nullptr, h->drag, h->Dv, h->bv, A, iD);
     WF_CHECK_LAUNCH();
+    h->vcoef_step = coef;
     return WF_OK;
 }
 
@@ -235,8 +242,12 @@ int do_pres_precompute(wf_solver* h) {
         WF_CHECK_LAUNCH();
         return WF_OK;
     }
-    wf::launch_pres_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iF], h->pr, h->Dv, cur_inv_d(h), h->Dp, h->bp);
+    // the fast path's pressure face coefficients come out of the same pass
+    // (they depend on D only, like the cache generation they are keyed by)
+    float* c3 = h->fast ? h->pcoef : nullptr;
+    wf::launch_pres_precompute(h->P, h->B, h->st, h->fl, h->vb[h->iF], h->pr, h->Dv, cur_inv_d(h), h->Dp, h->bp, c3);
     WF_CHECK_LAUNCH();
+    if (c3) h->c3_gen = h->d_gen;
     return WF_OK;
 }
 
@@ -291,6 +302,13 @@ int do_apply_vel(wf_solver* h) {
     WF_CHECK_LAUNCH();
     return WF_OK;
 }
+// ApplyVelCorrection together with ApplyPresCorrection (p += p'), one pass;
+// the velocity correction does not read p, so the two commute.
+int do_apply_vel_pres(wf_solver* h) {
+    wf::launch_apply_vel(h->P, h->st, h->fl, pc_cur(h), h->Dv, cur_inv_d(h), h->uc, h->vb[h->iF], h->pr);
+    WF_CHECK_LAUNCH();
+    return WF_OK;
+}
 
 // PisoCorrection (FvmSolverGpu.cs:1482-1533) with n pressure sweeps; p'
 // starts from the zero state.
@@ -311,14 +329,16 @@ int do_piso(wf_solver* h, int n, bool allow_fast) {
         }
         std::swap(h->iPCL, h->iPC);
     }
-    wf::launch_apply_pres(P, h->st, h->fl, pc_cur(h), h->pr);
+    // PisoApplyPresCorrection (p += p'') in the same pass as the velocity
+    // correction, which does not read p
     const float* pc = pc_cur(h);
     if (pc) {
-        wf::launch_piso_vel(P, h->st, h->fl, pc, h->Dv, cur_inv_d(h), h->aodu, h->uc, h->vb[h->iF]);
+        wf::launch_piso_vel(P, h->st, h->fl, pc, h->Dv, cur_inv_d(h), h->aodu, h->uc, h->vb[h->iF], h->pr);
     } else {
         // p'' == 0: PisoVelCorrection with a zero field still applies -D^-1 AodU
         WF_TRY(materialize_pc(h));
-        wf::launch_piso_vel(P, h->st, h->fl, h->pcb[h->iPC], h->Dv, cur_inv_d(h), h->aodu, h->uc, h->vb[h->iF]);
+        wf::launch_piso_vel(P, h->st, h->fl, h->pcb[h->iPC], h->Dv, cur_inv_d(h), h->aodu, h->uc, h->vb[h->iF],
+                            h->pr);
     }
     WF_CHECK_LAUNCH();
     h->pc_zero = true;  // SetPresCorrectFieldtoZero (:1532)
@@ -339,6 +359,7 @@ int enqueue_step(wf_solver* h) {
     h->in_step = true;
     const int s = enqueue_step_body(h);
     h->in_step = false;
+    h->vcoef_step = false;
     return s;
 }
 
@@ -349,9 +370,16 @@ int enqueue_step_body(wf_solver* h) {
     WF_TRY(do_vel_sweeps(h, c.vel_iters, true));
     WF_TRY(do_pres_precompute(h));
     WF_TRY(do_pres_sweeps(h, c.pres_iters, true));
-    WF_TRY(do_apply_pres(h));
-    if (!any_fixed_pres(c)) WF_TRY(do_normalize(h));
-    WF_TRY(do_apply_vel(h));
+    if (h->nonuniform) {
+        WF_TRY(do_apply_pres(h));
+        if (!any_fixed_pres(c)) WF_TRY(do_normalize(h));
+        WF_TRY(do_apply_vel(h));
+    } else {
+        // p += p' in the velocity-correction pass; the normalisation reads
+        // the corrected p and the velocity correction does not read p
+        WF_TRY(do_apply_vel_pres(h));
+        if (!any_fixed_pres(c)) WF_TRY(do_normalize(h));
+    }
     h->pc_zero = true;  // SetPresCorrectFieldtoZero (:1088)
     if (c.solver_type == WF_SOLVER_PISO)
         for (int n = 0; n < c.piso_correctors; ++n) WF_TRY(do_piso(h, c.pres_iters, true));
@@ -929,9 +957,14 @@ int wf_step_phases(wf_solver* h, float* phase_ms) {
         if ((st = mark(WF_PHASE_PRES_SWEEPS)) != WF_OK) break;
         if ((st = do_pres_sweeps(h, c.pres_iters, true)) != WF_OK) break;
         if ((st = mark(WF_PHASE_CORRECT)) != WF_OK) break;
-        if ((st = do_apply_pres(h)) != WF_OK) break;
-        if (!any_fixed_pres(c) && (st = do_normalize(h)) != WF_OK) break;
-        if ((st = do_apply_vel(h)) != WF_OK) break;
+        if (h->nonuniform) {
+            if ((st = do_apply_pres(h)) != WF_OK) break;
+            if (!any_fixed_pres(c) && (st = do_normalize(h)) != WF_OK) break;
+            if ((st = do_apply_vel(h)) != WF_OK) break;
+        } else {
+            if ((st = do_apply_vel_pres(h)) != WF_OK) break;
+            if (!any_fixed_pres(c) && (st = do_normalize(h)) != WF_OK) break;
+        }
         h->pc_zero = true;  // SetPresCorrectFieldtoZero (:1088)
         if ((st = mark(WF_PHASE_PISO)) != WF_OK) break;
         if (c.solver_type == WF_SOLVER_PISO)
@@ -942,6 +975,7 @@ int wf_step_phases(wf_solver* h, float* phase_ms) {
         st = mark(WF_PHASE_COUNT);
     } while (false);
     h->in_step = false;
+    h->vcoef_step = false;
     if (phase >= 0 && phase < WF_PHASE_COUNT) nvtxRangePop();
     h->launches += wf::g_launches - l0;
     if (st != WF_OK) return st;

@@ -361,11 +361,15 @@ __global__ void k_les_term(const __grid_constant__ Params P, const Bnd B, const 
 // ------------------------------------------------------- momentum predictor
 // CSVelPredictPreCompute, FvmColl.compute:1292-1859.  bles (may be null when
 // LES is off) holds the LES term; D and b are written.  bles may alias b.
+// A, iD (nullable): also stores the fast momentum sweeps' coefficients of
+// this D, the values k_vel_coef computes: A_f = nu_f ds/dx -/+ ds (u_P +
+// u_f)/4 on fluid-fluid faces (6 planes) and 1/D (3 planes), 0 on non-fluid
+// cells; the expressions are k_vel_coef's.
 __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
                                  const float* __restrict__ uT, const float* __restrict__ pr,
                                  const float* __restrict__ eddy, const float* __restrict__ face,
                                  const float* bles, const float* __restrict__ drag, float* __restrict__ Dv,
-                                 float* bv) {
+                                 float* bv, float* __restrict__ A, float* __restrict__ iD) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     (void)fl;
@@ -389,7 +393,15 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
 #pragma unroll
     for (int k = 0; k < 3; ++k) bl[k] = add_les ? bles[k * N + c.i] : 0.f;
     const float dr = drag ? ld(drag, c.i) : 0.f;
-    if (!(m & 64u)) return;
+    if (!(m & 64u)) {
+        if (A) {
+#pragma unroll
+            for (int f = 0; f < 6; ++f) A[f * N + c.i] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) iD[k * N + c.i] = 0.f;
+        }
+        return;
+    }
     const float dvdt = P.dv / P.dt;
     float D[3] = {dvdt, dvdt, dvdt};
     float b[3] = {0.f, 0.f, 0.f};
@@ -472,6 +484,21 @@ __global__ void k_vel_precompute(const __grid_constant__ Params P, const Bnd B, 
         Dv[k * N + c.i] = D[k];
         bv[k * N + c.i] = b[k];
     }
+    if (A) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            float cf = 0.f;
+            if (nb_fluid(m, f)) {
+                const float conv = P.ds * 0.25f * (uP[face_axis(f)] + uq[f]);
+                const float vis = P.les ? P.nu + 0.5f * (eP + eq[f]) : P.nu;
+                const float dif = vis * P.ds * P.rdx;
+                cf = face_sign(f) > 0 ? dif - conv : dif + conv;
+            }
+            A[f * N + c.i] = cf;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) iD[k * N + c.i] = 1.0f / D[k];
+    }
 }
 
 // CSVelPredict, FvmColl.compute:1863-2069.  uI == nullptr is not allowed
@@ -516,10 +543,13 @@ __global__ void k_vel_sweep(const __grid_constant__ Params P, const uint8_t* __r
 // ----------------------------------------------------- pressure correction
 // CSPresCorrectRhieChowPreCompute, FvmColl.compute:2481-2787.  iD
 // (nullable): cached 1/D of the same D.
+// c3 (nullable): also stores the pressure sweeps' face coefficients c_E,
+// c_N, c_U (three planes; (dv/den) DInv / dx on fluid-fluid faces, else 0),
+// the values k_pres_coef computes from the same D, as the same products.
 __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
                                   const float* __restrict__ u, const float* __restrict__ pr,
                                   const float* __restrict__ Dv, const float* __restrict__ iD,
-                                  float* __restrict__ Dp, float* __restrict__ bp) {
+                                  float* __restrict__ Dp, float* __restrict__ bp, float* __restrict__ c3) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     (void)fl;
@@ -549,15 +579,25 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
         pq[f] = ld(pr, q);
         pq2[f] = ld(pr, q2);
     }
-    if (!(m & 64u)) return;
+    if (!(m & 64u)) {
+        if (c3) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) c3[a * N + c.i] = 0.f;
+        }
+        return;
+    }
     float DP = 0.f, bP = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         const int a = face_axis(f), s = face_sign(f);
         if (face_in(P, c.x, c.y, c.z, f)) {
-            if (!nb_fluid(m, f)) continue;
+            if (!nb_fluid(m, f)) {
+                if (c3 && s > 0) c3[a * N + c.i] = 0.f;
+                continue;
+            }
             const float DInv = 0.5f * (dP[a] + dq[f]);
             DP -= P.dvden * DInv * P.rdx;
+            if (c3 && s > 0) c3[a * N + c.i] = __fmul_rn(__fmul_rn(P.dvden, DInv), P.rdx);
             const float fl_ = 0.5f * (uP[a] + uq[f]);
             bP = s > 0 ? bP + fl_ : bP - fl_;
             // Rhie-Chow over the face between low cell L and high cell H: the
@@ -577,6 +617,7 @@ __global__ void k_pres_precompute(const __grid_constant__ Params P, const Bnd B,
             const float vct = -(P.dv * DInv) * P.rden * (presGrad - ave);
             bP = s > 0 ? bP + vct : bP - vct;
         } else {
+            if (c3 && s > 0) c3[a * N + c.i] = 0.f;
             const int bc = face_bc(f), vb = P.vbc[bc];
             if (vb == WF_BND_FIXED_VALUE) {
                 const float t = bnd_comp(P, B, bc, c.x, c.y, c.z, a);
@@ -659,9 +700,13 @@ __global__ void k_norm_apply(const __grid_constant__ Params P, const uint8_t* __
 
 // CSApplyVelCorrectionDivergenceTheorem, FvmColl.compute:2951-3121.
 // pc == nullptr reads as zero; iD (nullable): cached 1/D of the same D.
+// pr (nullable): also applies the pressure correction p += p' on the fluid
+// cells (CSApplyPresCorrection, :2851-2862, the same addition), so the step
+// needs no separate pass over p.
 __global__ void k_apply_vel(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                             const float* __restrict__ pc, const float* __restrict__ Dv,
-                            const float* __restrict__ iD, float* __restrict__ uc, float* __restrict__ u) {
+                            const float* __restrict__ iD, float* __restrict__ uc, float* __restrict__ u,
+                            float* __restrict__ pr) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     (void)fl;
@@ -678,6 +723,7 @@ __global__ void k_apply_vel(const __grid_constant__ Params P, const uint8_t* __r
         uo[a] = ld(u, a * N + c.i);
     }
     if (!(m & 64u)) return;
+    if (pr) pr[c.i] += pP;
     float pf[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -779,10 +825,12 @@ __global__ void k_piso_pres_sweep(const __grid_constant__ Params P, const uint8_
 
 // CSPisoVelCorrection, PisoColl.compute:270-337.  iD (nullable): cached
 // 1/D of the same D.
+// pr (nullable): also applies p += p'' on the fluid cells
+// (CSPisoApplyPresCorrection, PisoColl.compute:259-267, the same addition).
 __global__ void k_piso_vel(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                            const float* __restrict__ pc, const float* __restrict__ Dv,
                            const float* __restrict__ iD, const float* __restrict__ aodu, float* __restrict__ uc,
-                           float* __restrict__ u) {
+                           float* __restrict__ u, float* __restrict__ pr) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     (void)fl;
@@ -800,6 +848,7 @@ __global__ void k_piso_vel(const __grid_constant__ Params P, const uint8_t* __re
         uo[a] = ld(u, a * N + c.i);
     }
     if (!(m & 64u)) return;
+    if (pr) pr[c.i] += pP;
     float pf[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) pf[f] = nb_fluid(m, f) ? 0.5f * (pP + pn[f]) : pP;
@@ -1046,16 +1095,16 @@ void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8
 }
 void launch_vel_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
                            const float* pr, const float* eddy, const float* face, const float* bles,
-                           const float* drag, float* Dv, float* bv) {
-    WF_LAUNCH(k_vel_precompute, B, fl, uT, pr, eddy, face, bles, drag, Dv, bv);
+                           const float* drag, float* Dv, float* bv, float* A, float* iD) {
+    WF_LAUNCH(k_vel_precompute, B, fl, uT, pr, eddy, face, bles, drag, Dv, bv, A, iD);
 }
 void launch_vel_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uI, const float* uT,
                       const float* eddy, const float* face, const float* Dv, const float* bv, float* uo) {
     WF_LAUNCH(k_vel_sweep, fl, uI, uT, eddy, face, Dv, bv, uo);
 }
 void launch_pres_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* u,
-                            const float* pr, const float* Dv, const float* iD, float* Dp, float* bp) {
-    WF_LAUNCH(k_pres_precompute, B, fl, u, pr, Dv, iD, Dp, bp);
+                            const float* pr, const float* Dv, const float* iD, float* Dp, float* bp, float* c3) {
+    WF_LAUNCH(k_pres_precompute, B, fl, u, pr, Dv, iD, Dp, bp, c3);
 }
 void launch_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pin, const float* Dv,
                        const float* Dp, const float* bp, float* pout) {
@@ -1076,8 +1125,8 @@ void launch_normalize(const Params& P, cudaStream_t st, const uint8_t* fl, float
     WF_LAUNCH(k_norm_apply, fl, ref, pr);
 }
 void launch_apply_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
-                      const float* iD, float* uc, float* u) {
-    WF_LAUNCH(k_apply_vel, fl, pc, Dv, iD, uc, u);
+                      const float* iD, float* uc, float* u, float* pr) {
+    WF_LAUNCH(k_apply_vel, fl, pc, Dv, iD, uc, u, pr);
 }
 void launch_piso_aodu(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uc, const float* uT,
                       const float* eddy, const float* face, float* aodu) {
@@ -1088,8 +1137,8 @@ void launch_piso_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl,
     WF_LAUNCH(k_piso_pres_sweep, fl, pin, Dv, aodu, pout);
 }
 void launch_piso_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
-                     const float* iD, const float* aodu, float* uc, float* u) {
-    WF_LAUNCH(k_piso_vel, fl, pc, Dv, iD, aodu, uc, u);
+                     const float* iD, const float* aodu, float* uc, float* u, float* pr) {
+    WF_LAUNCH(k_piso_vel, fl, pc, Dv, iD, aodu, uc, u, pr);
 }
 void launch_nbmask(const Params& P, cudaStream_t st, const uint8_t* fl, uint8_t* nbm) {
     WF_LAUNCH(k_nbmask, fl, nbm);

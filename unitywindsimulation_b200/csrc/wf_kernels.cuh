@@ -21,24 +21,25 @@ void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8
 // drag (nullable): Brinkman drag coefficient per cell, added to D as dv*drag.
 void launch_vel_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
                            const float* pr, const float* eddy, const float* face, const float* bles,
-                           const float* drag, float* Dv, float* bv);
+                           const float* drag, float* Dv, float* bv, float* A = nullptr, float* iD = nullptr);
 void launch_vel_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uI, const float* uT,
                       const float* eddy, const float* face, const float* Dv, const float* bv, float* uo);
 // iD (nullable): cached 1/D of the same D (bit-identical to dividing).
 void launch_pres_precompute(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* u,
-                            const float* pr, const float* Dv, const float* iD, float* Dp, float* bp);
+                            const float* pr, const float* Dv, const float* iD, float* Dp, float* bp,
+                            float* c3 = nullptr);
 void launch_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pin, const float* Dv,
                        const float* Dp, const float* bp, float* pout);
 void launch_apply_pres(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, float* pr);
 void launch_normalize(const Params& P, cudaStream_t st, const uint8_t* fl, float* pr, float* ref);
 void launch_apply_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
-                      const float* iD, float* uc, float* u);
+                      const float* iD, float* uc, float* u, float* pr = nullptr);
 void launch_piso_aodu(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uc, const float* uT,
                       const float* eddy, const float* face, float* aodu);
 void launch_piso_pres_sweep(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pin, const float* Dv,
                             const float* aodu, float* pout);
 void launch_piso_vel(const Params& P, cudaStream_t st, const uint8_t* fl, const float* pc, const float* Dv,
-                     const float* iD, const float* aodu, float* uc, float* u);
+                     const float* iD, const float* aodu, float* uc, float* u, float* pr = nullptr);
 // Neighbour masks (Params::nbm) from the flags; run after every flag change.
 void launch_nbmask(const Params& P, cudaStream_t st, const uint8_t* fl, uint8_t* nbm);
 void launch_vel_residual(const Params& P, cudaStream_t st, const float* Dv, const float* u, const float* uI,

@@ -63,6 +63,9 @@ struct wf_solver {
     // three pressure solves of a step share D, so they share the coefficients
     long long d_gen = 1, c3_gen = 0;
     long long id_gen = 0;     // generation of D the cached 1/D (vcoef + 6N) belongs to
+    // the momentum pre-compute of the step in progress wrote vcoef (A and
+    // 1/D) for the current D; the step's sweeps take them as they are
+    bool vcoef_step = false;
     // scratch
     double* part = nullptr;
     double* dsum = nullptr;   // 4 doubles

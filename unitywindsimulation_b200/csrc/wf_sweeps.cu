@@ -765,6 +765,11 @@ void vel_coef(wf_solver* h) {
         h->id_gen = h->d_gen;
         return;
     }
+    if (h->in_step && h->vcoef_step) {  // this step's momentum pre-compute stored them
+        h->vcoef_step = false;
+        h->id_gen = h->d_gen;
+        return;
+    }
     WF_COUNT_LAUNCH();
     k_vel_coef<<<grd(P), blk(), 0, h->st>>>(P, h->fl, h->vb[h->iT], h->eddy, h->face, h->Dv, h->vcoef,
                                             h->vcoef + 6 * N);
