@@ -164,8 +164,8 @@ int materialize_pc(wf_solver* h) {
 int do_les(wf_solver* h) {
     const Params& P = h->P;
     const float* uT = h->vb[h->iT];
-    wf::launch_wallfunc(P, h->st, h->fl, uT, h->face);
-    wf::launch_eddy_vis(P, h->B, h->st, h->fl, uT, h->eddy, h->grad);
+    // CalWallFunc and CSCalEddyVis in one pass over velFieldLastTime
+    wf::launch_eddy_vis(P, h->B, h->st, h->fl, uT, h->eddy, h->grad, h->face);
     wf::launch_les_term(P, h->B, h->st, h->fl, uT, h->eddy, h->face, h->grad, h->bv);
     WF_CHECK_LAUNCH();
     return WF_OK;

@@ -228,8 +228,13 @@ __global__ void k_wallfunc(const __grid_constant__ Params P, const uint8_t* __re
 // When `grad` is given, the cell-centre gradient tensor is also stored (9
 // planes, g[i][j] at plane 3i+j) for the LES term, which needs it at the cell
 // and its six neighbours.
+// `face` (nullable): also runs the wall function first (CSCalLogLawWallFunc,
+// WallFunc.compute:128-190, the same values as k_wallfunc) from the
+// velocities this kernel loads anyway: a fluid cell's own, a solid cell's
+// W/S/D neighbours'.
 __global__ void k_eddy_vis(const __grid_constant__ Params P, const Bnd B, const uint8_t* __restrict__ fl,
-                           const float* __restrict__ uT, float* __restrict__ eddy, float* __restrict__ grad) {
+                           const float* __restrict__ uT, float* __restrict__ eddy, float* __restrict__ grad,
+                           float* __restrict__ face) {
     Cell c;
     if (!cell_of_thread(P, c)) return;
     (void)fl;
@@ -243,6 +248,25 @@ __global__ void k_eddy_vis(const __grid_constant__ Params P, const Bnd B, const 
         const int q = nb_idx(P, c.x, c.y, c.z, c.i, f);
 #pragma unroll
         for (int k = 0; k < 3; ++k) uq[f][k] = ld(uT, (size_t)k * P.N + q);
+    }
+    if (face) {
+        // faces W (1), S (3), D (5); a neighbour outside the domain counts as
+        // not fluid only for the ground of a fixed-value Y0 (fluid cells)
+        float fe0 = 0.f, fe1 = 0.f, fe2 = 0.f;
+        const bool w_in = c.x > 0, s_in = c.y > 0, d_in = c.z > 0;
+        if (m & 64u) {
+            if (w_in && !nb_fluid(m, 1)) fe0 += log_law(hypot2(uP[1], uP[2]), P.dx, P.nu, P.den);
+            if ((s_in && !nb_fluid(m, 3)) || (!s_in && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE))
+                fe1 += log_law(hypot2(uP[0], uP[2]), P.dx, P.nu, P.den);
+            if (d_in && !nb_fluid(m, 5)) fe2 += log_law(hypot2(uP[0], uP[1]), P.dx, P.nu, P.den);
+        } else {
+            if (nb_fluid(m, 1)) fe0 += log_law(hypot2(uq[1][1], uq[1][2]), P.dx, P.nu, P.den);
+            if (nb_fluid(m, 3)) fe1 += log_law(hypot2(uq[3][0], uq[3][2]), P.dx, P.nu, P.den);
+            if (nb_fluid(m, 5)) fe2 += log_law(hypot2(uq[5][0], uq[5][1]), P.dx, P.nu, P.den);
+        }
+        face[c.i] = fe0;
+        face[P.N + c.i] = fe1;
+        face[2 * (size_t)P.N + c.i] = fe2;
     }
     if (!(m & 64u)) return;
     float g[3][3];
@@ -1082,8 +1106,8 @@ void launch_wallfunc(const Params& P, cudaStream_t st, const uint8_t* fl, const 
     WF_LAUNCH(k_wallfunc, fl, uT, face);
 }
 void launch_eddy_vis(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT, float* eddy,
-                     float* grad) {
-    WF_LAUNCH(k_eddy_vis, B, fl, uT, eddy, grad);
+                     float* grad, float* face) {
+    WF_LAUNCH(k_eddy_vis, B, fl, uT, eddy, grad, face);
 }
 void launch_cell_grad(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
                       float* grad) {

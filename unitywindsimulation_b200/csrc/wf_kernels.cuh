@@ -12,8 +12,10 @@ int cell_grid_blocks(const Params& P);
 void launch_wallfunc(const Params& P, cudaStream_t st, const uint8_t* fl, const float* uT, float* face);
 // grad (nullable): 9 planes receiving / holding the cell-centre velocity
 // gradient tensors.
+// face (nullable): the wall function's face viscosities (k_wallfunc's
+// values) from the same pass.
 void launch_eddy_vis(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT, float* eddy,
-                     float* grad);
+                     float* grad, float* face = nullptr);
 void launch_cell_grad(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
                       float* grad);
 void launch_les_term(const Params& P, const Bnd& B, cudaStream_t st, const uint8_t* fl, const float* uT,
