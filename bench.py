@@ -266,7 +266,7 @@ def cpu_baseline(case, steps: int):
                       f"{cores} threads"}
 
 
-def batched_section(steps: int, local: int, small: bool = False):
+def batched_section(steps: int, local: int, small: bool = False, group=None):
     """Batched form on 16 cases: the direction sweep (uneven grids 96..192 x
     48..80(up) x 96..160, wind rotated by 22.5 degree steps), or with
     small=True 16 small grids (about 0.1 M cells each).  The same cases are
@@ -276,27 +276,37 @@ def batched_section(steps: int, local: int, small: bool = False):
     both modes over `steps` steps: child graphs (one parent graph launch per
     step, autotuned chain width) and persistent loops (one cooperative launch
     per Jacobi loop over all cases); the faster is the batched figure.
-    Device time from CUDA events."""
+    Device time from CUDA events.  Under torchrun the cases are dealt to the
+    ranks (replicas.deal: largest first onto the least-loaded rank); each
+    rank steps its share, and the whole-job rates are all cases' cell-steps
+    over the slowest rank's time (barrier and max over ranks around each
+    timed form)."""
     from unitywindsimulation_b200 import FvmSolverCuda, _lib, autotune, cases
+    from unitywindsimulation_b200.replicas import LocalGroup, deal
     from unitywindsimulation_b200.solver import BatchSolver
 
-    cs = cases.batch_small() if small else cases.batch_directions()
+    group = group or LocalGroup()
+    all_cs = cases.batch_small() if small else cases.batch_directions()
+    mine = deal([c.n_cells for c in all_cs], group.world)[group.rank]
+    cs = [all_cs[i] for i in mine]
     solvers = [FvmSolverCuda(c.cfg, device=local) for c in cs]
     for s, c in zip(solvers, cs):
         cases.apply_case(s, c)
-    cache = os.path.join(tempfile.gettempdir(), "windfvm_autotune.json")
+    cache = os.path.join(tempfile.gettempdir(), f"windfvm_autotune_rank{group.rank}.json")  # one file per process
     tuned = []
     for s in solvers:
         s.Step(1)
         tuned.append(autotune.tune(s, cache, reps=3))
-    cells = sum(c.n_cells for c in cs)
+    cells = sum(c.n_cells for c in all_cs)
     for s in solvers:
         s.Step(2)
         s.prepare_graphs()  # every step graph captured before timing
+    group.barrier()
     plain_ms = 0.0
     for s in solvers:
         s.Step(steps)
         plain_ms += s.last_step_ms()
+    plain_ms = group.max_over_ranks(plain_ms)
     b = BatchSolver(solvers)
     width = autotune.tune_batch(b, steps=2, modes=(_lib.BATCH_GRAPHS,))
     modes = {}
@@ -306,9 +316,10 @@ def batched_section(steps: int, local: int, small: bool = False):
             b.set_width(width["width"])
         b.step(1)
         b.prepare_graphs()
+        group.barrier()
         l0 = b.kernel_launches()
         b.step(steps)
-        ms = b.last_step_ms()
+        ms = group.max_over_ranks(b.last_step_ms())
         modes[name] = {"mcell_steps_s": cells * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
                        "gpu_launches": b.kernel_launches() - l0}
     b.close()
@@ -318,8 +329,9 @@ def batched_section(steps: int, local: int, small: bool = False):
     best = max(modes, key=lambda k: modes[k]["mcell_steps_s"])
     batched = modes[best]["mcell_steps_s"]
     name = "batch_small" if small else "batch_directions"
-    return {"workload": f"{name}: {len(cs)} cases, {cells} cells total, grids "
-                        f"{min(c.n_cells for c in cs)}..{max(c.n_cells for c in cs)} cells, nV=50 nP=30 nC=2",
+    return {"workload": f"{name}: {len(all_cs)} cases, {cells} cells total, grids "
+                        f"{min(c.n_cells for c in all_cs)}..{max(c.n_cells for c in all_cs)} cells, nV=50 nP=30 nC=2",
+            "ranks": group.world, "cases_rank0": mine if group.rank == 0 else None,
             "plain_mcell_steps_s": plain, "batched_mcell_steps_s": batched, "batched_over_plain": batched / plain,
             "batched_mode": best, "modes": modes, "steps": steps, "gpu_launches": modes[best]["gpu_launches"],
             "tuned": sorted({(t["pres_k"], t["pres_rows"], t["vel_k"], tuple(t["vel_block"])) for t in tuned}),
@@ -630,9 +642,10 @@ def run_windfvm(args):
 
     solver.close()
     batched = batched_small = None
-    if world == 1 and not args.no_batched:
-        batched = batched_section(BATCH_STEPS, local)
-        batched_small = batched_section(BATCH_STEPS, local, small=True)
+    if not args.no_batched:
+        # the independent cases are dealt to the ranks (replicas.deal)
+        batched = batched_section(BATCH_STEPS, local, group=group)
+        batched_small = batched_section(BATCH_STEPS, local, small=True, group=group)
 
     adjoint = adjoint_scale = None
     if world == 1 and not args.no_adjoint:

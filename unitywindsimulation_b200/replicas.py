@@ -1,6 +1,7 @@
 """Replica plumbing for multi-GPU runs: one process per GPU, each stepping its
-own copy of a workload (the step has no exchange between GPUs, so there is no
-data-path collective).  The only collectives are a barrier around timed
+own copy of a workload, or its share of a set of independent cases (deal);
+the step has no exchange between GPUs, so there is no data-path
+collective.  The only collectives are a barrier around timed
 regions and a max over ranks of each timed duration, so a whole-job figure is
 every rank's work divided by the slowest rank's time.
 
@@ -28,6 +29,23 @@ def whole_job_rate(units_per_rank: float, steps: int, ms_max: float, world: int)
     if ms_max <= 0:
         raise ValueError("non-positive duration")
     return world * units_per_rank * steps / (ms_max / 1e3) / 1e6
+
+
+def deal(sizes, world: int):
+    """Deals independent cases (uneven sizes: grid cells) to `world` ranks:
+    largest first onto the least-loaded rank (ties to the lower rank), so
+    the slowest rank carries as little as the sizes allow.  Returns a list
+    of case indices per rank, each in ascending order.  Deterministic: every
+    rank computes the same deal without communicating."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(x) for x in out]
 
 
 class ReplicaGroup:
@@ -64,3 +82,19 @@ class ReplicaGroup:
             self._torch.distributed.barrier()
             self._torch.distributed.destroy_process_group()
             self.dist = False
+
+
+class LocalGroup:
+    """The group of a single process (rank 0 of 1): barrier and max are
+    no-ops; used where no process group was set up."""
+
+    rank, world, local, dist = 0, 1, 0, False
+
+    def barrier(self) -> None:
+        pass
+
+    def max_over_ranks(self, x: float) -> float:
+        return float(x)
+
+    def close(self) -> None:
+        pass
