@@ -618,12 +618,13 @@ def run_windfvm(args):
                       "runs the next step)"}
 
     # ---- roofline of the dominant kernel ----
-    # The four-sweep pressure wavefront (30 launches, 42 % of the step's
-    # kernel time) leads the momentum sweep (50 launches, 39 %); the roofline
-    # object is the pressure wavefront, the momentum sweep's figures ride
-    # beside it.  Achieved = algorithmic bytes of the launch's sweeps over
-    # its CUDA-event time; traffic = DRAM bytes of one launch (ncu), below
-    # the algorithmic bytes because the wavefront keeps 4 sweeps on chip.
+    # The four-sweep pressure wavefront (k_pres_tma4: TMA-staged tiles, 30
+    # launches per step) and the momentum sweep (50 launches) share the
+    # step's kernel time about equally; the roofline object is the pressure
+    # wavefront, the momentum sweep's figures ride beside it.  Achieved =
+    # algorithmic bytes of the launch's sweeps over its CUDA-event time;
+    # traffic = DRAM bytes of one launch (ncu), below the algorithmic bytes
+    # because the wavefront keeps 4 sweeps on chip.
     peak, peak_kind = measured_peaks()
     v_ms, v_bytes, v_sweeps = solver.time_kernel(_lib.KERNEL_VEL_SWEEP, reps=20, flush_l2=True)
     k_ms, k_bytes, k_sweeps = solver.time_kernel(_lib.KERNEL_PRES_SWEEP, reps=20, flush_l2=True)
@@ -632,7 +633,8 @@ def run_windfvm(args):
     tv, tp = committed_traffic("vel_sweep"), committed_traffic("pres_sweep")
     roofline = {"bound": "hbm", "achieved": k_gbs, "peak": peak, "unit": "GB/s", "frac": k_gbs / peak,
                 "traffic": (tp * N) if tp is not None else None,
-                "kernel": "pressure Jacobi wavefront (4 sweeps per launch)", "ms_per_launch": k_ms,
+                "kernel": "k_pres_tma4: pressure Jacobi wavefront, 4 sweeps per launch, tiles staged by TMA "
+                          "(cp.async.bulk.tensor onto mbarriers)", "ms_per_launch": k_ms,
                 "sweeps_per_launch": k_sweeps, "alg_bytes_per_launch": k_bytes,
                 "peak_source": f"hbm_gbs of {peak_kind}"}
     vel_kernel = {"kernel": "momentum Jacobi sweep (four cells per thread)", "ms_per_launch": v_ms,

@@ -454,6 +454,17 @@ int wf_batch_set_barrier_timeout(wf_batch* b, double ms);
  * barrier released (extra == 0), WF_ERR_TIMEOUT when its wait ran out (extra
  * > 0: arrivals that never come).  No counterpart in the reference. */
 int wf_grid_barrier_selftest(int device, int blocks, int extra, double timeout_ms, int* status);
+/* Self-test of the bounded stage waits of the TMA-staged pressure sweep (the
+ * four-sweep pass the handle's pressure loops use where nx % 4 == 0): one
+ * pass over the handle's current pressure coefficients into its host-I/O
+ * staging buffer (no solver field is written), with every wait limited to
+ * timeout_ms.  short_stage != 0 makes each block's first stage expect 16
+ * bytes more than its loads deliver, so that wait runs out: every block then
+ * returns after its loads in flight have landed.  *status = WF_OK when the
+ * pass completed, WF_ERR_TIMEOUT when a wait ran out; WF_ERR_UNSUPPORTED
+ * where the TMA pass does not apply.  The handle stays usable either way.
+ * No counterpart in the reference. */
+int wf_stage_wait_selftest(wf_solver* h, int short_stage, double timeout_ms, int* status);
 
 /* Temporal-blocking depths of the Jacobi loops: pressure sweeps per pass
  * (1..4) and momentum sweeps per pass (1..2).  Results do not depend on

@@ -197,6 +197,7 @@ _SIGNATURES = {
     "wf_batch_get_mode": (c_int, [c_void_p, POINTER(c_int)]),
     "wf_batch_set_barrier_timeout": (c_int, [c_void_p, c_double]),
     "wf_grid_barrier_selftest": (c_int, [c_int, c_int, c_int, c_double, POINTER(c_int)]),
+    "wf_stage_wait_selftest": (c_int, [c_void_p, c_int, c_double, POINTER(c_int)]),
     "wf_set_tiles": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
     "wf_get_tiles": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "wf_set_blocking": (c_int, [c_void_p, c_int, c_int]),

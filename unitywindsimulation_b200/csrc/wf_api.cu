@@ -119,6 +119,7 @@ void free_all(wf_solver* h) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->hsum) cudaFreeHost(h->hsum);
+    if (h->hstat) cudaFreeHost(h->hstat);
     if (h->cst) {
         cudaStreamSynchronize(h->cst);
         cudaStreamDestroy(h->cst);
@@ -138,6 +139,11 @@ void free_all(wf_solver* h) {
 
 int sync(wf_solver* h) {
     WF_CUDA(cudaStreamSynchronize(h->st));
+    if (h->hstat && *(volatile int*)h->hstat) {
+        *(volatile int*)h->hstat = 0;
+        return set_err(h, WF_ERR_TIMEOUT,
+                       "a bounded wait of the TMA-staged pressure sweep ran out; the pressure fields are not valid");
+    }
     return WF_OK;
 }
 
@@ -647,6 +653,7 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     if (const char* vk = std::getenv("WF_VEL_K")) h->vel_k = std::min(std::max(std::atoi(vk), 1), 2);
     if (const char* v4 = std::getenv("WF_VEC4")) h->vec4 = std::atoi(v4);
     if (const char* pd = std::getenv("WF_PDL")) h->pdl = std::atoi(pd);
+    if (const char* tm = std::getenv("WF_TMA")) h->pres_tma = std::atoi(tm);
 
     Params& P = h->P;
     P.nx = cfg->nx; P.ny = cfg->ny; P.nz = cfg->nz;
@@ -707,6 +714,9 @@ int wf_create(const wf_config* cfg, int device, wf_solver** out) {
     for (int f = 1; f < 6; ++f) h->bnd[f] = h->bnd[f - 1] + 3 * (size_t)P.plane[f - 1];
     for (int f = 0; f < 6; ++f) h->B.p[f] = h->bnd[f];
     if (cudaMallocHost((void**)&h->hsum, 4 * sizeof(double)) != cudaSuccess) return fail(WF_ERR_OOM);
+    if (cudaHostAlloc((void**)&h->hstat, sizeof(int), cudaHostAllocMapped) != cudaSuccess) return fail(WF_ERR_OOM);
+    *h->hstat = 0;
+    if (cudaHostGetDevicePointer((void**)&h->dstat, h->hstat, 0) != cudaSuccess) return fail(WF_ERR_CUDA);
 
     // Constructor sequence, FvmSolverGpu.cs:207-221.  Flags start all fluid
     // (zeroed allocation = CELL_FLUID); faceEddyVis starts at 0 because
@@ -1315,6 +1325,24 @@ int wf_last_step_ms(const wf_solver* h, float* ms) {
 int wf_kernel_launches(const wf_solver* h, int64_t* total) {
     if (!h || !total) return WF_ERR_INVALID_ARG;
     *total = h->launches;
+    return WF_OK;
+}
+
+int wf_stage_wait_selftest(wf_solver* h, int short_stage, double timeout_ms, int* status) {
+    if (!h || !status || !(timeout_ms > 0)) return WF_ERR_INVALID_ARG;
+    if (h->nonuniform) return set_err(h, WF_ERR_UNSUPPORTED, "the TMA pass runs on the uniform grid only");
+    WF_CUDA(cudaSetDevice(h->device));
+    const size_t N = h->P.N;
+    if (!h->stage) WF_TRY(alloc(h, &h->stage, 4 * N * sizeof(float)));
+    float* out = static_cast<float*>(h->stage);
+    if (!wf::pres_tma_ok(h->P, h->pcoef, h->pcoef + 3 * N, h->bp, nullptr))
+        return set_err(h, WF_ERR_UNSUPPORTED, "the TMA pass needs nx % 4 == 0");
+    WF_TRY(sync(h));
+    WF_CUDA(wf::launch_pres_tma4(h->P, h->st, h->num_sms, h->pcoef, h->bp, nullptr, out, nullptr, h->dstat,
+                                 timeout_ms, short_stage != 0));
+    WF_CUDA(cudaStreamSynchronize(h->st));
+    *status = *(volatile int*)h->hstat ? WF_ERR_TIMEOUT : WF_OK;
+    *(volatile int*)h->hstat = 0;
     return WF_OK;
 }
 

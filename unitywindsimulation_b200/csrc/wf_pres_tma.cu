@@ -1,0 +1,391 @@
+// wf_pres_tma.cu - four pressure Jacobi sweeps per pass with TMA-staged
+// halo tiles (CSPresCorrectRhieChow, FvmColl.compute:2790-2848, and
+// CSPisoPresCorrection, PisoColl.compute:181-256).
+//
+// Same 2.5D wavefront as k_pres_msweep<4, 32> (wf_sweeps.cu): a block of
+// 32 x 32 threads owns a 32 x 32 column tile of the x-y plane (a 24 x 24
+// output tile with a 4-cell halo on every side) and streams a chunk of z
+// planes; level s (1..4) is sweep s and computes plane zs + t - s at step t.
+// What differs is how a plane reaches shared memory.  Each z plane of the
+// tile arrives as six 32 x 32 FP32 planes (24 KB): c_E, c_N, c_U and 1/Dp
+// (two 4-D tensor-map boxes of two planes over the contiguous coefficient
+// cache), the right-hand side and the input iterate, written by up to four
+// cp.async.bulk.tensor loads that complete on one mbarrier.  One thread
+// issues them TD planes ahead of the plane the block consumes, into two
+// rings (below) that hold every plane a level still reads.  So no thread
+// issues a global load or a staging store: per step a thread reads its own
+// column's new values (input, c_U, 1/Dp, rhs) into register rings and, per
+// level, the four neighbour values and the four face coefficients from
+// shared memory, at offsets the unrolled z loop fixes at compile time.
+//
+// Out-of-domain cells: the tensor maps' bounds give zeros outside the domain
+// (a box may start at x = -4, y = -4 or a plane below 0, and run past the
+// far edges), which is the reference's InRegion test without branches.
+// Non-fluid cells have 1/Dp = 0 and are never written.
+// The arithmetic, its order and every stored value are those of
+// k_pres_msweep<4, 32>, so the two kernels give bit-identical iterates.
+//
+// Every wait on a stage's mbarrier is bounded (kWaitNs of %globaltimer).  A
+// wait that runs out sets *status, the block agrees on the failure at its
+// next barrier, the issuing thread waits (bounded again) for the loads it
+// still has in flight, and every thread returns; the host reports
+// WF_ERR_TIMEOUT.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+
+#include "wf_sweeps.cuh"
+
+namespace wf {
+namespace {
+
+constexpr int TK = 4;              // sweeps per pass
+constexpr int TT = 32;             // tile edge (threads per row, rows)
+constexpr int TO = TT - 2 * TK;    // output tile edge
+#ifndef WF_TMA_AHEAD
+#define WF_TMA_AHEAD 3
+#endif
+constexpr int TD = WF_TMA_AHEAD;   // planes loaded ahead of the consumed one
+constexpr int TPL = TT * TT;       // floats per tile plane
+// Two rings.  The face ring holds c_E, c_N of a plane (the x/y neighbours of
+// every level read them, level K four steps after the plane arrived); the
+// column ring holds c_U, 1/Dp, rhs and the input iterate (read into the own
+// column's registers when the plane arrives, the input also as level 1's
+// neighbours one step later).  The z loop is unrolled by TU steps, a
+// multiple of both ring lengths and of every register-ring period, so every
+// slot, mbarrier and parity below is a compile-time constant.
+constexpr int TU = 12;             // unrolled z steps per loop trip
+constexpr int TF = 12;             // face-ring slots (plane t in slot t % TF)
+constexpr int TC = 6;              // column-ring slots, one mbarrier each
+enum { F_CE = 0, F_CN = 1, TFQ = 2 };
+enum { C_CU = 0, C_AI = 1, C_RHS = 2, C_PIN = 3, TCQ = 4 };
+constexpr int kFace = TFQ * TPL;   // floats per face-ring slot
+constexpr int kCol = TCQ * TPL;    // floats per column-ring slot
+constexpr int kR = 6;              // register-ring period (c_U, 1/Dp, rhs)
+// shared memory: the two rings, level planes 1..K-1 (double-buffered), TC
+// mbarriers; plus slack to align the base to 1 KB.
+constexpr size_t kSmemFloats = (size_t)TF * kFace + (size_t)TC * kCol + (size_t)(TK - 1) * 2 * TPL;
+constexpr size_t kSmemBytes = kSmemFloats * sizeof(float) + TC * sizeof(unsigned long long) + 1024;
+constexpr unsigned long long kWaitNs = 1000000000ull;  // default limit of one wait: 1 s
+
+static_assert(TO % 4 == 0 && TK % 4 == 0, "tile origins x = bx*TO - TK must be 16-byte aligned");
+static_assert(kSmemBytes <= 232448, "rings exceed the shared memory of one block");
+static_assert(TU % TF == 0 && TU % TC == 0 && TU % kR == 0 && TU % 3 == 0 && TU % 2 == 0,
+              "the unrolled trip must be a multiple of every ring period");
+// Slot reuse: the column slot of plane t is refilled (at the end of step
+// t - 1 - TD + TC) after its last reader, level 1 at step t + 1; the face
+// slot after level K's read at step t + K.
+static_assert(TD + 2 <= TC && TK + 1 + TD <= TF, "rings too short for the prefetch distance");
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase of the given parity, bounded by limit_ns; false when
+// it ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_3d(unsigned dst, const CUtensorMap* map, int x, int y, int z, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(dst),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tma_4d(unsigned dst, const CUtensorMap* map, int x, int y, int z, int q,
+                                       unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(dst),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(q), "r"(bar)
+        : "memory");
+}
+
+struct TmaMaps {
+    CUtensorMap coef;  // 4-D {nx, ny, nz, 4} (c_E, c_N, c_U, 1/Dp), box of two planes
+    CUtensorMap rhs;   // 3-D {nx, ny, nz}
+    CUtensorMap pin;   // 3-D {nx, ny, nz}
+};
+
+struct TmaWave {
+    float* face;            // TF slots of kFace floats
+    float* colr;            // TC slots of kCol floats
+    float (*V)[2][TT][TT];  // V[s - 1]: level s = 1..K-1
+    unsigned bar0;          // shared address of mbarrier 0 (column slot c: bar0 + 8c)
+    const TmaMaps* maps;
+    float* __restrict__ pout;
+    float* __restrict__ pprev;
+    int me, xe, xw, yn, ys;  // own, east, west, north, south offsets in a tile plane
+    int ty, zs, z0, z1, T, sxy, col, x0, y0, tfail;
+    unsigned long long wait_ns;
+    unsigned extra_tx;      // self-test: bytes the block's first stage expects beyond its loads
+    unsigned tx_bytes;      // bytes the loads of one plane deliver
+    bool out_col, has_rhs, has_pin, bad;
+    float h[TK + 1][3];            // level values, ring of the last 3 planes
+    float qa[kR], qr[kR], qu[kR];  // own column's 1/Dp, rhs, c_U of the last kR planes
+
+    // Issued by thread 0: the loads of plane zs + t (t = trip base + PH)
+    // into face slot PH % TF and column slot PH % TC, completing on the
+    // column slot's mbarrier.  Planes outside [0, nz) read as zeros.
+    template <int PH>
+    __device__ __forceinline__ void issue(int t) const {
+        constexpr int fs = PH % TF, cs = PH % TC;
+        const unsigned bar = bar0 + cs * 8;
+        const int p = zs + t;
+        const unsigned fdst = smem_addr(face + fs * kFace);
+        const unsigned cdst = smem_addr(colr + cs * kCol);
+        mbar_expect(bar, tx_bytes + (t == 0 ? extra_tx : 0u));
+        tma_4d(fdst, &maps->coef, x0, y0, p, 0, bar);                    // c_E, c_N
+        tma_4d(cdst, &maps->coef, x0, y0, p, 2, bar);                    // c_U, 1/Dp
+        if (has_rhs) tma_3d(cdst + sizeof(float) * TPL * C_RHS, &maps->rhs, x0, y0, p, bar);
+        if (has_pin) tma_3d(cdst + sizeof(float) * TPL * C_PIN, &maps->pin, x0, y0, p, bar);
+    }
+
+    // Step t = trip base + PH: plane zs + t enters level 0, level s computes
+    // plane zs + t - s.  Planes before zs (t < s) feed only values outside
+    // the pass's dependency cone; their slots hold zeros.
+    template <int PH>
+    __device__ __forceinline__ void step(int t) {
+        if (t >= T) return;  // uniform over the block
+        constexpr int cur = PH & 1, prv = cur ^ 1;
+        constexpr int h0 = PH % 3, hm1 = (PH + 2) % 3, hm2 = (PH + 1) % 3;
+        constexpr int cs = PH % TC;
+        constexpr unsigned parity = (PH / TC) & 1;  // use t / TC of the slot; TU / TC is even
+        if (!bad) bad = !mbar_wait(bar0 + cs * 8, parity, wait_ns);
+        // plane zs + t enters level 0 and the own-column rings
+        const float* cn = colr + cs * kCol + me;
+        h[0][h0] = cn[C_PIN * TPL];
+        qu[PH % kR] = cn[C_CU * TPL];
+        qa[PH % kR] = cn[C_AI * TPL];
+        qr[PH % kR] = cn[C_RHS * TPL];
+#pragma unroll
+        for (int s = 1; s <= TK; ++s) {
+            if (ty >= s && ty < TT - s) {  // rows this level must produce
+                const int rs = (PH - s + 2 * kR) % kR;
+                const int rd = (PH - s - 1 + 2 * kR) % kR;
+                const float* fq = face + ((PH - s + TF) % TF) * kFace;
+                // level s-1 on plane zs+t-s: the input iterate (column ring) or a level plane
+                const float* L = s == 1 ? colr + ((PH - 1 + TC) % TC) * kCol + C_PIN * TPL : &V[s - 2][prv][0][0];
+                float acc = -(fq[F_CE * TPL + me] * L[xe]);
+                acc -= fq[F_CE * TPL + xw] * L[xw];
+                acc -= fq[F_CN * TPL + me] * L[yn];
+                acc -= fq[F_CN * TPL + ys] * L[ys];
+                acc -= qu[rs] * h[s - 1][h0];
+                acc -= qu[rd] * h[s - 1][hm2];
+                const float v = qa[rs] * (acc + qr[rs]);
+                if (s == TK && pout) {
+                    const int q = zs + t - TK;
+                    if (out_col && q >= z0 && q < z1 && qa[rs] != 0.f) {
+                        const int i = q * sxy + col;
+                        pout[i] = v;
+                        if (pprev) pprev[i] = h[TK - 1][hm1];
+                    }
+                }
+                h[s][h0] = v;
+                if (s < TK) (&V[s - 1][cur][0][0])[me] = v;
+            }
+        }
+        // every read of step t is done: the slots of plane zs + t + 1 + TD
+        // (last read by level 1 at step t + TD + 2 - TC and by level K at
+        // step t + TD + 1 + K - TF) may be refilled
+        if (__syncthreads_or(bad)) {
+            bad = true;
+            tfail = t;
+            return;
+        }
+        if (me == 0 && t + 1 + TD < T) issue<(PH + 1 + TD) % TU>(t + 1 + TD);
+    }
+};
+
+// Prologue: thread 0 issues planes 0..TD.
+template <int P>
+__device__ __forceinline__ void issue_first(const TmaWave& w) {
+    if constexpr (P <= TD) {
+        if (P < w.T) w.issue<P>(P);
+        issue_first<P + 1>(w);
+    }
+}
+
+// Steps t0 + PH .. t0 + TU - 1 of one unrolled trip; false once a wait ran out.
+template <int PH>
+__device__ __forceinline__ bool trip(TmaWave& w, int t0) {
+    if constexpr (PH < TU) {
+        w.step<PH>(t0 + PH);
+        if (w.bad) return false;
+        return trip<PH + 1>(w, t0);
+    } else {
+        return true;
+    }
+}
+
+static_assert((TU / TC) % 2 == 0, "a trip must advance every column slot by an even number of uses");
+
+__global__ void __launch_bounds__(TT* TT, 1)
+    k_pres_tma4(const __grid_constant__ TmaMaps maps, int nx, int ny, int nz, int has_rhs, int has_pin,
+                float* __restrict__ pout, float* __restrict__ pprev, int zchunk, int* __restrict__ status,
+                unsigned long long wait_ns, unsigned extra_tx) {
+    extern __shared__ __align__(1024) unsigned char tsm_raw[];
+    // offset (not an integer round trip) keeps every pointer in the shared
+    // window, so the compiler emits shared-memory loads
+    const unsigned pad = (1024u - (smem_addr(tsm_raw) & 1023u)) & 1023u;
+    float* base = reinterpret_cast<float*>(tsm_raw + pad);
+    TmaWave w;
+    w.face = base;
+    w.colr = base + TF * kFace;
+    w.V = reinterpret_cast<float(*)[2][TT][TT]>(w.colr + TC * kCol);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(w.colr + TC * kCol + (TK - 1) * 2 * TPL);
+    w.bar0 = smem_addr(bars);
+    w.maps = &maps;
+    const int tx = threadIdx.x;
+    w.ty = threadIdx.y;
+    w.me = w.ty * TT + tx;
+    w.xe = w.ty * TT + min(tx + 1, TT - 1);
+    w.xw = w.ty * TT + max(tx - 1, 0);
+    w.yn = min(w.ty + 1, TT - 1) * TT + tx;
+    w.ys = max(w.ty - 1, 0) * TT + tx;
+    w.x0 = blockIdx.x * TO - TK;
+    w.y0 = blockIdx.y * TO - TK;
+    const int x = w.x0 + tx;
+    const int y = w.y0 + w.ty;
+    w.z0 = blockIdx.z * zchunk;
+    w.z1 = min(w.z0 + zchunk, nz);
+    const bool inxy = x >= 0 && x < nx && y >= 0 && y < ny;
+    w.out_col = inxy && tx >= TK && tx < TT - TK && w.ty >= TK && w.ty < TT - TK;
+    w.sxy = nx * ny;
+    w.col = inxy ? y * nx + x : 0;
+    w.pout = pout;
+    w.pprev = pprev;
+    w.has_rhs = has_rhs != 0;
+    w.has_pin = has_pin != 0;
+    w.tx_bytes = (unsigned)(sizeof(float) * TPL * (4 + (has_rhs ? 1 : 0) + (has_pin ? 1 : 0)));
+    w.bad = false;
+    w.tfail = 0;
+    w.wait_ns = wait_ns;
+    w.extra_tx = extra_tx;
+    // The rings and the level planes start at zero (the rhs and input planes
+    // stay zero when absent: no load writes them).
+    for (int i = w.me; i < (int)kSmemFloats; i += TT * TT) base[i] = 0.f;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) w.qa[r] = w.qr[r] = w.qu[r] = 0.f;
+#pragma unroll
+    for (int s = 0; s <= TK; ++s) w.h[s][0] = w.h[s][1] = w.h[s][2] = 0.f;
+    w.zs = w.z0 - TK;
+    w.T = (w.z1 - w.z0) + 2 * TK;
+    if (w.me == 0) {
+        for (int c = 0; c < TC; ++c) mbar_init(w.bar0 + c * 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // generic-proxy zeroing above before any async-proxy write to the rings
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (w.me == 0) issue_first<0>(w);
+    for (int t0 = 0; t0 < w.T; t0 += TU)
+        if (!trip<0>(w, t0)) break;
+    if (w.bad && w.me == 0) {
+        if (status) atomicExch(status, 1);
+        // Loads still in flight: the plane of the failed step and the TD
+        // planes issued ahead of it.  Wait for them (bounded) before the
+        // block's shared memory is released.
+        for (int t = w.tfail; t <= w.tfail + TD && t < w.T; ++t)
+            mbar_wait(w.bar0 + (t % TC) * 8, (unsigned)((t / TC) & 1), wait_ns);
+    }
+}
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encoder() {
+    static EncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeFn>(p);
+    });
+    return fn;
+}
+
+#ifndef WF_TMA_L2P
+#define WF_TMA_L2P CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+#endif
+constexpr CUtensorMapL2promotion kL2Promotion = WF_TMA_L2P;
+
+// Tiled map over `planes` consecutive N-float planes of a grid (rank 3 when
+// planes == 1, else rank 4), box 32 x 32 x 1 (x box_planes), zero fill
+// outside.
+bool encode(CUtensorMap* m, const Params& P, const float* base, int planes, int box_planes) {
+    EncodeFn fn = encoder();
+    if (!fn || !base) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)P.nx, (cuuint64_t)P.ny, (cuuint64_t)P.nz, (cuuint64_t)planes};
+    const cuuint64_t strides[3] = {sizeof(float) * (cuuint64_t)P.nx, sizeof(float) * (cuuint64_t)P.nx * P.ny,
+                                   sizeof(float) * (cuuint64_t)P.N};
+    const cuuint32_t box[4] = {TT, TT, 1, (cuuint32_t)box_planes};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, planes > 1 ? 4 : 3, const_cast<float*>(base), dims, strides, box,
+              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, kL2Promotion,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+size_t pres_tma_smem() { return kSmemBytes; }
+const void* pres_tma_kernel() { return reinterpret_cast<const void*>(k_pres_tma4); }
+
+bool pres_tma_ok(const Params& P, const float* c3, const float* ainv, const float* rhs, const float* in) {
+    return P.nx % 4 == 0 && ainv == c3 + 3 * (size_t)P.N && aligned16(c3) && aligned16(rhs) && aligned16(in) &&
+           encoder() != nullptr;
+}
+
+cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const float* c3, const float* rhs,
+                             const float* in, float* out, float* prev, int* status, double wait_ms,
+                             bool short_stage) {
+    TmaMaps maps;
+    std::memset(&maps, 0, sizeof(maps));
+    if (!encode(&maps.coef, P, c3, 4, 2)) return cudaErrorInvalidValue;
+    if (rhs && !encode(&maps.rhs, P, rhs, 1, 1)) return cudaErrorInvalidValue;
+    if (in && !encode(&maps.pin, P, in, 1, 1)) return cudaErrorInvalidValue;
+    const int gx = (P.nx + TO - 1) / TO, gy = (P.ny + TO - 1) / TO;
+    sms = sms > 0 ? sms : 148;
+    int nchunk = std::max(1, sms / std::max(gx * gy, 1));
+    const int zchunk = std::max(2 * TK + 2, (P.nz + nchunk - 1) / nchunk);
+    nchunk = (P.nz + zchunk - 1) / zchunk;
+    WF_COUNT_LAUNCH();
+    const unsigned long long wait_ns = wait_ms > 0 ? (unsigned long long)(wait_ms * 1e6) : kWaitNs;
+    k_pres_tma4<<<dim3(gx, gy, nchunk), dim3(TT, TT), kSmemBytes, st>>>(
+        maps, P.nx, P.ny, P.nz, rhs ? 1 : 0, in ? 1 : 0, out, prev, zchunk, status, wait_ns, short_stage ? 16u : 0u);
+    return cudaGetLastError();
+}
+
+}  // namespace wf

@@ -91,6 +91,12 @@ struct wf_solver {
     int pres_k = 4;           // pressure sweeps per multi-sweep pass (1..4)
     int vel_k = 1;            // momentum sweeps per multi-sweep pass (1..2)
     int pres_ty = 32;         // tile rows of the pressure multi-sweep kernel (32 or 16)
+    int pres_tma = 1;         // four-sweep passes with TMA-staged tiles where they apply
+                              // (WF_TMA=0: the per-thread-staged kernel; same iterates)
+    // sticky status of the bounded waits in the TMA-staged kernel: page-locked
+    // host word (hstat) and its device alias (dstat); nonzero = a wait ran out
+    int* hstat = nullptr;
+    int* dstat = nullptr;
     int vel_blk[3] = {32, 4, 2};  // block of the four-cell momentum sweep (256 threads)
     int num_sms = 148;        // multiprocessors of the device
     int pdl = 1;              // programmatic dependent launch in the non-uniform grid's sweep chains

@@ -881,6 +881,8 @@ int sweeps_setup() {
     opt_in(k_pres_msweep<3, 16>, pres_msweep_smem(3, 16));
     opt_in(k_pres_msweep<4, 16>, pres_msweep_smem(4, 16));
     if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pres_tma_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_tma_smem());
+    if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_vel_msweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_msweep_smem(1));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_vel_msweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_msweep_smem(2));
@@ -982,6 +984,9 @@ void launch_msweep_k(wf_solver* h, const float* rhs, const float* in, float* out
     int zchunk = 0, nchunk = 0;
     wave_chunks_n(h->num_sms * (TY == 32 ? 1 : 2), P.nz, gx * gy, K, zchunk, nchunk);
     const size_t smem = pres_msweep_smem(K, TY);
+    if (K == 4 && TY == 32 && h->pres_tma && h->dstat && pres_tma_ok(P, h->pcoef, h->pcoef + 3 * N, rhs, in) &&
+        launch_pres_tma4(P, h->st, h->num_sms, h->pcoef, rhs, in, out, prev, h->dstat) == cudaSuccess)
+        return;
     WF_COUNT_LAUNCH();
     k_pres_msweep<K, TY><<<dim3(gx, gy, nchunk), dim3(MS_TX, TY), smem, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
                                                                                in, out, prev, zchunk, nullptr);

@@ -142,6 +142,20 @@ cudaError_t launch_fused_pres_loop(cudaStream_t st, int blocks, const FusedPresC
 cudaError_t launch_barrier_selftest(cudaStream_t st, int blocks, int extra, GridBar* bar,
                                     unsigned long long timeout_ns);
 
+// Four pressure sweeps per pass with TMA-staged tiles (wf_pres_tma.cu):
+// the same iterates as k_pres_msweep<4, 32>, bit for bit.  Applies where
+// pres_tma_ok (nx % 4 == 0, ainv == c3 + 3N, 16-byte aligned planes, the
+// driver's tensor-map encoder present).  A bounded wait that runs out
+// (wait_ms per wait; <= 0: 1 s) sets *status (device-visible) to 1.
+// short_stage (self-test only): each block's first loaded stage expects 16
+// bytes more than its loads deliver, so its wait runs out.
+size_t pres_tma_smem();
+const void* pres_tma_kernel();
+bool pres_tma_ok(const Params& P, const float* c3, const float* ainv, const float* rhs, const float* in);
+cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const float* c3, const float* rhs,
+                             const float* in, float* out, float* prev, int* status, double wait_ms = 0.0,
+                             bool short_stage = false);
+
 // Event-timed launches of one hot kernel (WF_KERNEL_*), see wf_time_kernel.
 int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double* bytes, int* sweeps);
 
