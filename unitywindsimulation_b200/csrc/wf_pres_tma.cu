@@ -14,9 +14,10 @@
 // issues them TD planes ahead of the plane the block consumes, into two
 // rings (below) that hold every plane a level still reads.  So no thread
 // issues a global load or a staging store: per step a thread reads its own
-// column's new values (input, c_U, 1/Dp, rhs) into register rings and, per
-// level, the four neighbour values and the four face coefficients from
-// shared memory, at offsets the unrolled z loop fixes at compile time.
+// column's new values (input, c_E, c_N, c_U, 1/Dp, rhs) into register rings
+// and, per level, the four neighbour values and the west and south face
+// coefficients from shared memory, at offsets the unrolled z loop fixes at
+// compile time.
 //
 // Out-of-domain cells: the tensor maps' bounds give zeros outside the domain
 // (a box may start at x = -4, y = -4 or a plane below 0, and run past the
@@ -151,6 +152,7 @@ struct TmaWave {
     bool out_col, has_rhs, has_pin, bad;
     float h[TK + 1][3];            // level values, ring of the last 3 planes
     float qa[kR], qr[kR], qu[kR];  // own column's 1/Dp, rhs, c_U of the last kR planes
+    float qe[kR], qn[kR];          // own column's c_E, c_N of the last kR planes
 
     // Issued by thread 0: the loads of plane zs + t (t = trip base + PH)
     // into face slot PH % TF and column slot PH % TC, completing on the
@@ -186,6 +188,8 @@ struct TmaWave {
         qu[PH % kR] = cn[C_CU * TPL];
         qa[PH % kR] = cn[C_AI * TPL];
         qr[PH % kR] = cn[C_RHS * TPL];
+        qe[PH % kR] = face[(PH % TF) * kFace + F_CE * TPL + me];
+        qn[PH % kR] = face[(PH % TF) * kFace + F_CN * TPL + me];
 #pragma unroll
         for (int s = 1; s <= TK; ++s) {
             if (ty >= s && ty < TT - s) {  // rows this level must produce
@@ -194,9 +198,9 @@ struct TmaWave {
                 const float* fq = face + ((PH - s + TF) % TF) * kFace;
                 // level s-1 on plane zs+t-s: the input iterate (column ring) or a level plane
                 const float* L = s == 1 ? colr + ((PH - 1 + TC) % TC) * kCol + C_PIN * TPL : &V[s - 2][prv][0][0];
-                float acc = -(fq[F_CE * TPL + me] * L[xe]);
+                float acc = -(qe[rs] * L[xe]);
                 acc -= fq[F_CE * TPL + xw] * L[xw];
-                acc -= fq[F_CN * TPL + me] * L[yn];
+                acc -= qn[rs] * L[yn];
                 acc -= fq[F_CN * TPL + ys] * L[ys];
                 acc -= qu[rs] * h[s - 1][h0];
                 acc -= qu[rd] * h[s - 1][hm2];
