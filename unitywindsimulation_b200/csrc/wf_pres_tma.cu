@@ -2,10 +2,13 @@
 // halo tiles (CSPresCorrectRhieChow, FvmColl.compute:2790-2848, and
 // CSPisoPresCorrection, PisoColl.compute:181-256).
 //
-// Same 2.5D wavefront as k_pres_msweep<4, 32> (wf_sweeps.cu): a block of
-// 32 x 32 threads owns a 32 x 32 column tile of the x-y plane (a 24 x 24
-// output tile with a 4-cell halo on every side) and streams a chunk of z
-// planes; level s (1..4) is sweep s and computes plane zs + t - s at step t.
+// Same 2.5D wavefront as k_pres_msweep<4, 32> (wf_sweeps.cu): a block owns a
+// 32 x 32 column tile of the x-y plane (a 24 x 24 output tile with a 4-cell
+// halo on every side) and streams a chunk of z planes; level s (1..4) is
+// sweep s and computes plane zs + t - s at step t.  The block has 32 x 16
+// threads, each owning two adjacent tile rows (TR), so one of each row's two
+// y neighbours and one south face coefficient come from the thread's own
+// registers; 16 warps per SM with two independent cells each.
 // What differs is how a plane reaches shared memory.  Each z plane of the
 // tile arrives as six 32 x 32 FP32 planes (24 KB): c_E, c_N, c_U and 1/Dp
 // (two 4-D tensor-map boxes of two planes over the contiguous coefficient
@@ -136,6 +139,11 @@ struct TmaMaps {
     CUtensorMap pin;   // 3-D {nx, ny, nz}
 };
 
+// One block of TT x (TT / R) threads; thread (tx, j) owns the R adjacent
+// tile rows R*j .. R*j + R - 1 of column tx.  With R = 2 a thread's second
+// row takes its south neighbour values and south face coefficient, and its
+// first row its north neighbour values, from the thread's own registers.
+template <int R>
 struct TmaWave {
     float* face;            // TF slots of kFace floats
     float* colr;            // TC slots of kCol floats
@@ -144,15 +152,17 @@ struct TmaWave {
     const TmaMaps* maps;
     float* __restrict__ pout;
     float* __restrict__ pprev;
-    int me, xe, xw, yn, ys;  // own, east, west, north, south offsets in a tile plane
-    int ty, zs, z0, z1, T, sxy, col, x0, y0, tfail;
+    int me, xe, xw, yn, ys;  // row 0: own, east, west offsets; north of the last row, south of row 0
+    int r0, zs, z0, z1, T, sxy, x0, y0, tfail;
+    int col[R];             // grid index (x, y) of each row's column
     unsigned long long wait_ns;
     unsigned extra_tx;      // self-test: bytes the block's first stage expects beyond its loads
     unsigned tx_bytes;      // bytes the loads of one plane deliver
-    bool out_col, has_rhs, has_pin, bad;
-    float h[TK + 1][3];            // level values, ring of the last 3 planes
-    float qa[kR], qr[kR], qu[kR];  // own column's 1/Dp, rhs, c_U of the last kR planes
-    float qe[kR], qn[kR];          // own column's c_E, c_N of the last kR planes
+    bool out_col[R];
+    bool has_rhs, has_pin, bad, lead;
+    float h[R][TK + 1][3];            // level values, ring of the last 3 planes
+    float qa[R][kR], qr[R][kR], qu[R][kR];  // own column's 1/Dp, rhs, c_U of the last kR planes
+    float qe[R][kR], qn[R][kR];       // own column's c_E, c_N of the last kR planes
 
     // Issued by thread 0: the loads of plane zs + t (t = trip base + PH)
     // into face slot PH % TF and column slot PH % TC, completing on the
@@ -183,38 +193,56 @@ struct TmaWave {
         constexpr unsigned parity = (PH / TC) & 1;  // use t / TC of the slot; TU / TC is even
         if (!bad) bad = !mbar_wait(bar0 + cs * 8, parity, wait_ns);
         // plane zs + t enters level 0 and the own-column rings
-        const float* cn = colr + cs * kCol + me;
-        h[0][h0] = cn[C_PIN * TPL];
-        qu[PH % kR] = cn[C_CU * TPL];
-        qa[PH % kR] = cn[C_AI * TPL];
-        qr[PH % kR] = cn[C_RHS * TPL];
-        qe[PH % kR] = face[(PH % TF) * kFace + F_CE * TPL + me];
-        qn[PH % kR] = face[(PH % TF) * kFace + F_CN * TPL + me];
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const float* cn = colr + cs * kCol + me + k * TT;
+            h[k][0][h0] = cn[C_PIN * TPL];
+            qu[k][PH % kR] = cn[C_CU * TPL];
+            qa[k][PH % kR] = cn[C_AI * TPL];
+            qr[k][PH % kR] = cn[C_RHS * TPL];
+            qe[k][PH % kR] = face[(PH % TF) * kFace + F_CE * TPL + me + k * TT];
+            qn[k][PH % kR] = face[(PH % TF) * kFace + F_CN * TPL + me + k * TT];
+        }
 #pragma unroll
         for (int s = 1; s <= TK; ++s) {
-            if (ty >= s && ty < TT - s) {  // rows this level must produce
+            // rows this level must produce: [s, TT - s); a thread computes all
+            // its rows when any of them is in that range (the others give values
+            // no later level reads)
+            if (r0 + R - 1 >= s && r0 < TT - s) {
                 const int rs = (PH - s + 2 * kR) % kR;
                 const int rd = (PH - s - 1 + 2 * kR) % kR;
                 const float* fq = face + ((PH - s + TF) % TF) * kFace;
                 // level s-1 on plane zs+t-s: the input iterate (column ring) or a level plane
                 const float* L = s == 1 ? colr + ((PH - 1 + TC) % TC) * kCol + C_PIN * TPL : &V[s - 2][prv][0][0];
-                float acc = -(qe[rs] * L[xe]);
-                acc -= fq[F_CE * TPL + xw] * L[xw];
-                acc -= qn[rs] * L[yn];
-                acc -= fq[F_CN * TPL + ys] * L[ys];
-                acc -= qu[rs] * h[s - 1][h0];
-                acc -= qu[rd] * h[s - 1][hm2];
-                const float v = qa[rs] * (acc + qr[rs]);
-                if (s == TK && pout) {
-                    const int q = zs + t - TK;
-                    if (out_col && q >= z0 && q < z1 && qa[rs] != 0.f) {
-                        const int i = q * sxy + col;
-                        pout[i] = v;
-                        if (pprev) pprev[i] = h[TK - 1][hm1];
-                    }
+                float v[R];
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    // level s-1 on plane zs+t-s in the rows above and below,
+                    // and the south face coefficient
+                    const float ln = k + 1 < R ? h[k + 1][s - 1][hm1] : L[yn];
+                    const float ls = k > 0 ? h[k - 1][s - 1][hm1] : L[ys];
+                    const float cs_ = k > 0 ? qn[k - 1][rs] : fq[F_CN * TPL + ys];
+                    float acc = -(qe[k][rs] * L[xe + k * TT]);
+                    acc -= fq[F_CE * TPL + xw + k * TT] * L[xw + k * TT];
+                    acc -= qn[k][rs] * ln;
+                    acc -= cs_ * ls;
+                    acc -= qu[k][rs] * h[k][s - 1][h0];
+                    acc -= qu[k][rd] * h[k][s - 1][hm2];
+                    v[k] = qa[k][rs] * (acc + qr[k][rs]);
                 }
-                h[s][h0] = v;
-                if (s < TK) (&V[s - 1][cur][0][0])[me] = v;
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    if (s == TK && pout) {
+                        const int q = zs + t - TK;
+                        if (out_col[k] && q >= z0 && q < z1 && qa[k][rs] != 0.f) {
+                            const int i = q * sxy + col[k];
+                            pout[i] = v[k];
+                            if (pprev) pprev[i] = h[k][TK - 1][hm1];
+                        }
+                    }
+                    h[k][s][h0] = v[k];
+                    if (s < TK) (&V[s - 1][cur][0][0])[me + k * TT] = v[k];
+                }
             }
         }
         // every read of step t is done: the slots of plane zs + t + 1 + TD
@@ -225,24 +253,24 @@ struct TmaWave {
             tfail = t;
             return;
         }
-        if (me == 0 && t + 1 + TD < T) issue<(PH + 1 + TD) % TU>(t + 1 + TD);
+        if (lead && t + 1 + TD < T) issue<(PH + 1 + TD) % TU>(t + 1 + TD);
     }
 };
 
 // Prologue: thread 0 issues planes 0..TD.
-template <int P>
-__device__ __forceinline__ void issue_first(const TmaWave& w) {
+template <int P, int R>
+__device__ __forceinline__ void issue_first(const TmaWave<R>& w) {
     if constexpr (P <= TD) {
-        if (P < w.T) w.issue<P>(P);
+        if (P < w.T) w.template issue<P>(P);
         issue_first<P + 1>(w);
     }
 }
 
 // Steps t0 + PH .. t0 + TU - 1 of one unrolled trip; false once a wait ran out.
-template <int PH>
-__device__ __forceinline__ bool trip(TmaWave& w, int t0) {
+template <int PH, int R>
+__device__ __forceinline__ bool trip(TmaWave<R>& w, int t0) {
     if constexpr (PH < TU) {
-        w.step<PH>(t0 + PH);
+        w.template step<PH>(t0 + PH);
         if (w.bad) return false;
         return trip<PH + 1>(w, t0);
     } else {
@@ -252,7 +280,16 @@ __device__ __forceinline__ bool trip(TmaWave& w, int t0) {
 
 static_assert((TU / TC) % 2 == 0, "a trip must advance every column slot by an even number of uses");
 
-__global__ void __launch_bounds__(TT* TT, 1)
+#ifndef WF_TMA_ROWS
+#define WF_TMA_ROWS 2
+#endif
+// Tile rows per thread.  Measured on the 256 x 96 x 192 urban block, four
+// sweeps per pass: 68.3 us with one row (1024 threads), 65.7 us with two
+// (512 threads), 78.9 us with four (256 threads); bit-identical iterates.
+constexpr int TR = WF_TMA_ROWS;
+static_assert(TT % TR == 0, "rows per thread must divide the tile");
+
+__global__ void __launch_bounds__(TT* TT / TR, 1)
     k_pres_tma4(const __grid_constant__ TmaMaps maps, int nx, int ny, int nz, int has_rhs, int has_pin,
                 float* __restrict__ pout, float* __restrict__ pprev, int zchunk, int* __restrict__ status,
                 unsigned long long wait_ns, unsigned extra_tx) {
@@ -261,7 +298,7 @@ __global__ void __launch_bounds__(TT* TT, 1)
     // window, so the compiler emits shared-memory loads
     const unsigned pad = (1024u - (smem_addr(tsm_raw) & 1023u)) & 1023u;
     float* base = reinterpret_cast<float*>(tsm_raw + pad);
-    TmaWave w;
+    TmaWave<TR> w;
     w.face = base;
     w.colr = base + TF * kFace;
     w.V = reinterpret_cast<float(*)[2][TT][TT]>(w.colr + TC * kCol);
@@ -269,22 +306,27 @@ __global__ void __launch_bounds__(TT* TT, 1)
     w.bar0 = smem_addr(bars);
     w.maps = &maps;
     const int tx = threadIdx.x;
-    w.ty = threadIdx.y;
-    w.me = w.ty * TT + tx;
-    w.xe = w.ty * TT + min(tx + 1, TT - 1);
-    w.xw = w.ty * TT + max(tx - 1, 0);
-    w.yn = min(w.ty + 1, TT - 1) * TT + tx;
-    w.ys = max(w.ty - 1, 0) * TT + tx;
+    const int tid = threadIdx.y * TT + tx;
+    w.lead = tid == 0;
+    w.r0 = threadIdx.y * TR;
+    w.me = w.r0 * TT + tx;
+    w.xe = w.r0 * TT + min(tx + 1, TT - 1);
+    w.xw = w.r0 * TT + max(tx - 1, 0);
+    w.yn = min(w.r0 + TR, TT - 1) * TT + tx;  // north of the last row
+    w.ys = max(w.r0 - 1, 0) * TT + tx;        // south of the first row
     w.x0 = blockIdx.x * TO - TK;
     w.y0 = blockIdx.y * TO - TK;
     const int x = w.x0 + tx;
-    const int y = w.y0 + w.ty;
     w.z0 = blockIdx.z * zchunk;
     w.z1 = min(w.z0 + zchunk, nz);
-    const bool inxy = x >= 0 && x < nx && y >= 0 && y < ny;
-    w.out_col = inxy && tx >= TK && tx < TT - TK && w.ty >= TK && w.ty < TT - TK;
+#pragma unroll
+    for (int k = 0; k < TR; ++k) {
+        const int r = w.r0 + k, y = w.y0 + r;
+        const bool inxy = x >= 0 && x < nx && y >= 0 && y < ny;
+        w.out_col[k] = inxy && tx >= TK && tx < TT - TK && r >= TK && r < TT - TK;
+        w.col[k] = inxy ? y * nx + x : 0;
+    }
     w.sxy = nx * ny;
-    w.col = inxy ? y * nx + x : 0;
     w.pout = pout;
     w.pprev = pprev;
     w.has_rhs = has_rhs != 0;
@@ -296,24 +338,27 @@ __global__ void __launch_bounds__(TT* TT, 1)
     w.extra_tx = extra_tx;
     // The rings and the level planes start at zero (the rhs and input planes
     // stay zero when absent: no load writes them).
-    for (int i = w.me; i < (int)kSmemFloats; i += TT * TT) base[i] = 0.f;
+    for (int i = tid; i < (int)kSmemFloats; i += TT * TT / TR) base[i] = 0.f;
 #pragma unroll
-    for (int r = 0; r < kR; ++r) w.qa[r] = w.qr[r] = w.qu[r] = 0.f;
+    for (int k = 0; k < TR; ++k) {
 #pragma unroll
-    for (int s = 0; s <= TK; ++s) w.h[s][0] = w.h[s][1] = w.h[s][2] = 0.f;
+        for (int r = 0; r < kR; ++r) w.qa[k][r] = w.qr[k][r] = w.qu[k][r] = w.qe[k][r] = w.qn[k][r] = 0.f;
+#pragma unroll
+        for (int s = 0; s <= TK; ++s) w.h[k][s][0] = w.h[k][s][1] = w.h[k][s][2] = 0.f;
+    }
     w.zs = w.z0 - TK;
     w.T = (w.z1 - w.z0) + 2 * TK;
-    if (w.me == 0) {
+    if (w.lead) {
         for (int c = 0; c < TC; ++c) mbar_init(w.bar0 + c * 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // generic-proxy zeroing above before any async-proxy write to the rings
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (w.me == 0) issue_first<0>(w);
+    if (w.lead) issue_first<0>(w);
     for (int t0 = 0; t0 < w.T; t0 += TU)
         if (!trip<0>(w, t0)) break;
-    if (w.bad && w.me == 0) {
+    if (w.bad && w.lead) {
         if (status) atomicExch(status, 1);
         // Loads still in flight: the plane of the failed step and the TD
         // planes issued ahead of it.  Wait for them (bounded) before the
@@ -387,7 +432,7 @@ cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const fl
     nchunk = (P.nz + zchunk - 1) / zchunk;
     WF_COUNT_LAUNCH();
     const unsigned long long wait_ns = wait_ms > 0 ? (unsigned long long)(wait_ms * 1e6) : kWaitNs;
-    k_pres_tma4<<<dim3(gx, gy, nchunk), dim3(TT, TT), kSmemBytes, st>>>(
+    k_pres_tma4<<<dim3(gx, gy, nchunk), dim3(TT, TT / TR), kSmemBytes, st>>>(
         maps, P.nx, P.ny, P.nz, rhs ? 1 : 0, in ? 1 : 0, out, prev, zchunk, status, wait_ns, short_stage ? 16u : 0u);
     return cudaGetLastError();
 }
