@@ -38,6 +38,12 @@
 
 struct wf_adjoint;
 
+namespace {
+// Wait status of the TMA-staged pressure passes, or nullptr where the
+// handle runs the per-thread-staged kernel (WF_TMA=0).
+int* tma_status(const wf_solver* h) { return h->pres_tma ? h->dstat : nullptr; }
+}  // namespace
+
 namespace wf {
 namespace {
 
@@ -889,6 +895,15 @@ int adj_fail(wf_adjoint* a, int code, const char* msg) {
         }                                                                      \
     } while (0)
 
+// WF_ERR_TIMEOUT when a bounded wait of the TMA-staged pressure passes ran
+// out since the last check (the solver's sticky wait status).
+int adj_check_waits(wf_adjoint* a) {
+    volatile int* st = a->h->hstat;
+    if (!st || !*st) return WF_OK;
+    *st = 0;
+    return adj_fail(a, WF_ERR_TIMEOUT, "a bounded wait of the TMA-staged pressure pass ran out; results are not valid");
+}
+
 float* V(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * 3 * a->N; }
 float* S(const wf_adjoint* a, float* base, int k) { return base + (size_t)k * a->N; }
 float* SIT(const wf_adjoint* a, const Tape& t, int m, int k) {
@@ -971,7 +986,7 @@ int record_step(wf_adjoint* a, Tape& t, const float* u_in, const float* p_in, in
         wf::launch_pres_coef_ptr(P, st, h->fl, t.D, t.iD, t.c3);
         wf::launch_inv_ptr(P, st, h->fl, t.Dp, t.ainv);
         WFA_CUDA(cudaMemsetAsync(t.qit, 0, s, st));
-        wf::launch_pres_stack(P, st, h->num_sms, t.c3, t.ainv, t.bp, t.qit, a->nP, true);
+        wf::launch_pres_stack(P, st, h->num_sms, t.c3, t.ainv, t.bp, t.qit, a->nP, true, tma_status(h));
         const float* q = S(a, t.qit, a->nP);
         WFA_CUDA(cudaMemsetAsync(t.cbuf, 0, v, st));
         wf::launch_apply_vel(P, st, h->fl, q, t.D, t.iD, V(a, t.cbuf, 0), t.uout);
@@ -985,7 +1000,7 @@ int record_step(wf_adjoint* a, Tape& t, const float* u_in, const float* p_in, in
             wf::launch_piso_aodu(P, st, h->fl, V(a, t.cbuf, m), t.uT, h->eddy, h->face, V(a, t.aod, m));
             wf::launch_piso_pre_ptr(P, st, h->fl, t.D, t.iD, V(a, t.aod, m), S(a, t.pai, m), S(a, t.prhs, m));
             wf::launch_pres_stack(P, st, h->num_sms, t.c3, S(a, t.pai, m), S(a, t.prhs, m), SIT(a, t, m, 0),
-                                  a->nP, true);
+                                  a->nP, true, tma_status(h));
             const float* ss = SIT(a, t, m, a->nP);
             wf::launch_apply_pres(P, st, h->fl, ss, t.pout);
             wf::launch_piso_vel(P, st, h->fl, ss, t.D, t.iD, V(a, t.aod, m), V(a, t.cbuf, m + 1), t.uout);
@@ -1011,7 +1026,7 @@ void reverse_pres_loop(wf_adjoint* a, const float* ai, const float* c3, const fl
     }
     // slot j of a->Wp holds W^{n-j}
     wf::k_adj_pinit<<<wf::lin_blocks(a->N), 256, 0, st>>>((int)a->N, ai, a->sb, a->Wp);
-    if (n > 1) wf::launch_pres_stack(P, st, a->h->num_sms, c3, ai, nullptr, a->Wp, n - 1, false);
+    if (n > 1) wf::launch_pres_stack(P, st, a->h->num_sms, c3, ai, nullptr, a->Wp, n - 1, false, tma_status(a->h));
     if (wf::quad_ok(P, {ai, a->Wp, sstack, a->rb, a->dgb, a->c3b})) {
         const dim3 b4 = wf::cblk(), g4q((P.nx / 4 + b4.x - 1) / b4.x, (P.ny + b4.y - 1) / b4.y, (P.nz + b4.z - 1) / b4.z);
         wf::k_adj_pacc4<<<g4q, b4, 0, st>>>(P, n, ai, a->Wp, sstack, a->rb, a->dgb, a->c3b);
@@ -1204,7 +1219,7 @@ int wf_adj_step_vjp(wf_adjoint* a, int phases, const float* ubar_out, const floa
                                  a->st));
     if (dragbar) WFA_CUDA(cudaMemcpyAsync(dragbar, a->dragb, s, cudaMemcpyDeviceToHost, a->st));
     WFA_CUDA(cudaStreamSynchronize(a->st));
-    return WF_OK;
+    return adj_check_waits(a);
 }
 
 int wf_adj_step_forward(wf_adjoint* a, int phases, float* u_out, float* p_out) {
@@ -1218,7 +1233,7 @@ int wf_adj_step_forward(wf_adjoint* a, int phases, float* u_out, float* p_out) {
     WFA_CUDA(cudaMemcpyAsync(u_out, t.uout, 3 * a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
     WFA_CUDA(cudaMemcpyAsync(p_out, t.pout, a->N * sizeof(float), cudaMemcpyDeviceToHost, a->st));
     WFA_CUDA(cudaStreamSynchronize(a->st));
-    return WF_OK;
+    return adj_check_waits(a);
 }
 
 int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int checkpoint_every, int include_init,
@@ -1399,6 +1414,7 @@ int wf_adj_gradient(wf_adjoint* a, const wf_objective* obj, int n_steps, int che
     }
     WFA_CUDA(cudaEventRecord(E.ev[2], a->st));
     WFA_CUDA(cudaStreamSynchronize(a->st));
+    if (const int w = adj_check_waits(a)) return w;
     // ---- chain to the inflow parameters: X0 plane g_x(y) = u*/k ln((y_c+z0)/z0)
     const int np = P.plane[WF_FACE_X0];
     std::vector<float> gx(np);

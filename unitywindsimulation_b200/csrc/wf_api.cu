@@ -1338,8 +1338,8 @@ int wf_stage_wait_selftest(wf_solver* h, int short_stage, double timeout_ms, int
     if (!wf::pres_tma_ok(h->P, h->pcoef, h->pcoef + 3 * N, h->bp, nullptr))
         return set_err(h, WF_ERR_UNSUPPORTED, "the TMA pass needs nx % 4 == 0");
     WF_TRY(sync(h));
-    WF_CUDA(wf::launch_pres_tma4(h->P, h->st, h->num_sms, h->pcoef, h->bp, nullptr, out, nullptr, h->dstat,
-                                 timeout_ms, short_stage != 0));
+    WF_CUDA(wf::launch_pres_tma4(h->P, h->st, h->num_sms, h->pcoef, h->pcoef + 3 * N, h->bp, nullptr, out, nullptr,
+                                 nullptr, h->dstat, timeout_ms, short_stage != 0));
     WF_CUDA(cudaStreamSynchronize(h->st));
     *status = *(volatile int*)h->hstat ? WF_ERR_TIMEOUT : WF_OK;
     *(volatile int*)h->hstat = 0;

@@ -563,6 +563,15 @@ int wf_batch_step(wf_batch* b, int n_steps) {
     const cudaError_t e = cudaStreamSynchronize(b->st);
     if (e != cudaSuccess) return fail(b, WF_ERR_CUDA, std::string("batch step: ") + cudaGetErrorString(e));
     cudaEventElapsedTime(&b->last_ms, b->e0, b->e1);
+    bool waits_ran_out = false;
+    for (wf_solver* h : b->s)
+        if (h->hstat && *(volatile int*)h->hstat) {
+            *(volatile int*)h->hstat = 0;
+            waits_ran_out = true;
+        }
+    if (waits_ran_out)
+        return fail(b, WF_ERR_TIMEOUT, "a bounded wait of a TMA-staged pressure pass ran out; the cases' fields are "
+                                       "not valid");
     if (persistent) {
         wf::GridBar hb{};
         if (cudaMemcpy(&hb, b->bar, sizeof(hb), cudaMemcpyDeviceToHost) != cudaSuccess)

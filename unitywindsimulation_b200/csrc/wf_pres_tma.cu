@@ -134,7 +134,9 @@ __device__ __forceinline__ void tma_4d(unsigned dst, const CUtensorMap* map, int
 }
 
 struct TmaMaps {
-    CUtensorMap coef;  // 4-D {nx, ny, nz, 4} (c_E, c_N, c_U, 1/Dp), box of two planes
+    CUtensorMap face;  // 4-D {nx, ny, nz, 2} (c_E, c_N), box of both planes
+    CUtensorMap cu;    // 3-D {nx, ny, nz}: c_U
+    CUtensorMap ai;    // 3-D {nx, ny, nz}: 1/Dp
     CUtensorMap rhs;   // 3-D {nx, ny, nz}
     CUtensorMap pin;   // 3-D {nx, ny, nz}
 };
@@ -152,6 +154,8 @@ struct TmaWave {
     const TmaMaps* maps;
     float* __restrict__ pout;
     float* __restrict__ pprev;
+    float* __restrict__ stack;  // optional: level s of every cell to stack + s*N
+    size_t N;
     int me, xe, xw, yn, ys;  // row 0: own, east, west offsets; north of the last row, south of row 0
     int r0, zs, z0, z1, T, sxy, x0, y0, tfail;
     int col[R];             // grid index (x, y) of each row's column
@@ -175,8 +179,9 @@ struct TmaWave {
         const unsigned fdst = smem_addr(face + fs * kFace);
         const unsigned cdst = smem_addr(colr + cs * kCol);
         mbar_expect(bar, tx_bytes + (t == 0 ? extra_tx : 0u));
-        tma_4d(fdst, &maps->coef, x0, y0, p, 0, bar);                    // c_E, c_N
-        tma_4d(cdst, &maps->coef, x0, y0, p, 2, bar);                    // c_U, 1/Dp
+        tma_4d(fdst, &maps->face, x0, y0, p, 0, bar);  // c_E, c_N
+        tma_3d(cdst + sizeof(float) * TPL * C_CU, &maps->cu, x0, y0, p, bar);
+        tma_3d(cdst + sizeof(float) * TPL * C_AI, &maps->ai, x0, y0, p, bar);
         if (has_rhs) tma_3d(cdst + sizeof(float) * TPL * C_RHS, &maps->rhs, x0, y0, p, bar);
         if (has_pin) tma_3d(cdst + sizeof(float) * TPL * C_PIN, &maps->pin, x0, y0, p, bar);
     }
@@ -232,6 +237,10 @@ struct TmaWave {
                 }
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
+                    if (stack) {  // every level, non-fluid cells included (v = 0 there)
+                        const int q = zs + t - s;
+                        if (out_col[k] && q >= z0 && q < z1) stack[(size_t)s * N + q * sxy + col[k]] = v[k];
+                    }
                     if (s == TK && pout) {
                         const int q = zs + t - TK;
                         if (out_col[k] && q >= z0 && q < z1 && qa[k][rs] != 0.f) {
@@ -291,8 +300,8 @@ static_assert(TT % TR == 0, "rows per thread must divide the tile");
 
 __global__ void __launch_bounds__(TT* TT / TR, 1)
     k_pres_tma4(const __grid_constant__ TmaMaps maps, int nx, int ny, int nz, int has_rhs, int has_pin,
-                float* __restrict__ pout, float* __restrict__ pprev, int zchunk, int* __restrict__ status,
-                unsigned long long wait_ns, unsigned extra_tx) {
+                float* __restrict__ pout, float* __restrict__ pprev, int zchunk, float* __restrict__ stack,
+                int* __restrict__ status, unsigned long long wait_ns, unsigned extra_tx) {
     extern __shared__ __align__(1024) unsigned char tsm_raw[];
     // offset (not an integer round trip) keeps every pointer in the shared
     // window, so the compiler emits shared-memory loads
@@ -329,6 +338,8 @@ __global__ void __launch_bounds__(TT* TT / TR, 1)
     w.sxy = nx * ny;
     w.pout = pout;
     w.pprev = pprev;
+    w.stack = stack;
+    w.N = (size_t)nx * ny * nz;
     w.has_rhs = has_rhs != 0;
     w.has_pin = has_pin != 0;
     w.tx_bytes = (unsigned)(sizeof(float) * TPL * (4 + (has_rhs ? 1 : 0) + (has_pin ? 1 : 0)));
@@ -413,16 +424,18 @@ size_t pres_tma_smem() { return kSmemBytes; }
 const void* pres_tma_kernel() { return reinterpret_cast<const void*>(k_pres_tma4); }
 
 bool pres_tma_ok(const Params& P, const float* c3, const float* ainv, const float* rhs, const float* in) {
-    return P.nx % 4 == 0 && ainv == c3 + 3 * (size_t)P.N && aligned16(c3) && aligned16(rhs) && aligned16(in) &&
+    return P.nx % 4 == 0 && c3 && ainv && aligned16(c3) && aligned16(ainv) && aligned16(rhs) && aligned16(in) &&
            encoder() != nullptr;
 }
 
-cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const float* c3, const float* rhs,
-                             const float* in, float* out, float* prev, int* status, double wait_ms,
-                             bool short_stage) {
+cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
+                             const float* rhs, const float* in, float* out, float* prev, float* stack, int* status,
+                             double wait_ms, bool short_stage) {
     TmaMaps maps;
     std::memset(&maps, 0, sizeof(maps));
-    if (!encode(&maps.coef, P, c3, 4, 2)) return cudaErrorInvalidValue;
+    if (!encode(&maps.face, P, c3, 2, 2) || !encode(&maps.cu, P, c3 + 2 * (size_t)P.N, 1, 1) ||
+        !encode(&maps.ai, P, ainv, 1, 1))
+        return cudaErrorInvalidValue;
     if (rhs && !encode(&maps.rhs, P, rhs, 1, 1)) return cudaErrorInvalidValue;
     if (in && !encode(&maps.pin, P, in, 1, 1)) return cudaErrorInvalidValue;
     const int gx = (P.nx + TO - 1) / TO, gy = (P.ny + TO - 1) / TO;
@@ -433,7 +446,8 @@ cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const fl
     WF_COUNT_LAUNCH();
     const unsigned long long wait_ns = wait_ms > 0 ? (unsigned long long)(wait_ms * 1e6) : kWaitNs;
     k_pres_tma4<<<dim3(gx, gy, nchunk), dim3(TT, TT / TR), kSmemBytes, st>>>(
-        maps, P.nx, P.ny, P.nz, rhs ? 1 : 0, in ? 1 : 0, out, prev, zchunk, status, wait_ns, short_stage ? 16u : 0u);
+        maps, P.nx, P.ny, P.nz, rhs ? 1 : 0, in ? 1 : 0, out, prev, zchunk, stack, status, wait_ns,
+        short_stage ? 16u : 0u);
     return cudaGetLastError();
 }
 

@@ -985,7 +985,8 @@ void launch_msweep_k(wf_solver* h, const float* rhs, const float* in, float* out
     wave_chunks_n(h->num_sms * (TY == 32 ? 1 : 2), P.nz, gx * gy, K, zchunk, nchunk);
     const size_t smem = pres_msweep_smem(K, TY);
     if (K == 4 && TY == 32 && h->pres_tma && h->dstat && pres_tma_ok(P, h->pcoef, h->pcoef + 3 * N, rhs, in) &&
-        launch_pres_tma4(P, h->st, h->num_sms, h->pcoef, rhs, in, out, prev, h->dstat) == cudaSuccess)
+        launch_pres_tma4(P, h->st, h->num_sms, h->pcoef, h->pcoef + 3 * N, rhs, in, out, prev, nullptr, h->dstat) ==
+            cudaSuccess)
         return;
     WF_COUNT_LAUNCH();
     k_pres_msweep<K, TY><<<dim3(gx, gy, nchunk), dim3(MS_TX, TY), smem, h->st>>>(P, h->pcoef, h->pcoef + 3 * N, rhs,
@@ -1161,6 +1162,8 @@ int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double
     return WF_OK;
 }
 
+bool aligned_slots(const float* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 // Multi-sweep passes with every iterate kept (see launch_pres_stack).
 template <int K>
 void launch_stack_pass(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
@@ -1174,12 +1177,17 @@ void launch_stack_pass(const Params& P, cudaStream_t st, int sms, const float* c
         P, c3, ainv, rhs, in, nullptr, nullptr, zchunk, slots);
 }
 void launch_pres_stack(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
-                       const float* rhs, float* stack, int n, bool from_zero) {
+                       const float* rhs, float* stack, int n, bool from_zero, int* status) {
     const size_t N = P.N;
     for (int base = 0; base < n;) {
         const int k = std::min(4, n - base);
         const float* in = (base == 0 && from_zero) ? nullptr : stack + base * N;
         float* slots = stack + base * N;
+        if (k == 4 && status && pres_tma_ok(P, c3, ainv, rhs, in) && aligned_slots(slots) &&
+            launch_pres_tma4(P, st, sms, c3, ainv, rhs, in, nullptr, nullptr, slots, status) == cudaSuccess) {
+            base += k;
+            continue;
+        }
         switch (k) {
             case 1: launch_stack_pass<1>(P, st, sms, c3, ainv, rhs, in, slots); break;
             case 2: launch_stack_pass<2>(P, st, sms, c3, ainv, rhs, in, slots); break;

@@ -39,8 +39,10 @@ void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, co
 // multi-sweep kernel, every iterate kept: slot k of `stack` (stride N floats)
 // receives iterate k for k = 1..n on every cell (0 on non-fluid cells).  The
 // first pass reads slot 0, or the all-zero iterate when from_zero is set.
+// Four-sweep passes take the TMA-staged kernel where it applies and
+// `status` is given (the handle's wait status), else k_pres_msweep<4, 32>.
 void launch_pres_stack(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
-                       const float* rhs, float* stack, int n, bool from_zero);
+                       const float* rhs, float* stack, int n, bool from_zero, int* status = nullptr);
 
 // ---- loop recording and persistent multi-case loops (wf_batch.cu) ----
 //
@@ -143,18 +145,19 @@ cudaError_t launch_barrier_selftest(cudaStream_t st, int blocks, int extra, Grid
                                     unsigned long long timeout_ns);
 
 // Four pressure sweeps per pass with TMA-staged tiles (wf_pres_tma.cu):
-// the same iterates as k_pres_msweep<4, 32>, bit for bit.  Applies where
-// pres_tma_ok (nx % 4 == 0, ainv == c3 + 3N, 16-byte aligned planes, the
-// driver's tensor-map encoder present).  A bounded wait that runs out
-// (wait_ms per wait; <= 0: 1 s) sets *status (device-visible) to 1.
-// short_stage (self-test only): each block's first loaded stage expects 16
-// bytes more than its loads deliver, so its wait runs out.
+// the same iterates (and, with `stack`, the same per-level slots) as
+// k_pres_msweep<4, 32>, bit for bit.  Applies where pres_tma_ok (nx % 4 ==
+// 0, 16-byte aligned planes, the driver's tensor-map encoder present).  c3
+// holds c_E, c_N, c_U as consecutive N-float planes.  A bounded wait that
+// runs out (wait_ms per wait; <= 0: 1 s) sets *status (device-visible) to
+// 1.  short_stage (self-test only): each block's first loaded stage expects
+// 16 bytes more than its loads deliver, so its wait runs out.
 size_t pres_tma_smem();
 const void* pres_tma_kernel();
 bool pres_tma_ok(const Params& P, const float* c3, const float* ainv, const float* rhs, const float* in);
-cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const float* c3, const float* rhs,
-                             const float* in, float* out, float* prev, int* status, double wait_ms = 0.0,
-                             bool short_stage = false);
+cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,
+                             const float* rhs, const float* in, float* out, float* prev, float* stack, int* status,
+                             double wait_ms = 0.0, bool short_stage = false);
 
 // Event-timed launches of one hot kernel (WF_KERNEL_*), see wf_time_kernel.
 int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double* bytes, int* sweeps);
