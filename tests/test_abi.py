@@ -115,3 +115,14 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setenv("WINDFVM_LIB", str(tmp_path / "nope.so"))
     with pytest.raises(_lib.WindFvmError):
         _lib.load(str(tmp_path / "nope.so"))
+
+
+@pytest.mark.timeout(60)
+def test_tensor_map_probe_returns(built):
+    """The TMA-staged passes ask whether the driver's tensor-map encoder is
+    present before every launch; the probe must answer (False on a machine
+    without a CUDA driver) rather than spin."""
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    probe = lib._ZN2wf13tma_availableEv
+    probe.restype = ctypes.c_bool
+    assert probe() in (True, False)

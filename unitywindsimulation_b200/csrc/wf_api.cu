@@ -211,6 +211,7 @@ int read_residual(wf_solver* h, double* out) {
 int do_vel_sweeps(wf_solver* h, int n, bool allow_fast) {
     const Params& P = h->P;
     const bool resid = h->cfg.calc_residual != 0;
+    const bool from_alias = h->iter_alias;
     int k = 0;
     if (allow_fast && h->fast && !resid && n > 0) {
         // Multi-sweep path: same buffer roles, several sweeps per launch.
@@ -236,9 +237,9 @@ int do_vel_sweeps(wf_solver* h, int n, bool allow_fast) {
         h->iter_alias = false;
     }
     std::swap(h->iI, h->iF);
-    if (k == n && n == 0) {
-        // zero sweeps: the two swaps cancel, nothing else changes
-    }
+    // one complete sweep from the aliased state: iterate 0 (velFieldLastIter
+    // after the loop) is velFieldLastTime itself
+    if (k == 1 && n == 1 && from_alias) h->iter_alias = true;
     return WF_OK;
 }
 

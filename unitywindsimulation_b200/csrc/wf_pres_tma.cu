@@ -41,9 +41,12 @@
 #include <mutex>
 
 #include "wf_sweeps.cuh"
+#include "wf_tma.cuh"
 
 namespace wf {
 namespace {
+
+using namespace tma;
 
 constexpr int TK = 4;              // sweeps per pass
 constexpr int TT = 32;             // tile edge (threads per row, rows)
@@ -82,56 +85,6 @@ static_assert(TU % TF == 0 && TU % TC == 0 && TU % kR == 0 && TU % 3 == 0 && TU 
 // t - 1 - TD + TC) after its last reader, level 1 at step t + 1; the face
 // slot after level K's read at step t + K.
 static_assert(TD + 2 <= TC && TK + 1 + TD <= TF, "rings too short for the prefetch distance");
-
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Wait for the phase of the given parity, bounded by limit_ns; false when
-// it ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
-    if (mbar_try(bar, parity)) return true;
-    const unsigned long long t0 = global_ns();
-    while (!mbar_try(bar, parity))
-        if (global_ns() - t0 > limit_ns) return false;
-    return true;
-}
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void tma_3d(unsigned dst, const CUtensorMap* map, int x, int y, int z, unsigned bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];" ::"r"(dst),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
-        : "memory");
-}
-__device__ __forceinline__ void tma_4d(unsigned dst, const CUtensorMap* map, int x, int y, int z, int q,
-                                       unsigned bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(dst),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(q), "r"(bar)
-        : "memory");
-}
 
 struct TmaMaps {
     CUtensorMap face;  // 4-D {nx, ny, nz, 2} (c_E, c_N), box of both planes
@@ -293,8 +246,9 @@ static_assert((TU / TC) % 2 == 0, "a trip must advance every column slot by an e
 #define WF_TMA_ROWS 2
 #endif
 // Tile rows per thread.  Measured on the 256 x 96 x 192 urban block, four
-// sweeps per pass: 68.3 us with one row (1024 threads), 65.7 us with two
-// (512 threads), 78.9 us with four (256 threads); bit-identical iterates.
+// sweeps per pass, on two machines: 68.3 / 87.1 us with one row (1024
+// threads), 65.7 / 73.0 us with two (512 threads), 78.9 us (first machine)
+// with four (256 threads); bit-identical iterates.
 constexpr int TR = WF_TMA_ROWS;
 static_assert(TT % TR == 0, "rows per thread must divide the tile");
 
@@ -400,20 +354,29 @@ EncodeFn encoder() {
 #endif
 constexpr CUtensorMapL2promotion kL2Promotion = WF_TMA_L2P;
 
-// Tiled map over `planes` consecutive N-float planes of a grid (rank 3 when
-// planes == 1, else rank 4), box 32 x 32 x 1 (x box_planes), zero fill
-// outside.
-bool encode(CUtensorMap* m, const Params& P, const float* base, int planes, int box_planes) {
+}  // namespace
+
+bool tma_available() { return encoder() != nullptr; }
+
+bool tma_encode(CUtensorMap* m, const Params& P, const float* base, int planes, int box_w, int box_h,
+                int box_planes) {
     EncodeFn fn = encoder();
     if (!fn || !base) return false;
     const cuuint64_t dims[4] = {(cuuint64_t)P.nx, (cuuint64_t)P.ny, (cuuint64_t)P.nz, (cuuint64_t)planes};
     const cuuint64_t strides[3] = {sizeof(float) * (cuuint64_t)P.nx, sizeof(float) * (cuuint64_t)P.nx * P.ny,
                                    sizeof(float) * (cuuint64_t)P.N};
-    const cuuint32_t box[4] = {TT, TT, 1, (cuuint32_t)box_planes};
+    const cuuint32_t box[4] = {(cuuint32_t)box_w, (cuuint32_t)box_h, 1, (cuuint32_t)box_planes};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, planes > 1 ? 4 : 3, const_cast<float*>(base), dims, strides, box,
               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, kL2Promotion,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+namespace {
+
+// Map of this pass's 32 x 32 tiles.
+bool encode(CUtensorMap* m, const Params& P, const float* base, int planes, int box_planes) {
+    return tma_encode(m, P, base, planes, TT, TT, box_planes);
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -425,7 +388,7 @@ const void* pres_tma_kernel() { return reinterpret_cast<const void*>(k_pres_tma4
 
 bool pres_tma_ok(const Params& P, const float* c3, const float* ainv, const float* rhs, const float* in) {
     return P.nx % 4 == 0 && c3 && ainv && aligned16(c3) && aligned16(ainv) && aligned16(rhs) && aligned16(in) &&
-           encoder() != nullptr;
+           tma_available();
 }
 
 cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const float* c3, const float* ainv,

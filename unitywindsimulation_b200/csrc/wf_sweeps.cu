@@ -848,6 +848,10 @@ template <int K>
 void launch_vmsweep_k(wf_solver* h, const float* in, float* out, float* prev) {
     const Params& P = h->P;
     const size_t N = P.N;
+    if (K == 2 && h->pres_tma && h->dstat && vel_tma_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, in) &&
+        launch_vel_tma2(P, h->st, h->num_sms, h->vcoef, h->vcoef + 6 * N, h->bv, in, out, prev, h->dstat) ==
+            cudaSuccess)
+        return;
     constexpr int OX = MV_TX - 2 * K, OY = MV_TY - 2 * K;
     const int gx = (P.nx + OX - 1) / OX, gy = (P.ny + OY - 1) / OY;
     int zchunk = 0, nchunk = 0;
@@ -883,6 +887,8 @@ int sweeps_setup() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(pres_tma_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pres_tma_smem());
     if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(vel_tma_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_tma_smem());
+    if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_vel_msweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_msweep_smem(1));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_vel_msweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel_msweep_smem(2));
@@ -903,6 +909,7 @@ int record_vel_loop(wf_solver* h, int n) {
     L.iD = h->vcoef + 6 * N;
     L.bv = h->bv;
     L.vec4 = quad_ok(P, {L.A, L.iD, L.bv, h->vb[0], h->vb[1], h->vb[2], h->vb[3]});
+    const bool from_alias = h->iter_alias;
     for (int k = 0; k < n; ++k) {
         L.src.push_back(h->iter_alias ? h->vb[h->iT] : h->vb[h->iI]);
         L.dst.push_back(h->vb[h->iF]);
@@ -910,6 +917,7 @@ int record_vel_loop(wf_solver* h, int n) {
         h->iter_alias = false;
     }
     std::swap(h->iI, h->iF);
+    if (n == 1 && from_alias) h->iter_alias = true;  // iterate 0 is velFieldLastTime
     h->rec->kinds.push_back(0);
     h->rec->vel.push_back(std::move(L));
     return WF_OK;
@@ -961,6 +969,9 @@ int vel_sweeps_fast(wf_solver* h, int n) {
         }
         return cudaGetLastError() == cudaSuccess ? WF_OK : WF_ERR_CUDA;
     }
+    // After one sweep from the aliased state, iterate n-1 = iterate 0 is
+    // velFieldLastTime itself: the alias stays (the buffer at iI is scratch).
+    const bool from_alias = h->iter_alias;
     for (int k = 0; k < n; ++k) {
         const float* src = h->iter_alias ? h->vb[h->iT] : h->vb[h->iI];
         launch_vel_sweep_fast(h, src, h->vb[h->iF]);
@@ -968,6 +979,7 @@ int vel_sweeps_fast(wf_solver* h, int n) {
         h->iter_alias = false;
     }
     std::swap(h->iI, h->iF);
+    if (n == 1 && from_alias) h->iter_alias = true;
     return cudaGetLastError() == cudaSuccess ? WF_OK : WF_ERR_CUDA;
 }
 

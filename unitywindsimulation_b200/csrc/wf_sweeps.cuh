@@ -159,6 +159,19 @@ cudaError_t launch_pres_tma4(const Params& P, cudaStream_t st, int sms, const fl
                              const float* rhs, const float* in, float* out, float* prev, float* stack, int* status,
                              double wait_ms = 0.0, bool short_stage = false);
 
+// Two momentum sweeps per pass with TMA-staged tiles (wf_vel_tma.cu): the
+// same iterates n and n-1 as two k_vel_sweep4 sweeps, bit for bit.  A holds
+// A_E..A_D and iD the three components of 1/D, each as consecutive N-float
+// planes.  Applies where vel_tma_ok (nx % 4 == 0, 16-byte aligned planes,
+// the driver's tensor-map encoder present).  A bounded wait that runs out
+// sets *status to 1.
+size_t vel_tma_smem();
+const void* vel_tma_kernel();
+bool vel_tma_ok(const Params& P, const float* A, const float* iD, const float* bv, const float* in);
+cudaError_t launch_vel_tma2(const Params& P, cudaStream_t st, int sms, const float* A, const float* iD,
+                            const float* bv, const float* in, float* out, float* prev, int* status,
+                            double wait_ms = 0.0);
+
 // Event-timed launches of one hot kernel (WF_KERNEL_*), see wf_time_kernel.
 int time_kernel(wf_solver* h, int which, int reps, bool flush, float* ms, double* bytes, int* sweeps);
 
