@@ -36,34 +36,14 @@ namespace {
 __device__ __forceinline__ float ld(const float* p, size_t i) { return __ldg(p + i); }
 __device__ __forceinline__ bool fluid_at(const uint8_t* fl, int i) { return __ldg(fl + i) == WF_CELL_FLUID; }
 
-__device__ __forceinline__ float face_read(const Params& P, const float* face, int i, int axis) {
-    if ((P.compat & WF_COMPAT_RFLOAT_FACE_EDDY_VIS) && axis != 0) return 0.f;
-    return ld(face, (size_t)axis * P.N + i);
-}
-// Same face viscosity as the reference sweep (FvmColl.compute:1962-2001).
-__device__ __forceinline__ float vis_face(const Params& P, const uint8_t* fl, const float* eddy, const float* face,
-                                          int x, int y, int z, int i, int f) {
-    if (!P.les) return P.nu;
-    const int X = x + face_ox(f), Y = y + face_oy(f), Z = z + face_oz(f);
-    const float eP = ld(eddy, i);
-    float v = P.nu + eP;
-    if (in_region(P, X, Y, Z)) {
-        const int q = cidx(P, X, Y, Z);
-        if (fluid_at(fl, q)) v = P.nu + 0.5f * (eP + ld(eddy, q));
-        else v = P.nu + face_read(P, face, face_sign(f) > 0 ? q : i, face_axis(f));
-    } else if (f == 3 && P.vbc[WF_FACE_Y0] == WF_BND_FIXED_VALUE) {
-        v = P.nu + face_read(P, face, i, 1);
-    }
-    return v;
-}
-
 __device__ __forceinline__ float inv_d(const float* iD, const float* Dv, size_t N, int a, int i) {
     return iD ? ld(iD, a * N + i) : 1.f / ld(Dv, a * N + i);
 }
 
 // Momentum coefficients.  A: 6 planes (faces E,W,N,S,U,D), iD: 3 planes.
 // A is non-zero only on fluid-fluid faces, where the face viscosity is
-// nu + (eddy_P + eddy_Q) / 2 (nu without LES), as in vis_face.
+// nu + (eddy_P + eddy_Q) / 2 (nu without LES), as in the reference sweep's
+// face viscosity (FvmColl.compute:1962-2001).
 __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __restrict__ fl,
                            const float* __restrict__ uT, const float* __restrict__ eddy,
                            const float* __restrict__ face, const float* __restrict__ Dv,
