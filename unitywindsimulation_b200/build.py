@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 SOURCES = ["wf_api.cu", "wf_kernels.cu", "wf_sweeps.cu", "wf_batch.cu", "wf_noalloc.cu", "wf_adjoint.cu", "wf_nested.cu", "wf_export.cu", "wf_raster.cu", "wf_nonuniform.cu", "wf_pres_tma.cu", "wf_vel_tma.cu"]
-HEADERS = ["wf_common.cuh", "wf_kernels.cuh", "wf_solver.cuh", "wf_sweeps.cuh", "wf_tma.cuh"]
+HEADERS = ["wf_common.cuh", "wf_kernels.cuh", "wf_solver.cuh", "wf_sweeps.cuh", "wf_tma.cuh", "wf_gridbar.cuh"]
 OUT = os.path.join(HERE, "libwindfvm.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

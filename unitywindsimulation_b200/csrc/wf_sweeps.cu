@@ -22,6 +22,7 @@
 
 #include "wf_kernels.cuh"
 #include "wf_sweeps.cuh"
+#include "wf_gridbar.cuh"
 
 namespace wf {
 
@@ -99,7 +100,22 @@ __global__ void k_vel_coef(const __grid_constant__ Params P, const uint8_t* __re
 // not once for 1/D and again for the rest (76 -> 63 us per sweep on the
 // urban block; indices are clamped in-domain, so the loads of non-fluid cells
 // are harmless and their results unused).
-template <bool kCopyAll>
+// Loads of an iterate.  kCoh: the iterate was written earlier in the same
+// kernel by other blocks (the persistent loops, across a grid barrier), so it
+// is read through L2 (ld.global.cg), never through the non-coherent
+// read-only path that __ldg uses.
+template <bool kCoh>
+__device__ __forceinline__ float ldi(const float* p, size_t i) {
+    if constexpr (kCoh) return __ldcg(p + i);
+    else return __ldg(p + i);
+}
+template <bool kCoh>
+__device__ __forceinline__ float4 ldi4(const float* p, size_t i) {
+    if constexpr (kCoh) return __ldcg(reinterpret_cast<const float4*>(p + i));
+    else return __ldg(reinterpret_cast<const float4*>(p + i));
+}
+
+template <bool kCopyAll, bool kCoh = false>
 __device__ __forceinline__ void vel_sweep1_at(const Params& P, const float* __restrict__ A,
                                               const float* __restrict__ iD, const float* __restrict__ bv,
                                               const float* __restrict__ ui, float* __restrict__ uo, int x, int y,
@@ -121,18 +137,18 @@ __device__ __forceinline__ void vel_sweep1_at(const Params& P, const float* __re
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float* u = ui + k * N;
-        float s = a0 * ld(u, iE);
-        s += a1 * ld(u, iW);
-        s += a2 * ld(u, iN);
-        s += a3 * ld(u, iS);
-        s += a4 * ld(u, iU);
-        s += a5 * ld(u, iDn);
+        float s = a0 * ldi<kCoh>(u, iE);
+        s += a1 * ldi<kCoh>(u, iW);
+        s += a2 * ldi<kCoh>(u, iN);
+        s += a3 * ldi<kCoh>(u, iS);
+        s += a4 * ldi<kCoh>(u, iU);
+        s += a5 * ldi<kCoh>(u, iDn);
         r[k] = s + ld(bv, k * N + i);
     }
     if (d0 == 0.f) {  // non-fluid cell
         if (kCopyAll)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) uo[k * N + i] = ld(ui, k * N + i);
+            for (int k = 0; k < 3; ++k) uo[k * N + i] = ldi<kCoh>(ui, k * N + i);
         return;
     }
     uo[i] = d0 * r[0];
@@ -159,7 +175,7 @@ __global__ void __launch_bounds__(256) k_vel_sweep1(const __grid_constant__ Para
 __device__ __forceinline__ float4 ld4(const float* p, size_t i) { return __ldg(reinterpret_cast<const float4*>(p + i)); }
 __device__ __forceinline__ float f4(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
 
-template <bool kCopyAll>
+template <bool kCopyAll, bool kCoh = false>
 __device__ __forceinline__ void vel_sweep4_at(const Params& P, const float* __restrict__ A,
                                               const float* __restrict__ iD, const float* __restrict__ bv,
                                               const float* __restrict__ ui, float* __restrict__ uo, int x0, int y,
@@ -184,13 +200,13 @@ __device__ __forceinline__ void vel_sweep4_at(const Params& P, const float* __re
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float* u = ui + k * N;
-        c[k] = ld4(u, i);
-        n[k] = ld4(u, iN);
-        so[k] = ld4(u, iS);
-        up[k] = ld4(u, iU);
-        dn[k] = ld4(u, iDn);
-        e3[k] = __ldg(u + iE);
-        w0[k] = __ldg(u + iW);
+        c[k] = ldi4<kCoh>(u, i);
+        n[k] = ldi4<kCoh>(u, iN);
+        so[k] = ldi4<kCoh>(u, iS);
+        up[k] = ldi4<kCoh>(u, iU);
+        dn[k] = ldi4<kCoh>(u, iDn);
+        e3[k] = ldi<kCoh>(u, iE);
+        w0[k] = ldi<kCoh>(u, iW);
         bb[k] = ld4(bv, k * N + i);
     }
     float r[3][4];
@@ -404,7 +420,7 @@ constexpr int MS_TX = 32;
 // or 16 (512 threads, two blocks per SM; more tiles for small grids).
 constexpr size_t pres_msweep_smem(int K, int TY = 32) { return sizeof(float) * MS_TX * TY * (2 * K + 2 * 6); }
 
-template <int K, int MS_TY>
+template <int K, int MS_TY, bool kCoh = false>
 struct PresWave {
     static_assert(K >= 1 && K <= 4, "ring of 6 planes holds K <= 4");
     static constexpr int R = 6;  // ring period: unrolled z steps per loop trip
@@ -430,7 +446,7 @@ struct PresWave {
     __device__ __forceinline__ void fetch(int p, float& a, float& r) {
         if (inxy && p >= 0 && p < nz) {
             const int i = p * sxy + col;
-            pv = pin ? __ldg(pin + i) : 0.f;
+            pv = pin ? ldi<kCoh>(pin, i) : 0.f;
             pe = __ldg(cE + i);
             pn = __ldg(cN + i);
             pu = __ldg(cU + i);
@@ -489,7 +505,7 @@ struct PresWave {
 
 // One tile (bx, by) and z chunk bz of a K-sweep pass, run by a block of
 // MS_TX x MS_TY threads over the shared memory at msm (pres_msweep_smem).
-template <int K, int MS_TY>
+template <int K, int MS_TY, bool kCoh = false>
 __device__ __forceinline__ void pres_wave_tile(const Params& P, const float* __restrict__ c3,
                                                const float* __restrict__ ainv, const float* __restrict__ rhs,
                                                const float* __restrict__ pin, float* __restrict__ pout,
@@ -497,10 +513,10 @@ __device__ __forceinline__ void pres_wave_tile(const Params& P, const float* __r
                                                int bx, int by, int bz, float* msm) {
     // shared memory: V[K][2][TY][TX] level planes, CE/CN[6][TY][TX]
     // coefficient rings
-    PresWave<K, MS_TY> w;
+    PresWave<K, MS_TY, kCoh> w;
     w.V = reinterpret_cast<float(*)[2][MS_TY][MS_TX]>(msm);
     w.CE = reinterpret_cast<float(*)[MS_TY][MS_TX]>(msm + K * 2 * MS_TY * MS_TX);
-    w.CN = w.CE + PresWave<K, MS_TY>::R;
+    w.CN = w.CE + PresWave<K, MS_TY, kCoh>::R;
     w.tx = threadIdx.x;
     w.ty = threadIdx.y;
     constexpr int OX = MS_TX - 2 * K, OY = MS_TY - 2 * K;
@@ -530,7 +546,7 @@ __device__ __forceinline__ void pres_wave_tile(const Params& P, const float* __r
 #pragma unroll
     for (int s = 0; s < K; ++s) w.V[s][0][w.ty][w.tx] = w.V[s][1][w.ty][w.tx] = 0.f;
 #pragma unroll
-    for (int r = 0; r < PresWave<K, MS_TY>::R; ++r) {
+    for (int r = 0; r < PresWave<K, MS_TY, kCoh>::R; ++r) {
         w.CE[r][w.ty][w.tx] = w.CN[r][w.ty][w.tx] = 0.f;
         w.qa[r] = w.qr[r] = w.qu[r] = 0.f;
     }
@@ -540,7 +556,7 @@ __device__ __forceinline__ void pres_wave_tile(const Params& P, const float* __r
     w.T = (w.z1 - w.z0) + 2 * K;
     w.fetch(w.zs, w.qa[0], w.qr[0]);
     __syncthreads();
-    for (int t = 0; t < w.T; t += PresWave<K, MS_TY>::R) {
+    for (int t = 0; t < w.T; t += PresWave<K, MS_TY, kCoh>::R) {
         w.template step<0>(t);
         w.template step<1>(t + 1);
         w.template step<2>(t + 2);
@@ -1233,52 +1249,6 @@ void launch_piso_pre_ptr(const Params& P, cudaStream_t st, const uint8_t* fl, co
 
 namespace {
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Grid-wide barrier for `expected` arriving blocks.  Returns false (on every
-// thread of the block) when the barrier's error word is or becomes set, or
-// when this block waited longer than timeout_ns.
-__device__ bool grid_barrier(GridBar* bar, unsigned expected, unsigned long long timeout_ns) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
-        volatile GridBar* vb = bar;
-        int good = vb->err == 0;
-        if (good) {
-            const unsigned gen = vb->gen;
-            __threadfence();
-            const unsigned arrived = atomicAdd(&bar->count, 1u) + 1u;
-            if (arrived == expected) {
-                bar->count = 0;
-                __threadfence();
-                atomicAdd(&bar->gen, 1u);
-            } else {
-                const unsigned long long t0 = global_ns();
-                while (vb->gen == gen) {
-                    if (vb->err != 0) {
-                        good = 0;
-                        break;
-                    }
-                    if (global_ns() - t0 > timeout_ns) {
-                        atomicExch(&bar->err, 1);
-                        good = 0;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-            __threadfence();
-        }
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
 // The momentum loop: nsweeps sweeps of every case, items = the blocks of
 // each case's sweep grid (32 x 4 x 2 threads; the four-cell form covers 128
 // x cells per block row).
@@ -1293,10 +1263,11 @@ __global__ void __launch_bounds__(256) k_fused_vel_loop(const FusedVelCase* __re
             const int local = it - q.item0;
             const int bx = local % q.gx, by = (local / q.gx) % q.gy, bz = local / (q.gx * q.gy);
             const int x = bx * 32 + threadIdx.x, y = by * 4 + threadIdx.y, z = bz * 2 + threadIdx.z;
+            // iterates written by earlier sweeps of this kernel: coherent loads
             if (q.vec4)
-                vel_sweep4_at<false>(q.P, q.A, q.iD, q.bv, q.src[s], q.dst[s], 4 * x, y, z);
+                vel_sweep4_at<false, true>(q.P, q.A, q.iD, q.bv, q.src[s], q.dst[s], 4 * x, y, z);
             else
-                vel_sweep1_at<false>(q.P, q.A, q.iD, q.bv, q.src[s], q.dst[s], x, y, z);
+                vel_sweep1_at<false, true>(q.P, q.A, q.iD, q.bv, q.src[s], q.dst[s], x, y, z);
         }
         if (s + 1 < nsweeps && !grid_barrier(bar, gridDim.x, timeout_ns)) return;
     }
@@ -1324,19 +1295,19 @@ __global__ void __launch_bounds__(1024, 1) k_fused_pres_loop(const FusedPresCase
             const int bx = local % ps.gx, by = (local / ps.gx) % ps.gy, bz = local / (ps.gx * ps.gy);
             switch (ps.k) {
                 case 1:
-                    pres_wave_tile<1, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                    pres_wave_tile<1, 32, true>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
                                           bz, fsm);
                     break;
                 case 2:
-                    pres_wave_tile<2, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                    pres_wave_tile<2, 32, true>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
                                           bz, fsm);
                     break;
                 case 3:
-                    pres_wave_tile<3, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                    pres_wave_tile<3, 32, true>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
                                           bz, fsm);
                     break;
                 default:
-                    pres_wave_tile<4, 32>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
+                    pres_wave_tile<4, 32, true>(q.P, q.c3, q.ainv, q.rhs, ps.in, ps.out, nullptr, ps.zchunk, nullptr, bx, by,
                                           bz, fsm);
                     break;
             }
