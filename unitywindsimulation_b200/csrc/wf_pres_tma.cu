@@ -10,10 +10,12 @@
 // y neighbours and one south face coefficient come from the thread's own
 // registers; 16 warps per SM with two independent cells each.
 // What differs is how a plane reaches shared memory.  Each z plane of the
-// tile arrives as six 32 x 32 FP32 planes (24 KB): c_E, c_N, c_U and 1/Dp
-// (two 4-D tensor-map boxes of two planes over the contiguous coefficient
-// cache), the right-hand side and the input iterate, written by up to four
-// cp.async.bulk.tensor loads that complete on one mbarrier.  One thread
+// tile arrives as six 32 x 32 FP32 planes (24 KB): c_E and c_N (one 4-D
+// tensor-map box of two consecutive planes of the coefficient cache), c_U,
+// 1/Dp, the right-hand side and the input iterate (3-D boxes), written by up
+// to five cp.async.bulk.tensor loads that complete on one mbarrier.  With a
+// `stack` the pass also writes every level of every cell (the adjoint's
+// taped and reversed loops).  One thread
 // issues them TD planes ahead of the plane the block consumes, into two
 // rings (below) that hold every plane a level still reads.  So no thread
 // issues a global load or a staging store: per step a thread reads its own
