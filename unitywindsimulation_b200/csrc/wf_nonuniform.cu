@@ -469,10 +469,23 @@ __device__ __forceinline__ NuPresCoef nu_pres_coef(const Params& P, const float*
     return k;
 }
 
-// The pressure update of the four cells at i (k_nu_pres_sweep's arithmetic
-// per cell) from their coefficients k and the iterate pin (null: zero).
-__device__ __forceinline__ void nu_pres_quad(const Params& P, const NuPresCoef& k, const float* __restrict__ pin,
-                                             float* __restrict__ pout, int i) {
+__global__ void __launch_bounds__(256) k_nu_pres_sweep4(const __grid_constant__ Params P,
+                                                        const float* __restrict__ pin,
+                                                        const float* __restrict__ coef,
+                                                        const float* __restrict__ bp, float* __restrict__ pout,
+                                                        int pre) {
+    // pre: the coefficient planes, bp and the masks were written before the
+    // previous grid of the chain (every sweep after the first): they load
+    // before chain_wait.
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = q < P.N / 4;
+    const int i = in ? 4 * q : 0;
+    NuPresCoef k{};
+    if (pre && in) k = nu_pres_coef(P, coef, bp, i);
+    chain_wait();
+    chain_release();
+    if (!in) return;
+    if (!pre) k = nu_pres_coef(P, coef, bp, i);
     const uchar4 mq = k.mq;
     const float4* c = k.c;
     const float4 inv = k.inv, b = k.b;
@@ -506,26 +519,6 @@ __device__ __forceinline__ void nu_pres_quad(const Params& P, const NuPresCoef& 
         for (int j = 0; j < 4; ++j)
             if (ms[j] & 64u) pout[i + j] = v[j];
     }
-}
-
-__global__ void __launch_bounds__(256) k_nu_pres_sweep4(const __grid_constant__ Params P,
-                                                        const float* __restrict__ pin,
-                                                        const float* __restrict__ coef,
-                                                        const float* __restrict__ bp, float* __restrict__ pout,
-                                                        int pre) {
-    // pre: the coefficient planes, bp and the masks were written before the
-    // previous grid of the chain (every sweep after the first): they load
-    // before chain_wait.
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool in = q < P.N / 4;
-    const int i = in ? 4 * q : 0;
-    NuPresCoef k{};
-    if (pre && in) k = nu_pres_coef(P, coef, bp, i);
-    chain_wait();
-    chain_release();
-    if (!in) return;
-    if (!pre) k = nu_pres_coef(P, coef, bp, i);
-    nu_pres_quad(P, k, pin, pout, i);
 }
 
 // CSApplyVelCorrectionDivergenceTheorem, FvmCollNonUniform.compute:1487-1731.
