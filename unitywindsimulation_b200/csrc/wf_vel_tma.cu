@@ -4,9 +4,9 @@
 // A block owns a 32 x 32 column tile of the x-y plane (a 28 x 28 output tile
 // with a 2-cell halo on every side) and streams a chunk of z planes; level 1
 // computes plane zs + t - 1 and level 2 plane zs + t - 2 at step t.  Each z
-// plane of the tile arrives as 13 planes of 36 x 32 FP32 values: the six
-// off-diagonal coefficients A_E..A_D, the first component of 1/D, the three
-// components of b and of the input iterate.  The boxes start at x = 28 bx - 4
+// plane of the tile arrives as 14 planes of 36 x 32 FP32 values: the six
+// off-diagonal coefficients A_E..A_D, the first two components of 1/D, the
+// three components of b and of the input iterate.  The boxes start at x = 28 bx - 4
 // (16-byte aligned) and are 36 wide, so the thread of column tx reads column
 // tx + 2 and its x neighbours are always inside the box.  One thread issues
 // the loads (four cp.async.bulk.tensor per plane, one mbarrier) one plane
@@ -20,8 +20,10 @@
 // coefficients from its ring slot and keeps them in registers for level 2 at
 // the next step (two register sets, alternating with the step's parity).
 // The three components of 1/D are bit-identical outside the cells with a
-// symmetry domain face (d_split); those cells read the other two components
-// from global memory.  Non-fluid cells (1/D = 0) carry their input value
+// symmetry domain face (d_split), and each differs from the others only by
+// the term of faces normal to its own axis: the third component is taken
+// from the first two, and read from global memory only on z-symmetry planes
+// and x-y symmetry edges.  Non-fluid cells (1/D = 0) carry their input value
 // through both levels and are never written.  The arithmetic, its order and
 // every stored value are those of k_vel_sweep4, so two sweeps of either give
 // bit-identical iterates.
@@ -30,9 +32,10 @@
 // and a wait that runs out sets the handle's sticky wait status.
 //
 // Selected by a momentum blocking depth of 2 (wf_set_blocking).  Not the
-// default: on the 256 x 96 x 192 urban block it takes 56.1 us per sweep
-// against 49.6 us for one k_vel_sweep4 launch per sweep, which is bound by
-// the on-chip path from L2, not by the DRAM bytes this pass halves.
+// default: on the 256 x 96 x 192 urban block it takes 52.3 us per sweep
+// against 49.3 us for one k_vel_sweep4 launch per sweep, which is bound by
+// the on-chip path from L2, not by the DRAM bytes this pass halves; the
+// autotuner picks it on some smaller grids.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -56,8 +59,8 @@ constexpr int VTHR = VT * VT / VR; // threads per block
 constexpr int VD = 1;              // planes loaded ahead of the consumed one
 constexpr int VC = VD + 2;         // ring slots (a plane is read at steps p and p + 1)
 constexpr int VU = 6;              // unrolled steps per trip: lcm of 3 (slots, rings) and 2 (sets)
-// staged planes of one slot: A_E..A_D, 1/D (first component), b, u
-enum { S_A = 0, S_ID = 6, S_B = 7, S_U = 10, VQ = 13 };
+// staged planes of one slot: A_E..A_D, 1/D (first two components), b, u
+enum { S_A = 0, S_ID = 6, S_ID1 = 7, S_B = 8, S_U = 11, VQ = 14 };
 constexpr int kVSlot = VQ * VPL;
 constexpr size_t kVSmemFloats = (size_t)VC * kVSlot + (size_t)2 * 3 * VPL;
 constexpr size_t kVSmemBytes = kVSmemFloats * sizeof(float) + VC * sizeof(unsigned long long) + 1024;
@@ -69,7 +72,7 @@ static_assert(VU % VC == 0 && (VU / VC) % 2 == 0 && VU % 2 == 0, "trip must cove
 
 struct VelMaps {
     CUtensorMap A;    // 4-D {nx, ny, nz, 6}, box 36 x 32 x 1 x 6
-    CUtensorMap iD;   // 3-D, box 36 x 32 x 1 (first component)
+    CUtensorMap iD;   // 4-D {nx, ny, nz, 2}, box of the first two components
     CUtensorMap b;    // 4-D {nx, ny, nz, 3}, box of three planes
     CUtensorMap u;    // 4-D {nx, ny, nz, 3}, box of three planes
 };
@@ -86,7 +89,7 @@ struct VelWaveT {
     int me;                   // row 0's own offset in a staged plane (column tx + 2)
     int r0, zs, z0, z1, T, sxy, x0, y0, tfail;
     int col[VR];
-    bool out_col[VR], in_xy[VR], split_xy[VR];  // split_xy: the cell has a symmetry x or y domain face
+    bool out_col[VR], in_xy[VR], split_x[VR], split_y[VR];  // the cell has a symmetry x / y domain face
     bool split_z0, split_zn;  // symmetry faces at z = 0 / z = nz - 1
     bool bad, lead;
     int nz;
@@ -102,7 +105,7 @@ struct VelWaveT {
         const unsigned dst = smem_addr(ring + slot * kVSlot);
         mbar_expect(bar, (unsigned)(sizeof(float) * VPL * VQ));
         tma_4d(dst + sizeof(float) * VPL * S_A, &maps->A, x0, y0, p, 0, bar);
-        tma_3d(dst + sizeof(float) * VPL * S_ID, &maps->iD, x0, y0, p, bar);
+        tma_4d(dst + sizeof(float) * VPL * S_ID, &maps->iD, x0, y0, p, 0, bar);
         tma_4d(dst + sizeof(float) * VPL * S_B, &maps->b, x0, y0, p, 0, bar);
         tma_4d(dst + sizeof(float) * VPL * S_U, &maps->u, x0, y0, p, 0, bar);
     }
@@ -151,15 +154,19 @@ struct VelWaveT {
                 const int o = me + k * VW;
 #pragma unroll
                 for (int f = 0; f < 6; ++f) cA[c1][k][f] = plane(sP, S_A + f)[o];
-                const float id0 = plane(sP, S_ID)[o];
-                cI[c1][k][0] = cI[c1][k][1] = cI[c1][k][2] = id0;
+                const float id0 = plane(sP, S_ID)[o], id1 = plane(sP, S_ID1)[o];
+                // component c of 1/D is the base value plus the symmetry term of
+                // faces normal to axis c: the third equals the first outside
+                // x-symmetry cells and the second outside y-symmetry cells; only
+                // z-symmetry planes and x-y symmetry edges read it from memory
+                cI[c1][k][0] = id0;
+                cI[c1][k][1] = id1;
+                cI[c1][k][2] = split_x[k] ? id1 : id0;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) cB[c1][k][c] = plane(sP, S_B + c)[o];
-                if (pin && in_xy[k] && (split_xy[k] || (p == 0 && split_z0) || (p == nz - 1 && split_zn))) {
-                    const size_t gi = (size_t)p * sxy + col[k];
-                    cI[c1][k][1] = __ldg(iDg + N + gi);
-                    cI[c1][k][2] = __ldg(iDg + 2 * N + gi);
-                }
+                if (pin && in_xy[k] &&
+                    ((split_x[k] && split_y[k]) || (p == 0 && split_z0) || (p == nz - 1 && split_zn)))
+                    cI[c1][k][2] = __ldg(iDg + 2 * N + (size_t)p * sxy + col[k]);
             }
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -258,10 +265,10 @@ __global__ void __launch_bounds__(VTHR, 1)
         w.in_xy[k] = inxy;
         w.out_col[k] = inxy && tx >= VK && tx < VT - VK && r >= VK && r < VT - VK;
         w.col[k] = inxy ? y * P.nx + x : 0;
-        w.split_xy[k] = inxy && ((x == 0 && P.vbc[WF_FACE_X0] == WF_BND_SYMMETRY) ||
-                                 (x == P.nx - 1 && P.vbc[WF_FACE_XN] == WF_BND_SYMMETRY) ||
-                                 (y == 0 && P.vbc[WF_FACE_Y0] == WF_BND_SYMMETRY) ||
-                                 (y == P.ny - 1 && P.vbc[WF_FACE_YN] == WF_BND_SYMMETRY));
+        w.split_x[k] = inxy && ((x == 0 && P.vbc[WF_FACE_X0] == WF_BND_SYMMETRY) ||
+                                (x == P.nx - 1 && P.vbc[WF_FACE_XN] == WF_BND_SYMMETRY));
+        w.split_y[k] = inxy && ((y == 0 && P.vbc[WF_FACE_Y0] == WF_BND_SYMMETRY) ||
+                                (y == P.ny - 1 && P.vbc[WF_FACE_YN] == WF_BND_SYMMETRY));
     }
     w.bad = false;
     w.tfail = 0;
@@ -316,7 +323,7 @@ cudaError_t launch_vel_tma2(const Params& P, cudaStream_t st, int sms, const flo
                             const float* bv, const float* in, float* out, float* prev, int* status, double wait_ms) {
     VelMaps maps;
     std::memset(&maps, 0, sizeof(maps));
-    if (!tma_encode(&maps.A, P, A, 6, VW, VT, 6) || !tma_encode(&maps.iD, P, iD, 1, VW, VT, 1) ||
+    if (!tma_encode(&maps.A, P, A, 6, VW, VT, 6) || !tma_encode(&maps.iD, P, iD, 2, VW, VT, 2) ||
         !tma_encode(&maps.b, P, bv, 3, VW, VT, 3) || !tma_encode(&maps.u, P, in, 3, VW, VT, 3))
         return cudaErrorInvalidValue;
     const int gx = (P.nx + VO - 1) / VO, gy = (P.ny + VO - 1) / VO;
