@@ -29,7 +29,7 @@ struct Params {
     float dx, ds, dv, dt, nu, den, cs;
     // Reciprocals computed once on the host: x * rdx in place of x / dx (and
     // the like) saves an IEEE division per use.  Exact where dx and den are
-    // powers of two (every BASELINE workload: dx = 0.5, den = 1); within one
+    // powers of two (every benchmarked workload: dx = 0.5, den = 1); within one
     // rounding of the quotient otherwise.  dvden = dv / den is the quotient
     // itself.
     float rdx, rdx2, rden, dvden;

@@ -305,7 +305,9 @@ __global__ void __launch_bounds__(TT* TT / TR, 1)
     w.extra_tx = extra_tx;
     // The rings and the level planes start at zero (the rhs and input planes
     // stay zero when absent: no load writes them).
-    for (int i = tid; i < (int)kSmemFloats; i += TT * TT / TR) base[i] = 0.f;
+    static_assert(kSmemFloats % 4 == 0, "the rings are cleared with 16-byte stores");
+    for (int i = tid; i < (int)(kSmemFloats / 4); i += TT * TT / TR)
+        reinterpret_cast<float4*>(base)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < TR; ++k) {
 #pragma unroll

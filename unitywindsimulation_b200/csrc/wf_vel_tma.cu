@@ -273,7 +273,9 @@ __global__ void __launch_bounds__(VTHR, 1)
     w.bad = false;
     w.tfail = 0;
     w.wait_ns = wait_ns;
-    for (int i = tid; i < (int)kVSmemFloats; i += VTHR) base[i] = 0.f;
+    static_assert(kVSmemFloats % 4 == 0, "the ring is cleared with 16-byte stores");
+    for (int i = tid; i < (int)(kVSmemFloats / 4); i += VTHR)
+        reinterpret_cast<float4*>(base)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < VR; ++k) {
 #pragma unroll
