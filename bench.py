@@ -70,6 +70,8 @@ def parse():
                          "(the target program of an ncu capture); prints one JSON line")
     ap.add_argument("--adjoint", action="store_true",
                     help="with --kernels: also run the objective gradient over --steps steps")
+    ap.add_argument("--vel-k", type=int, default=0,
+                    help="with --kernels: momentum sweeps per pass (1 or 2; 0: the library's default)")
     return ap.parse_args()
 
 
@@ -695,8 +697,11 @@ def run_kernels(args):
     case = make_case(args.workload)
     s = FvmSolverCuda(case.cfg)
     cases.apply_case(s, case)
+    if args.vel_k:
+        s.set_blocking(s.get_blocking()[0], args.vel_k)
     s.Step(args.steps)
-    out = {"workload": args.workload, "cells": case.n_cells, "step_ms": s.last_step_ms() / max(args.steps, 1)}
+    out = {"workload": args.workload, "cells": case.n_cells, "step_ms": s.last_step_ms() / max(args.steps, 1),
+           "blocking": list(s.get_blocking())}
     if case.faces is None:
         for name, k in (("pres_sweep", _lib.KERNEL_PRES_SWEEP), ("vel_sweep", _lib.KERNEL_VEL_SWEEP)):
             ms, by, sw = s.time_kernel(k, reps=2, flush_l2=True)
