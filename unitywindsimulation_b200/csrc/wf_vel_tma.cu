@@ -32,10 +32,11 @@
 // and a wait that runs out sets the handle's sticky wait status.
 //
 // Selected by a momentum blocking depth of 2 (wf_set_blocking).  Not the
-// default: on the 256 x 96 x 192 urban block it takes 52.3 us per sweep
-// against 49.3 us for one k_vel_sweep4 launch per sweep, which is bound by
-// the on-chip path from L2, not by the DRAM bytes this pass halves; the
-// autotuner picks it on some smaller grids.
+// default: on the 256 x 96 x 192 urban block it takes 47.7 us per sweep
+// against 50.2 us for one k_vel_sweep4 launch per sweep in isolation, but
+// the graph-replayed step gains only 0.6 % (back to back, the one-sweep
+// launches find part of their input in L2); the autotuner picks either per
+// grid.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -90,6 +91,7 @@ struct VelWaveT {
     int r0, zs, z0, z1, T, sxy, x0, y0, tfail;
     int col[VR];
     bool out_col[VR], in_xy[VR], split_x[VR], split_y[VR];  // the cell has a symmetry x / y domain face
+    bool edge_xy[VR];         // inside the domain with both an x and a y symmetry face
     bool split_z0, split_zn;  // symmetry faces at z = 0 / z = nz - 1
     bool bad, lead;
     int nz;
@@ -149,6 +151,8 @@ struct VelWaveT {
         {
             const int p = zs + t - 1;
             const bool pin = p >= 0 && p < nz;
+            const bool zface = (p == 0 && split_z0) || (p == nz - 1 && split_zn);  // implies pin
+            bool fl[VR];
 #pragma unroll
             for (int k = 0; k < VR; ++k) {
                 const int o = me + k * VW;
@@ -164,9 +168,9 @@ struct VelWaveT {
                 cI[c1][k][2] = split_x[k] ? id1 : id0;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) cB[c1][k][c] = plane(sP, S_B + c)[o];
-                if (pin && in_xy[k] &&
-                    ((split_x[k] && split_y[k]) || (p == 0 && split_z0) || (p == nz - 1 && split_zn)))
+                if ((pin && edge_xy[k]) || (zface && in_xy[k]))
                     cI[c1][k][2] = __ldg(iDg + 2 * N + (size_t)p * sxy + col[k]);
+                fl[k] = id0 != 0.f;  // 1/D is 0 on non-fluid cells
             }
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -179,7 +183,7 @@ struct VelWaveT {
                     const float us = k > 0 ? h0[k - 1][q1][c] : U[o + ys0];
                     const float r = stencil(cA[c1][k], cI[c1][k][c], cB[c1][k][c], U[o + 1], U[o - 1], un, us,
                                             h0[k][q0][c], h0[k][q2][c]);
-                    const float v = cI[c1][k][0] != 0.f ? r : h0[k][q1][c];
+                    const float v = fl[k] ? r : h0[k][q1][c];
                     h1[k][q1][c] = v;
                     W[o] = v;
                 }
@@ -189,6 +193,7 @@ struct VelWaveT {
         if (r0 >= VK && r0 + VR - 1 < VT - VK) {
             const int q = zs + t - 2;
             const bool emit = uout && q >= z0 && q < z1;
+            float r2[VR][3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const float* U = v1(prv, c);
@@ -197,12 +202,23 @@ struct VelWaveT {
                     const int o = me + k * VW;
                     const float un = k + 1 < VR ? h1[k + 1][q2][c] : U[o + VW];
                     const float us = k > 0 ? h1[k - 1][q2][c] : U[o - VW];
-                    const float r = stencil(cA[c2][k], cI[c2][k][c], cB[c2][k][c], U[o + 1], U[o - 1], un, us,
-                                            h1[k][q1][c], h1[k][q0][c]);
-                    if (emit && out_col[k] && cI[c2][k][0] != 0.f) {
-                        const size_t i = (size_t)q * sxy + col[k];
-                        uout[c * N + i] = r;
-                        if (uprev) uprev[c * N + i] = h1[k][q2][c];
+                    r2[k][c] = stencil(cA[c2][k], cI[c2][k][c], cB[c2][k][c], U[o + 1], U[o - 1], un, us,
+                                       h1[k][q1][c], h1[k][q0][c]);
+                }
+            }
+            if (emit) {
+#pragma unroll
+                for (int k = 0; k < VR; ++k) {
+                    if (!out_col[k] || cI[c2][k][0] == 0.f) continue;
+                    float* o = uout + (size_t)q * sxy + col[k];
+                    o[0] = r2[k][0];
+                    o[N] = r2[k][1];
+                    o[2 * N] = r2[k][2];
+                    if (uprev) {
+                        float* w = uprev + (size_t)q * sxy + col[k];
+                        w[0] = h1[k][q2][0];
+                        w[N] = h1[k][q2][1];
+                        w[2 * N] = h1[k][q2][2];
                     }
                 }
             }
@@ -269,6 +285,7 @@ __global__ void __launch_bounds__(VTHR, 1)
                                 (x == P.nx - 1 && P.vbc[WF_FACE_XN] == WF_BND_SYMMETRY));
         w.split_y[k] = inxy && ((y == 0 && P.vbc[WF_FACE_Y0] == WF_BND_SYMMETRY) ||
                                 (y == P.ny - 1 && P.vbc[WF_FACE_YN] == WF_BND_SYMMETRY));
+        w.edge_xy[k] = w.split_x[k] && w.split_y[k];
     }
     w.bad = false;
     w.tfail = 0;
