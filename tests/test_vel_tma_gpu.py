@@ -43,6 +43,23 @@ def test_two_sweep_passes_bit_identical(built, kw):
     b.close()
 
 
+def test_two_sweep_passes_with_x_and_y_symmetry_faces(built):
+    """Symmetry faces normal to x (outlet) and y (ground and top) on top of
+    the z ones: the pass derives the third component of 1/D from the first
+    two in x- and y-symmetry cells and reads it from memory on z-symmetry
+    planes and on the x-y edges; every field still agrees bit for bit."""
+    case = cases.small_case(nx=40, ny=22, nz=26, seed=8, les=True)
+    for f in (_lib.FACE_XN, _lib.FACE_Y0, _lib.FACE_YN):
+        case.cfg.vel_bc[f] = _lib.BND_SYMMETRY
+    a, b = _pair(case, 2), _pair(case, 1)
+    for s in (a, b):
+        s.Step(3)
+    for f in ALL_FIELDS:
+        assert np.array_equal(a.get_field(f), b.get_field(f)), _lib.FIELD_NAMES[f]
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 6])
 def test_two_sweep_loop_iterates_n_and_n_minus_1(built, n):
     """A loop outside a step, started right after a step (velFieldLastIter

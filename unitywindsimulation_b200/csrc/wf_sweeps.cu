@@ -844,7 +844,9 @@ template <int K>
 void launch_vmsweep_k(wf_solver* h, const float* in, float* out, float* prev) {
     const Params& P = h->P;
     const size_t N = P.N;
-    if (K == 2 && h->pres_tma && h->dstat && vel_tma_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, in) &&
+    // uniform grid only: the pass derives the third component of 1/D from the
+    // structure of the uniform momentum pre-compute's diagonal
+    if (K == 2 && !h->nonuniform && h->pres_tma && h->dstat && vel_tma_ok(P, h->vcoef, h->vcoef + 6 * N, h->bv, in) &&
         launch_vel_tma2(P, h->st, h->num_sms, h->vcoef, h->vcoef + 6 * N, h->bv, in, out, prev, h->dstat) ==
             cudaSuccess)
         return;
